@@ -1,0 +1,442 @@
+#!/usr/bin/env python3
+"""Benchmark: MAP-EM iterations/s of positron-range correction at 128x128x159 68Ga.
+
+Workload (the clinical configuration): a seeded torso phantom on a 128x128x159 grid of
+0.776x0.776x0.795 mm voxels, isotope 68Ga, 128 far rays, support density 0.05, RDP beta 0.03 /
+gamma 20, Biggs-Andrews acceleration on.  The measured data are the truth blurred by the
+projector and Poisson-sampled at 5e7 counts.  One step = one complete 6-iteration MAP-EM
+correction (initialisation included) of that volume.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Arms:
+  ours       the CUDA engine through its C ABI (libprc_b200.so).  `value` is device-resident
+             (data already in HBM); `e2e` times prc_em_run_host from pinned host buffers, with
+             the host->device copy of the data and the device->host copy of the result inside.
+  reference  the CPU restatement of the reference's algorithm (oracle/, rays re-marched every
+             projection as prc.cu does), on all host cores, over a bounded sample of sources.
+
+Multi-GPU (torchrun): every rank corrects its own frame (replicas, no collective on the data
+path); value = iterations of all ranks / max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "EM iters/sec at 128x128x159 68Ga, learned vs plain projector, NRMSE<=1% vs FP64"
+ISOTOPE, RAYS, BETA, GAMMA, ITERS, SUPPORT_RHO, COUNTS = "68Ga", 128, 0.03, 20.0, 6, 0.05, 5e7
+L2_BYTES = 126 * 2**20
+
+
+def parse():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--grid", type=int, nargs=3, metavar=("NZ", "NY", "NX"), default=(159, 128, 128),
+                    help="override the torso grid (profiling of smaller cases)")
+    ap.add_argument("--iterations", type=int, default=ITERS)
+    ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-forms", action="store_true", help="skip the per-form comparison")
+    ap.add_argument("--ops", type=int, default=0,
+                    help="only run this many forward+adjoint pairs of the headline form (profiling)")
+    return ap.parse_args()
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+class ClockSampler:
+    """Samples SM clocks and throttle reasons with nvidia-smi while the timed region runs."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, f[5:9]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_workload(grid):
+    from prc_mlem_b200 import phantoms
+    rho, truth, spacing = phantoms.torso_phantom(seed=2, shape=tuple(grid))
+    return rho, truth, spacing
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.is_file():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(kernel_key: str):
+    """Per-launch DRAM bytes of the headline kernel from the committed ncu summary, if any."""
+    p = ROOT / "profiles" / "ncu_traffic.json"
+    if not p.is_file():
+        return None
+    try:
+        return json.loads(p.read_text()).get(kernel_key)
+    except (ValueError, OSError):
+        return None
+
+
+# ------------------------------------------------------------------------------- our arm
+def run_ours(args):
+    import torch
+    import prc_mlem_b200 as pm
+    from prc_mlem_b200 import phantoms
+
+    world, rank, local = dist_env()
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.cuda.current_device()
+
+    rho, truth, spacing = make_workload(args.grid)
+    t0 = time.perf_counter()
+    P = pm.Projector(ISOTOPE, rho, spacing, rays=RAYS, support_rho=SUPPORT_RHO, cache=pm.PRC_CACHE_FULL,
+                     precision=pm.PRC_PRECISION_FP32)
+    P.synchronize()
+    setup_s = time.perf_counter() - t0
+    stream = torch.cuda.ExternalStream(P.stream)
+    d_truth = torch.from_numpy(truth).cuda()
+    d_blur = torch.empty_like(d_truth)
+    P.forward(d_truth, d_blur)
+    P.synchronize()
+    g_host = phantoms.poisson_counts(d_blur.cpu().numpy(), COUNTS, seed=100 + rank)
+    d_g = torch.from_numpy(g_host).cuda()
+    d_out = torch.empty_like(d_g)
+    flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device="cuda")
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    def l2_flush():
+        with torch.cuda.stream(stream):
+            flush.fill_(1.0)
+
+    if args.ops:  # profiling mode: a few operator pairs only
+        for _ in range(args.ops):
+            P.forward(d_g, d_out)
+            P.adjoint(d_g, d_out)
+        P.synchronize()
+        print(json.dumps({"ops": args.ops, "n_active": P.n_active, "cache": P.cache_mode}))
+        return
+
+    for _ in range(args.warmup):
+        P.correct(d_g, d_out, args.iterations, BETA, GAMMA, True)
+    barrier()
+
+    clocks = ClockSampler(dev)
+    clocks.start()
+    times = []
+    barrier()
+    for _ in range(args.steps):
+        l2_flush()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        P.correct(d_g, d_out, args.iterations, BETA, GAMMA, True)
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    barrier()
+    clock_info = clocks.stop()
+    total_ms = sum(times)
+    if world > 1:
+        t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    iters_total = world * args.steps * args.iterations
+    value = iters_total / (total_ms / 1e3)
+
+    # end to end through the public API from pinned host buffers
+    g_pin = torch.from_numpy(g_host).pin_memory()
+    out_pin = torch.empty_like(g_pin).pin_memory()
+    e2e_ms = []
+    for i in range(args.warmup + args.steps):
+        l2_flush()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        rc = pm.lib().prc_em_run_host(P._h, g_pin.data_ptr(), out_pin.data_ptr(), args.iterations, BETA, GAMMA, 1)
+        e1.record(stream)
+        e1.synchronize()
+        if rc != 0:
+            raise RuntimeError(pm.lib().prc_last_error().decode())
+        if i >= args.warmup:
+            e2e_ms.append(e0.elapsed_time(e1))
+    e2e_total = sum(e2e_ms)
+    if world > 1:
+        t = torch.tensor([e2e_total], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_total = float(t.item())
+    e2e_value = iters_total / (e2e_total / 1e3)
+    corrected = out_pin.numpy().copy()
+
+    # dominant kernel: time single launches of the stored-field forward and adjoint
+    n_active = P.n_active
+    deposits = P.count_deposits()
+    launch_ms = {}
+    for name, fn in (("forward", P.forward), ("adjoint", P.adjoint)):
+        ts = []
+        for i in range(8):
+            l2_flush()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn(d_g, d_out)
+            e1.record(stream)
+            e1.synchronize()
+            if i >= 2:
+                ts.append(e0.elapsed_time(e1))
+        launch_ms[name] = statistics.mean(ts)
+    top = max(launch_ms, key=launch_ms.get)
+    alg_bytes = 12 * n_active + 8 * deposits  # 8 B per deposit (weight + target value), 12 B per source
+    peak, peak_kind = measured_peaks()
+    achieved = alg_bytes / (launch_ms[top] / 1e3) / 1e9
+    mode, far_entries = P.cache_mode
+    traffic = ncu_traffic(f"{top}_fp32_field")
+
+    forms = None
+    if not args.no_forms and rank == 0:
+        forms = compare_forms(args, rho, spacing, d_g, stream, l2_flush, value, corrected, P)
+
+    if world > 1:
+        torch.distributed.barrier()
+    if rank != 0:
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        return
+    cpu = None if args.no_cpu_baseline else cpu_baseline(rho, spacing, g_host, sample_seconds=15.0)
+    nz, ny, nx = args.grid
+    n_vox = nx * ny * nz
+    line = {
+        "metric": METRIC,
+        "value": round(value, 3),
+        "unit": "EM iters/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(total_ms / args.steps, 4),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded torso phantom, projector-blurred, Poisson 5e7 counts)",
+        "config": {
+            "workload": f"torso {nx}x{ny}x{nz} at 0.776x0.776x0.795 mm, {ISOTOPE}, rays {RAYS}, beta {BETA}, "
+                        f"gamma {GAMMA:g}, accel on, {args.iterations} MAP-EM iterations per step",
+            "form": "plain projector, fp32 weights: near cache + stored far-field coefficient field",
+            "n_active": n_active,
+            "deposits_per_projection": deposits,
+            "far_field_entries": far_entries,
+            "voxels_per_s": round(value * n_vox, 1),
+            "setup_s": round(setup_s, 4),
+            "l2": "flushed (256 MB write) before every timed step; the step also streams a "
+                  f"{P.device_bytes / 1e9:.1f} GB coefficient field, far above the 126 MB L2",
+            "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+        },
+        "e2e": {"value": round(e2e_value, 3), "unit": "EM iters/s",
+                "h2d_bytes_per_step": int(g_host.nbytes), "d2h_bytes_per_step": int(g_host.nbytes)},
+        "roofline": {"bound": "hbm", "kernel": f"project_kernel {top} (stored fp32 field)",
+                     "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
+                     "traffic": traffic, "launch_ms": {k: round(v, 4) for k, v in launch_ms.items()},
+                     "algorithmic_bytes": alg_bytes},
+        "gpu_launches": args.steps * (3 + 6 * args.iterations),
+        "clocks": clock_info,
+    }
+    if forms:
+        line["forms"] = forms
+    if cpu:
+        line["cpu_baseline"] = cpu
+    print(json.dumps(line))
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+def nrmse(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.sqrt(np.mean((a - b) ** 2)) / np.sqrt(np.mean(b ** 2)))
+
+
+def compare_forms(args, rho, spacing, d_g, stream, l2_flush, value_fp32, corrected_fp32, P_fp32):
+    """EM iters/s of the other projector forms on the same data, and their agreement."""
+    import torch
+    import prc_mlem_b200 as pm
+    out = {"fp32_field": {"iters_per_s": round(value_fp32, 3)}}
+    for name, cache, prec in (("bf16_field", pm.PRC_CACHE_FULL, pm.PRC_PRECISION_BF16),
+                              ("traced", pm.PRC_CACHE_NEAR, pm.PRC_PRECISION_FP32)):
+        Q = pm.Projector(ISOTOPE, rho, spacing, rays=RAYS, support_rho=SUPPORT_RHO, cache=cache, precision=prec)
+        s = torch.cuda.ExternalStream(Q.stream)
+        d_out = torch.empty_like(d_g)
+        steps = max(1, min(args.steps, 3))
+        Q.correct(d_g, d_out, args.iterations, BETA, GAMMA, True)
+        Q.synchronize()
+        ts = []
+        for _ in range(steps):
+            l2_flush()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(s)
+            Q.correct(d_g, d_out, args.iterations, BETA, GAMMA, True)
+            e1.record(s)
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        v = args.iterations * steps / (sum(ts) / 1e3)
+        img = d_out.cpu().numpy()
+        out[name] = {"iters_per_s": round(v, 3), "nrmse_vs_fp32_field": nrmse(img, corrected_fp32),
+                     "device_gb": round(Q.device_bytes / 1e9, 3)}
+        Q.close()
+    return out
+
+
+# ------------------------------------------------------------------------------- CPU baseline
+def cpu_baseline(rho, spacing, g, sample_seconds=15.0, seed=7):
+    """The oracle's float restatement of prc.cu (near block cached, far rays re-marched each
+    projection, as the reference does) on all host cores, over a random sample of sources.
+    iters/s = 1 / (forward + adjoint time scaled to all sources + one RDP update)."""
+    sys.path.insert(0, str(ROOT))
+    from oracle import oracle
+    threads = os.cpu_count() or 1
+    full = oracle.Problem(ISOTOPE, rho, spacing, rays=RAYS, support_rho=SUPPORT_RHO, precision=32, threads=threads)
+    n_active = full.n_active
+    rng = np.random.default_rng(seed)
+    frac = 0.002
+    while True:
+        sample = np.sort(rng.choice(n_active, size=max(64, int(n_active * frac)), replace=False))
+        sub = oracle.Problem(ISOTOPE, rho, spacing, rays=RAYS, support_rho=SUPPORT_RHO, precision=32,
+                             threads=threads)
+        sub.active = np.ascontiguousarray(full.active[sample])
+        sub.normalize()
+        x = g.astype(np.float32)
+        t0 = time.perf_counter()
+        sub.forward(x)
+        sub.adjoint(x)
+        dt = time.perf_counter() - t0
+        if dt >= 0.5 * sample_seconds or frac >= 1.0:
+            break
+        frac = min(1.0, frac * max(2.0, 0.6 * sample_seconds / max(dt, 1e-3)))
+    t0 = time.perf_counter()
+    full.update(g, g, BETA, GAMMA, 1e-6)
+    t_update = time.perf_counter() - t0
+    per_iter = dt * n_active / len(sample) + t_update
+    return {"value": round(1.0 / per_iter, 5), "unit": "EM iters/s", "cores": threads, "kind": "port",
+            "sample": f"{len(sample)} of {n_active} sources ({100 * len(sample) / n_active:.2f}%): one forward "
+                      f"and one adjoint projection ({dt:.1f} s), scaled to all sources, plus one full RDP "
+                      f"update ({t_update:.2f} s)"}
+
+
+def run_reference(args):
+    world, rank, _ = dist_env()
+    if rank != 0:
+        return
+    rho, truth, spacing = make_workload(args.grid)
+    g = phantoms_poisson_without_gpu(truth)
+    vals = []
+    info = None
+    for i in range(args.warmup + args.steps):
+        c = cpu_baseline(rho, spacing, g, sample_seconds=8.0, seed=11 + i)
+        if i >= args.warmup:
+            vals.append(c["value"])
+            info = c
+    value = statistics.mean(vals)
+    info["value"] = round(value, 5)
+    nz, ny, nx = args.grid
+    line = {
+        "metric": METRIC, "impl": "reference", "value": round(value, 5), "unit": "EM iters/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded torso phantom)",
+        "config": {"workload": f"torso {nx}x{ny}x{nz} at 0.776x0.776x0.795 mm, {ISOTOPE}, rays {RAYS}, "
+                               f"beta {BETA}, gamma {GAMMA:g}, accel on, {args.iterations} MAP-EM iterations"},
+        "cpu_baseline": info,
+        "e2e": {"value": round(value, 5), "unit": "EM iters/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def phantoms_poisson_without_gpu(truth):
+    """Measured data for the CPU arm: the truth Poisson-sampled at 5e7 counts (projection cost
+    does not depend on the activity values, only on the density)."""
+    from prc_mlem_b200 import phantoms
+    return phantoms.poisson_counts(truth, COUNTS, seed=100)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

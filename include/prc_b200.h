@@ -1,0 +1,163 @@
+/*
+ * prc_b200.h -- C ABI of the B200 positron-range-correction engine (libprc_b200.so).
+ *
+ * The reference (jlherraiz/PRC_MLEM) exposes its hot path only through the `prc` executable
+ * (prc.cu:564-722); inside it the operator seam is `class Projector` (prc.cu:403-450) and the
+ * MAP-EM loop of main() (prc.cu:659-711).  This header is that seam as a library: every entry
+ * point names the reference code it replaces.  All functions:
+ *   - are host-callable, return 0 (PRC_OK) or a PRC_ERR_* code and never exit the process;
+ *   - take plain pointers and sizes; "d_" pointers are device (CUDA global memory) arrays of
+ *     nx*ny*nz float32 values, X fastest (NumPy shape nz, ny, nx), "host" pointers are host
+ *     memory of the same layout;
+ *   - take `stream` as a cudaStream_t passed as void*; NULL selects the handle's own stream.
+ *     Work is enqueued asynchronously unless the function says it synchronises;
+ *   - are not thread-safe on one handle; distinct handles are independent.
+ * prc_last_error() returns a message for the most recent failure on the calling thread.
+ */
+#ifndef PRC_B200_H
+#define PRC_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    PRC_OK = 0,
+    PRC_ERR_ARGUMENT = 1,    /* invalid geometry or solver parameter ("Invalid ..." in prc.cu:540-546) */
+    PRC_ERR_ISOTOPE = 2,     /* unknown isotope name (prc.cu:570-576) */
+    PRC_ERR_NONFINITE = 3,   /* NaN/inf in density or activity (prc.cu:599-602) */
+    PRC_ERR_NO_ACTIVITY = 4, /* no activity in the support (prc.cu:619-622) */
+    PRC_ERR_CUDA = 5,        /* a CUDA runtime call failed (prc.cu:24-32 exits instead) */
+    PRC_ERR_MEMORY = 6,      /* device allocation failed */
+    PRC_ERR_STATE = 7,       /* call order violated (e.g. iterate before begin) */
+    PRC_ERR_LIMIT = 8        /* voxel count beyond the INT_MAX index limit (prc.cu:547-551) */
+};
+
+/* Precision of the projector's stored weights (near cache and far-field coefficient field). */
+enum {
+    PRC_PRECISION_FP32 = 0, /* float weights: the reference's numerics */
+    PRC_PRECISION_BF16 = 1  /* bfloat16 stored weights, float accumulation, FP64 global sums */
+};
+
+/* What the projector keeps in device memory between projections.  The reference caches the
+ * 5x5x5 near block (prc.cu:411-419) and retraces the far rays in every projection. */
+enum {
+    PRC_CACHE_NONE = 0, /* retrace near block and far rays every projection (--no-cache-near) */
+    PRC_CACHE_NEAR = 1, /* cache the near block, retrace far rays (the reference's default) */
+    PRC_CACHE_FULL = 2  /* also store the far-field weights, indexed by a shared ray template;
+                           falls back to PRC_CACHE_NEAR when they do not fit in half the free memory */
+};
+
+/* Volume geometry: positional arguments NX NY NZ DX DY DZ of prc.cu:515-516. */
+typedef struct prc_geometry {
+    int nx, ny, nz;
+    float dx, dy, dz; /* voxel size [mm] */
+} prc_geometry;
+
+/* Projector options: --rays, --support-rho, --air-cap-mm, --exact-range, --no-cache-near of
+ * prc.cu:452-459, plus the cache mode and the stored-weight precision. */
+typedef struct prc_options {
+    int rays;          /* even far-field rays per source, >= 2 (default 128) */
+    float support_rho; /* voxels with density >= support_rho hold activity (default 0.05) */
+    float air_cap_mm;  /* a positron that crossed this much sub-support path escaped (default 50) */
+    int exact_range;   /* 1: analytic survival instead of the 4097-entry table */
+    int cache;         /* PRC_CACHE_* (default PRC_CACHE_FULL) */
+    int precision;     /* PRC_PRECISION_* */
+} prc_options;
+
+typedef struct prc_handle prc_handle;
+
+/* Fills the reference defaults (prc.cu:456-458). */
+void prc_default_options(prc_options* opts);
+
+/* Water-equivalent 99.95 % range cutoff [mm] of an isotope, with the weight fix of
+ * prc.cu:577-584 and the bisection of prc.cu:83-91.  Host only, no CUDA call. */
+int prc_isotope_cutoff(const char* isotope, float* cutoff_mm);
+
+/* Number of supported isotopes and the name of the i-th one (usage text, prc.cu:482). */
+int prc_isotope_count(void);
+const char* prc_isotope_name(int i);
+
+/* Builds the projector for one density map (host array, g/cm3): clamps density to >= 1e-3,
+ * derives the support and active-source list (prc.cu:598-613), uploads them, and runs the
+ * normalisation pass that computes W_s and the near-field cache (Projector::Projector,
+ * prc.cu:405-422).  Synchronises.  Rejects non-finite density with PRC_ERR_NONFINITE. */
+int prc_create(const prc_geometry* geometry, const char* isotope, const prc_options* opts,
+               const float* density_host, prc_handle** out);
+
+/* Releases every device allocation of the handle (Projector::~Projector, prc.cu:423-427). */
+void prc_destroy(prc_handle* h);
+
+/* Tissue (active) voxel count and the water-equivalent cutoff of the handle. */
+int prc_active_count(const prc_handle* h, int64_t* n_active);
+int prc_cutoff(const prc_handle* h, float* cutoff_mm);
+/* Bytes of device memory the handle owns. */
+int prc_device_bytes(const prc_handle* h, int64_t* bytes);
+/* The cache mode in effect (PRC_CACHE_*, after any fall-back) and the far-field entries stored. */
+int prc_cache_mode(const prc_handle* h, int* mode, int64_t* far_entries);
+/* The handle's stream (a cudaStream_t) as void*. */
+void* prc_stream(const prc_handle* h);
+
+/* d_out = A d_in, overwritten on every voxel (Projector::forward, prc.cu:430-434). */
+int prc_forward(prc_handle* h, const float* d_in, float* d_out, void* stream);
+
+/* d_out[s] = (A^T d_in)[s] on tissue voxels; other voxels are left untouched
+ * (Projector::adjoint, prc.cu:436). */
+int prc_adjoint(prc_handle* h, const float* d_in, float* d_out, void* stream);
+
+/* Starts a MAP-EM run on measured data d_g: clamps it to >= 0 and zeroes it off the support,
+ * computes eps = 1e-6 * sum / n_active, floors the estimate at 1000 eps and rescales it to the
+ * measured counts (prc.cu:604-613, 666-672).  All on device; no host synchronisation. */
+int prc_em_begin(prc_handle* h, const float* d_g, void* stream);
+
+/* Runs n further MAP-EM iterations (extrapolate, forward, ratio, adjoint, RDP update, count
+ * rescale, Biggs-Andrews step length; prc.cu:675-700).  beta >= 0 is the RDP strength, gamma >= 0
+ * its edge parameter, accelerate = 0 gives plain MAP-EM (--no-accel).  The step length and the
+ * count rescale are computed on device in FP64, so no call synchronises.  The acceleration
+ * history carries over between calls, so k calls of n iterations equal one call of k*n. */
+int prc_em_iterate(prc_handle* h, int n, float beta, float gamma, int accelerate, void* stream);
+
+/* Copies the current estimate into d_out (all voxels). */
+int prc_em_estimate(prc_handle* h, float* d_out, void* stream);
+
+/* prc_em_begin + prc_em_iterate + prc_em_estimate.  iterations == 0 returns the supported,
+ * clamped input unchanged, as prc.cu:669 skips initialisation. */
+int prc_em_run(prc_handle* h, const float* d_g, float* d_out, int iterations, float beta, float gamma,
+               int accelerate, void* stream);
+
+/* The same correction from and to host memory: copies g_host in, runs, copies the estimate
+ * back into out_host.  Synchronises. */
+int prc_em_run_host(prc_handle* h, const float* g_host, float* out_host, int iterations, float beta,
+                    float gamma, int accelerate);
+
+/* prc_em_begin from host memory, and the current estimate copied back to host memory (the
+ * checkpoint path of --save-every, prc.cu:705-709).  Synchronise. */
+int prc_em_begin_host(prc_handle* h, const float* g_host);
+int prc_em_estimate_host(prc_handle* h, float* out_host);
+
+/* Host-memory forms of the two operators (the --mode forward / adjoint paths, prc.cu:648-657).
+ * prc_adjoint_host writes every voxel of out_host: A^T in on tissue, 0 elsewhere.  Synchronise. */
+int prc_forward_host(prc_handle* h, const float* in_host, float* out_host);
+int prc_adjoint_host(prc_handle* h, const float* in_host, float* out_host);
+
+/* FP64 sum of a device volume (device_sum, prc.cu:392-395).  Synchronises. */
+int prc_sum(prc_handle* h, const float* d_x, double* sum, void* stream);
+
+/* Number of (source, target) deposits of one projection, near and far (the V of the
+ * algorithmic-bytes accounting).  Synchronises. */
+int prc_count_deposits(prc_handle* h, int64_t* deposits);
+
+/* Waits for all work on the handle's stream. */
+int prc_synchronize(prc_handle* h);
+
+/* Message of the most recent failure on this thread ("" if none). */
+const char* prc_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PRC_B200_H */

@@ -1,0 +1,272 @@
+"""B200 positron-range correction: Python binding of the C ABI in include/prc_b200.h.
+
+The reference (jlherraiz/PRC_MLEM) has no library API; its operator seam is
+``class Projector`` (prc.cu:403-450) with ``forward``/``adjoint`` and the MAP-EM loop of
+``main`` (prc.cu:659-711).  :class:`Projector` mirrors that seam over ``libprc_b200.so``
+(ctypes, no torch types in the ABI).  Device arrays are passed as torch CUDA tensors or raw
+device pointers; torch only provides device memory and streams.
+
+There is no CPU fallback: if the shared library has not been built, loading it raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+import numpy as np
+
+PKG_DIR = Path(__file__).resolve().parent
+LIB_PATH = PKG_DIR / "lib" / "libprc_b200.so"
+CLI_PATH = PKG_DIR / "bin" / "prc"
+HEADER_PATH = PKG_DIR.parent / "include" / "prc_b200.h"
+
+PRC_OK = 0
+PRC_PRECISION_FP32 = 0
+PRC_PRECISION_BF16 = 1
+PRC_CACHE_NONE = 0
+PRC_CACHE_NEAR = 1
+PRC_CACHE_FULL = 2
+ISOTOPES = ("11C", "13N", "15O", "18F", "64Cu", "68Ga", "82Rb", "124I")
+
+
+class PrcError(RuntimeError):
+    """A C-ABI call returned a non-zero status; ``code`` is the PRC_ERR_* value."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__(f"prc error {code}: {message}")
+        self.code = code
+
+
+class Geometry(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+                ("dx", ctypes.c_float), ("dy", ctypes.c_float), ("dz", ctypes.c_float)]
+
+
+class Options(ctypes.Structure):
+    _fields_ = [("rays", ctypes.c_int), ("support_rho", ctypes.c_float), ("air_cap_mm", ctypes.c_float),
+                ("exact_range", ctypes.c_int), ("cache", ctypes.c_int), ("precision", ctypes.c_int)]
+
+
+_P = ctypes.c_void_p
+_F = ctypes.POINTER(ctypes.c_float)
+_SIGNATURES = {
+    "prc_default_options": (None, [ctypes.POINTER(Options)]),
+    "prc_isotope_cutoff": (ctypes.c_int, [ctypes.c_char_p, _F]),
+    "prc_isotope_count": (ctypes.c_int, []),
+    "prc_isotope_name": (ctypes.c_char_p, [ctypes.c_int]),
+    "prc_create": (ctypes.c_int, [ctypes.POINTER(Geometry), ctypes.c_char_p, ctypes.POINTER(Options), _P,
+                                  ctypes.POINTER(_P)]),
+    "prc_destroy": (None, [_P]),
+    "prc_active_count": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int64)]),
+    "prc_cutoff": (ctypes.c_int, [_P, _F]),
+    "prc_device_bytes": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int64)]),
+    "prc_cache_mode": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int64)]),
+    "prc_stream": (_P, [_P]),
+    "prc_forward": (ctypes.c_int, [_P, _P, _P, _P]),
+    "prc_adjoint": (ctypes.c_int, [_P, _P, _P, _P]),
+    "prc_em_begin": (ctypes.c_int, [_P, _P, _P]),
+    "prc_em_iterate": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_int, _P]),
+    "prc_em_estimate": (ctypes.c_int, [_P, _P, _P]),
+    "prc_em_run": (ctypes.c_int, [_P, _P, _P, ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_int, _P]),
+    "prc_em_run_host": (ctypes.c_int, [_P, _P, _P, ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_int]),
+    "prc_em_begin_host": (ctypes.c_int, [_P, _P]),
+    "prc_em_estimate_host": (ctypes.c_int, [_P, _P]),
+    "prc_forward_host": (ctypes.c_int, [_P, _P, _P]),
+    "prc_adjoint_host": (ctypes.c_int, [_P, _P, _P]),
+    "prc_sum": (ctypes.c_int, [_P, _P, ctypes.POINTER(ctypes.c_double), _P]),
+    "prc_count_deposits": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int64)]),
+    "prc_synchronize": (ctypes.c_int, [_P]),
+    "prc_last_error": (ctypes.c_char_p, []),
+}
+
+_lib_handle = None
+
+
+def lib() -> ctypes.CDLL:
+    """The loaded ``libprc_b200.so``; raises if it was not built (no fallback exists)."""
+    global _lib_handle
+    if _lib_handle is None:
+        if not LIB_PATH.is_file():
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `make -C {PKG_DIR / 'csrc'}` "
+                               "or __graft_entry__.build(); there is no CPU fallback")
+        handle = ctypes.CDLL(str(LIB_PATH))
+        for name, (res, args) in _SIGNATURES.items():
+            fn = getattr(handle, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib_handle = handle
+    return _lib_handle
+
+
+def _check(rc: int) -> None:
+    if rc != PRC_OK:
+        raise PrcError(rc, lib().prc_last_error().decode())
+
+
+def isotope_cutoff(isotope: str) -> float:
+    """99.95 % water-equivalent range cutoff [mm] (prc.cu:83-91); host only."""
+    c = ctypes.c_float()
+    _check(lib().prc_isotope_cutoff(isotope.encode(), ctypes.byref(c)))
+    return c.value
+
+
+def default_options() -> Options:
+    o = Options()
+    lib().prc_default_options(ctypes.byref(o))
+    return o
+
+
+def _ptr(x) -> int:
+    """Device pointer of a torch CUDA tensor (or an int pointer)."""
+    if isinstance(x, int):
+        return x
+    if not x.is_cuda or x.dtype.itemsize != 4 or not x.is_contiguous():
+        raise ValueError("expected a contiguous float32 CUDA tensor")
+    return x.data_ptr()
+
+
+def _host(a: np.ndarray) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+class Projector:
+    """Heterogeneous range-blur operator A for one density map (prc.cu:403-450).
+
+    ``density`` is a float array of shape (nz, ny, nx) in g/cm3; ``spacing`` is (dx, dy, dz)
+    in mm.  Construction runs the normalisation pass on the current CUDA device.
+    """
+
+    def __init__(self, isotope: str, density: np.ndarray, spacing, rays: int = 128, support_rho: float = 0.05,
+                 air_cap_mm: float = 50.0, exact_range: bool = False, cache: int = PRC_CACHE_FULL,
+                 precision: int = PRC_PRECISION_FP32):
+        density = _host(density)
+        if density.ndim != 3:
+            raise ValueError("density must be a (nz, ny, nx) array")
+        nz, ny, nx = density.shape
+        self.shape = density.shape
+        self.spacing = tuple(float(s) for s in spacing)
+        self.isotope = isotope
+        geo = Geometry(nx, ny, nz, *self.spacing)
+        opts = default_options()
+        opts.rays, opts.support_rho, opts.air_cap_mm = rays, support_rho, air_cap_mm
+        opts.exact_range, opts.cache, opts.precision = int(exact_range), int(cache), int(precision)
+        h = _P()
+        _check(lib().prc_create(ctypes.byref(geo), isotope.encode(), ctypes.byref(opts),
+                                density.ctypes.data, ctypes.byref(h)))
+        self._h = h
+        self.support = np.maximum(density, np.float32(1e-3)) >= np.float32(support_rho)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().prc_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self) -> int:
+        return self._h.value
+
+    @property
+    def n_active(self) -> int:
+        v = ctypes.c_int64()
+        _check(lib().prc_active_count(self._h, ctypes.byref(v)))
+        return v.value
+
+    @property
+    def cutoff(self) -> float:
+        v = ctypes.c_float()
+        _check(lib().prc_cutoff(self._h, ctypes.byref(v)))
+        return v.value
+
+    @property
+    def device_bytes(self) -> int:
+        v = ctypes.c_int64()
+        _check(lib().prc_device_bytes(self._h, ctypes.byref(v)))
+        return v.value
+
+    @property
+    def cache_mode(self) -> tuple[int, int]:
+        """(PRC_CACHE_* in effect, stored far-field entries)."""
+        m, e = ctypes.c_int(), ctypes.c_int64()
+        _check(lib().prc_cache_mode(self._h, ctypes.byref(m), ctypes.byref(e)))
+        return m.value, e.value
+
+    @property
+    def stream(self) -> int:
+        return lib().prc_stream(self._h) or 0
+
+    # device-memory operators -------------------------------------------------------------
+    def forward(self, d_in, d_out, stream=None) -> None:
+        """d_out = A d_in (overwritten) -- Projector::forward, prc.cu:430-434."""
+        _check(lib().prc_forward(self._h, _ptr(d_in), _ptr(d_out), stream))
+
+    def adjoint(self, d_in, d_out, stream=None) -> None:
+        """d_out[s] = (A^T d_in)[s] on tissue voxels -- Projector::adjoint, prc.cu:436."""
+        _check(lib().prc_adjoint(self._h, _ptr(d_in), _ptr(d_out), stream))
+
+    def em_begin(self, d_g, stream=None) -> None:
+        _check(lib().prc_em_begin(self._h, _ptr(d_g), stream))
+
+    def em_iterate(self, n: int, beta: float, gamma: float, accelerate: bool, stream=None) -> None:
+        _check(lib().prc_em_iterate(self._h, n, beta, gamma, int(accelerate), stream))
+
+    def em_estimate(self, d_out, stream=None) -> None:
+        _check(lib().prc_em_estimate(self._h, _ptr(d_out), stream))
+
+    def correct(self, d_g, d_out, iterations: int, beta: float = 0.2, gamma: float = 20.0,
+                accelerate: bool = True, stream=None) -> None:
+        """MAP-EM correction of d_g into d_out (prc.cu:659-711), fully on device."""
+        _check(lib().prc_em_run(self._h, _ptr(d_g), _ptr(d_out), iterations, beta, gamma, int(accelerate), stream))
+
+    def synchronize(self) -> None:
+        _check(lib().prc_synchronize(self._h))
+
+    def sum(self, d_x) -> float:
+        v = ctypes.c_double()
+        _check(lib().prc_sum(self._h, _ptr(d_x), ctypes.byref(v), None))
+        return v.value
+
+    def count_deposits(self) -> int:
+        v = ctypes.c_int64()
+        _check(lib().prc_count_deposits(self._h, ctypes.byref(v)))
+        return v.value
+
+    # host-memory forms -------------------------------------------------------------------
+    def forward_host(self, x: np.ndarray) -> np.ndarray:
+        x = _host(x)
+        out = np.empty_like(x)
+        _check(lib().prc_forward_host(self._h, x.ctypes.data, out.ctypes.data))
+        return out
+
+    def adjoint_host(self, y: np.ndarray) -> np.ndarray:
+        y = _host(y)
+        out = np.empty_like(y)
+        _check(lib().prc_adjoint_host(self._h, y.ctypes.data, out.ctypes.data))
+        return out
+
+    def correct_host(self, g: np.ndarray, iterations: int, beta: float = 0.2, gamma: float = 20.0,
+                     accelerate: bool = True) -> np.ndarray:
+        g = _host(g)
+        out = np.empty_like(g)
+        _check(lib().prc_em_run_host(self._h, g.ctypes.data, out.ctypes.data, iterations, beta, gamma,
+                                     int(accelerate)))
+        return out
+
+
+def header_symbols() -> list[str]:
+    """Every function the public header declares (used to check the library's exports)."""
+    import re
+    text = HEADER_PATH.read_text()
+    return sorted(set(re.findall(r"^\s*(?:[\w\s\*]+?)\b(prc_\w+)\s*\(", text, re.M)))

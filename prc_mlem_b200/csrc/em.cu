@@ -1,0 +1,278 @@
+// em.cu -- the MAP-EM image-update chain around the projector (prc.cu:269-332, 659-700).
+//
+// Every kernel is a grid-stride pass over the volume with a fixed grid of kReduceBlocks blocks.
+// The three scalars that the reference reads back to the host every iteration (the count sum
+// for the rescale and the two Biggs-Andrews inner products, prc.cu:689, 695-696) are reduced
+// on the device in FP64 instead: each block writes its partial, and the last block to finish
+// combines the partials in block order (deterministic) and writes the derived scalar (scale,
+// lambda) into EmScalars, where the next kernel reads it.  So an iteration enqueues without a
+// single host synchronisation.
+#include "engine.h"
+
+namespace prc {
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int kWarpsPerBlock = kEmThreads / 32;
+
+// Grid-wide FP64 reduction of NV values.  Must be reached by every thread of every block.
+// The last block calls fin(totals) from thread 0 and re-arms the counter for the next launch.
+template <int NV, class Fin>
+__device__ __forceinline__ void grid_reduce(double (&v)[NV], const Reduction& r, Fin&& fin) {
+    __shared__ double sh[NV][kWarpsPerBlock];
+    __shared__ bool am_last;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+    for (int k = 0; k < NV; ++k)
+        for (int off = 16; off > 0; off >>= 1) v[k] += __shfl_xor_sync(kFull, v[k], off);
+    if (lane == 0)
+#pragma unroll
+        for (int k = 0; k < NV; ++k) sh[k][warp] = v[k];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            double t = 0.0;
+            for (int w = 0; w < kWarpsPerBlock; ++w) t += sh[k][w];
+            r.partials[blockIdx.x * NV + k] = t;
+        }
+        __threadfence();
+        am_last = atomicAdd(r.counter, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!am_last) return;
+    __threadfence();
+    double acc[NV];
+#pragma unroll
+    for (int k = 0; k < NV; ++k) acc[k] = 0.0;
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x)
+#pragma unroll
+        for (int k = 0; k < NV; ++k) acc[k] += __ldcg(r.partials + b * NV + k);
+#pragma unroll
+    for (int k = 0; k < NV; ++k)
+        for (int off = 16; off > 0; off >>= 1) acc[k] += __shfl_xor_sync(kFull, acc[k], off);
+    __syncthreads();  // sh is reused below
+    if (lane == 0)
+#pragma unroll
+        for (int k = 0; k < NV; ++k) sh[k][warp] = acc[k];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double tot[NV];
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            tot[k] = 0.0;
+            for (int w = 0; w < kWarpsPerBlock; ++w) tot[k] += sh[k][w];
+        }
+        fin(tot);
+        *r.counter = 0u;
+    }
+}
+
+#define GRID_STRIDE(i, n) \
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < (n); i += (size_t)gridDim.x * blockDim.x)
+
+// g = support ? max(g_in, 0) : 0 (prc.cu:604-612); f = g; support_sum, eps and the floor.
+__global__ void begin_kernel(const float* __restrict__ g_in, const unsigned char* __restrict__ support,
+                             float* __restrict__ g, float* __restrict__ f, size_t n, int n_active, EmScalars* sc,
+                             Reduction r) {
+    double v[1] = {0.0};
+    GRID_STRIDE(i, n) {
+        const float x = support[i] ? fmaxf(g_in[i], 0.0f) : 0.0f;
+        g[i] = x;
+        f[i] = x;
+        v[0] += x;
+    }
+    grid_reduce<1>(v, r, [&](const double* t) {
+        sc->support_sum = t[0];
+        const float eps = (float)(1.0e-6 * t[0] / n_active);  // prc.cu:668
+        sc->eps = eps;
+        sc->floor = 1000.0f * eps;  // prc.cu:670
+        sc->lambda = 0.0f;
+        sc->scale = 1.0f;
+    });
+}
+
+// initialize_kernel (prc.cu:311-314) fused with the FP64 sum that sets the initial rescale.
+__global__ void floor_kernel(float* __restrict__ f, const unsigned char* __restrict__ support, size_t n,
+                             EmScalars* sc, Reduction r) {
+    const float fl = sc->floor;
+    double v[1] = {0.0};
+    GRID_STRIDE(i, n) {
+        float x = f[i];
+        if (support[i]) x = fmaxf(x, fl);
+        f[i] = x;
+        v[0] += x;
+    }
+    grid_reduce<1>(v, r, [&](const double* t) { sc->init_scale = (float)(sc->support_sum / t[0]); });
+}
+
+// finish_kernel without a residual (prc.cu:325-332, called at prc.cu:671).
+__global__ void init_scale_kernel(float* __restrict__ f, size_t n, const EmScalars* sc) {
+    const float scale = sc->init_scale;
+    GRID_STRIDE(i, n) f[i] = __fmul_rn(f[i], scale);
+}
+
+// Biggs-Andrews prediction, kept above f/2 (prc.cu:318-321).
+__global__ void extrapolate_kernel(const float* __restrict__ f, const float* __restrict__ prev,
+                                   float* __restrict__ y, size_t n, const EmScalars* sc) {
+    const float lambda = sc->lambda;
+    GRID_STRIDE(i, n) {
+        const float fi = f[i];
+        y[i] = fmaxf(fi + lambda * (fi - prev[i]), 0.5f * fi);
+    }
+}
+
+// EM ratio g / max(A y, eps) on the support (prc.cu:270-274).
+__global__ void ratio_kernel(const float* __restrict__ g, float* __restrict__ est,
+                             const unsigned char* __restrict__ support, size_t n, const EmScalars* sc) {
+    const float eps = sc->eps;
+    GRID_STRIDE(i, n) est[i] = support[i] ? g[i] / fmaxf(est[i], eps) : 0.0f;
+}
+
+__device__ __forceinline__ bool in_grid(const Grid& g, int i, int j, int k) {
+    return i >= 0 && i < g.nx && j >= 0 && j < g.ny && k >= 0 && k < g.nz;
+}
+
+// RDP MAP-EM update over the 26 tissue neighbours (prc.cu:279-309), with the FP64 sum of the
+// new estimate that drives the count rescale (prc.cu:688-691) when SUM is set.
+template <bool SUM>
+__global__ void update_kernel(const float* __restrict__ f, const float* __restrict__ back,
+                              const unsigned char* __restrict__ support, float* __restrict__ next, Grid g,
+                              float beta, float gamma, EmScalars* sc, Reduction r) {
+    const float eps = sc->eps;
+    const size_t n = (size_t)g.nx * g.ny * g.nz;
+    double v[1] = {0.0};
+    GRID_STRIDE(idx, n) {
+        float out;
+        if (!support[idx]) {
+            out = 0.0f;
+        } else {
+            const float fj = f[idx], f_em = fj * back[idx];
+            if (beta == 0.0f) {
+                out = fmaxf(f_em, 0.0f);
+            } else {
+                const int i = idx % g.nx, j = (idx / g.nx) % g.ny, k = idx / ((size_t)g.nx * g.ny);
+                float grad = 0.0f, curv = 0.0f;
+                for (int dz = -1; dz <= 1; ++dz)
+                    for (int dy = -1; dy <= 1; ++dy)
+                        for (int dx = -1; dx <= 1; ++dx) {
+                            if (!(dx | dy | dz) || !in_grid(g, i + dx, j + dy, k + dz)) continue;
+                            const size_t nb = idx + ((long)dz * g.ny + dy) * g.nx + dx;
+                            if (!support[nb]) continue;
+                            const float mx = dx * g.sx, my = dy * g.sy, mz = dz * g.sz;
+                            const float w = fminf(g.sx, fminf(g.sy, g.sz)) * rsqrtf(mx * mx + my * my + mz * mz);
+                            const float fk = f[nb], d = fj - fk, ad = fabsf(d);
+                            const float D = fj + fk + gamma * ad + eps, invD = 1.0f / D;
+                            grad += w * d * (fj + 3.0f * fk + gamma * ad + 2.0f * eps) * invD * invD;
+                            const float half_quad = (2.0f * (fj + fk + eps) + gamma * ad) * invD * invD;
+                            const float hess = 2.0f * (2.0f * fk + eps) * (2.0f * fk + eps) * invD * invD * invD;
+                            curv += 2.0f * w * fmaxf(half_quad, hess);
+                        }
+                // positive root of a x^2 + B x - f_em = 0, stable form for each sign of B
+                const float a = beta * curv, B = 1.0f + beta * (grad - curv * fj);
+                const float root = sqrtf(B * B + 4.0f * a * f_em);
+                out = B >= 0.0f ? (f_em > 0.0f ? 2.0f * f_em / (B + root) : 0.0f) : (root - B) / (2.0f * a);
+            }
+        }
+        next[idx] = out;
+        if (SUM) v[0] += out;
+    }
+    if (SUM)
+        grid_reduce<1>(v, r, [&](const double* t) {
+            sc->sum = t[0];
+            sc->scale = t[0] > 0.0 ? (float)(sc->support_sum / t[0]) : 1.0f;
+        });
+}
+
+// Count rescale and, when accelerating, the step h = next - y and the two FP64 inner products
+// that give lambda = clamp(<h, h_prev> / <h_prev, h_prev>, 0, 1) (prc.cu:325-332, 693-696).
+template <bool RESIDUAL>
+__global__ void finish_kernel(float* __restrict__ next, float* __restrict__ residual,
+                              const float* __restrict__ h_prev, size_t n, bool use_scale, EmScalars* sc,
+                              Reduction r) {
+    const float scale = use_scale ? sc->scale : 1.0f;
+    double v[2] = {0.0, 0.0};
+    GRID_STRIDE(i, n) {
+        const float value = __fmul_rn(next[i], scale);
+        next[i] = value;
+        if (RESIDUAL) {
+            const float h = value - residual[i];
+            residual[i] = h;
+            const double hp = h_prev[i];
+            v[0] += (double)h * hp;
+            v[1] += hp * hp;
+        }
+    }
+    if (RESIDUAL)
+        grid_reduce<2>(v, r, [&](const double* t) {
+            const double hh = t[1];
+            sc->lambda = hh > 0.0 ? (float)fmin(1.0, fmax(0.0, t[0] / hh)) : 0.0f;
+        });
+}
+
+__global__ void sum_kernel(const float* __restrict__ x, size_t n, EmScalars* sc, Reduction r) {
+    double v[1] = {0.0};
+    GRID_STRIDE(i, n) v[0] += x[i];
+    grid_reduce<1>(v, r, [&](const double* t) { sc->sum = t[0]; });
+}
+
+__global__ void mask_copy_kernel(const float* __restrict__ src, float* __restrict__ dst,
+                                 const unsigned char* __restrict__ support, size_t n, float fill) {
+    GRID_STRIDE(i, n) dst[i] = support[i] ? src[i] : fill;
+}
+
+}  // namespace
+
+cudaError_t em_begin(const EmVolumes& v, const float* g_in, float* g, float* f, int n_active, bool initialize,
+                     cudaStream_t s) {
+    begin_kernel<<<kReduceBlocks, kEmThreads, 0, s>>>(g_in, v.support, g, f, v.n, n_active, v.scalars, v.red);
+    if (initialize) {
+        floor_kernel<<<kReduceBlocks, kEmThreads, 0, s>>>(f, v.support, v.n, v.scalars, v.red);
+        init_scale_kernel<<<kReduceBlocks, kEmThreads, 0, s>>>(f, v.n, v.scalars);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t em_extrapolate(const EmVolumes& v, const float* f, const float* prev, float* y, cudaStream_t s) {
+    extrapolate_kernel<<<kReduceBlocks, kEmThreads, 0, s>>>(f, prev, y, v.n, v.scalars);
+    return cudaGetLastError();
+}
+
+cudaError_t em_ratio(const EmVolumes& v, const float* g, float* est, cudaStream_t s) {
+    ratio_kernel<<<kReduceBlocks, kEmThreads, 0, s>>>(g, est, v.support, v.n, v.scalars);
+    return cudaGetLastError();
+}
+
+cudaError_t em_update(const EmVolumes& v, const Grid& grid, const float* start, const float* back, float* next,
+                      float beta, float gamma, cudaStream_t s) {
+    if (beta > 0.0f)
+        update_kernel<true><<<kReduceBlocks, kEmThreads, 0, s>>>(start, back, v.support, next, grid, beta, gamma,
+                                                                 v.scalars, v.red);
+    else
+        update_kernel<false><<<kReduceBlocks, kEmThreads, 0, s>>>(start, back, v.support, next, grid, beta, gamma,
+                                                                  v.scalars, v.red);
+    return cudaGetLastError();
+}
+
+cudaError_t em_finish(const EmVolumes& v, float* next, float* residual, const float* h_prev, bool use_scale,
+                      cudaStream_t s) {
+    if (residual)
+        finish_kernel<true><<<kReduceBlocks, kEmThreads, 0, s>>>(next, residual, h_prev, v.n, use_scale, v.scalars,
+                                                                 v.red);
+    else
+        finish_kernel<false><<<kReduceBlocks, kEmThreads, 0, s>>>(next, nullptr, nullptr, v.n, use_scale, v.scalars,
+                                                                  v.red);
+    return cudaGetLastError();
+}
+
+cudaError_t em_sum(const EmVolumes& v, const float* x, cudaStream_t s) {
+    sum_kernel<<<kReduceBlocks, kEmThreads, 0, s>>>(x, v.n, v.scalars, v.red);
+    return cudaGetLastError();
+}
+
+cudaError_t em_mask_copy(const EmVolumes& v, const float* src, float* dst, float fill, cudaStream_t s) {
+    mask_copy_kernel<<<kReduceBlocks, kEmThreads, 0, s>>>(src, dst, v.support, v.n, fill);
+    return cudaGetLastError();
+}
+
+}  // namespace prc

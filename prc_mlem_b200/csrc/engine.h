@@ -1,0 +1,131 @@
+// engine.h -- internal interface between the C ABI (prc_abi.cu) and the kernel files
+// (projector.cu, em.cu).  Not installed; the public surface is include/prc_b200.h.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+#include <cstdint>
+
+#include "range_model.h"
+
+namespace prc {
+
+// Uniform DDA state of one ray, derived once per run from ray(k, n) exactly as prc.cu:138-142
+// derives it at the start of every trace: distances [mm] to the first x/y/z voxel faces, the
+// distances between consecutive faces and the step signs.  Every source traces a ray k from
+// the same sub-voxel offset along the same direction, so this record is shared by all sources.
+struct RayStep {
+    float tx, ty, tz;
+    float dtx, dty, dtz;
+    int di, dj, dk;
+    int pad;
+};
+
+// Everything a projector kernel needs to know about one volume.
+struct ProjParams {
+    Grid g;
+    int nxy;                 // nx * ny
+    int n_active;            // tissue voxels (sources)
+    int n_rays;              // far-field rays per source
+    const float* rho;        // clamped density, nx*ny*nz
+    const int* active;       // linear voxel index of each source, increasing
+    const RayStep* far;      // n_rays records
+    const RayStep* near;     // kNearRays records
+    const float* table;      // kRangeBins + 1 survival samples, or nullptr for analytic
+    float table_scale;       // bins per mm
+    int n_branch;            // analytic model (used when table == nullptr)
+    Branch br[3];
+    // Far-field layout (used by the stored field; null until the layout pass has run).
+    const int* tmpl;                 // [n_rays][tmpl_len]: linear target offset of the m-th step
+                                     // of ray r after it left the near block (same for every source)
+    int tmpl_len;                    // nx + ny + nz: no ray takes more steps inside the image
+    const unsigned short* len;       // [n_groups][n_rays]: stored steps of ray r in group G
+    const long long* group_base;     // [n_groups]: element offset of group G's far field
+};
+
+// Stored far-field weights ("coefficient field"): for group G, ray r, post-block step m and
+// lane l, entry group_base[G] + (sum_{r'<r} len[G][r'] + m) * 32 + l.  Target voxels come from
+// the ray template, so no index is stored; forward and adjoint read the same field.
+struct FarField {
+    float* f32 = nullptr;
+    __nv_bfloat16* b16 = nullptr;
+    __host__ __device__ bool on() const { return f32 || b16; }
+};
+
+// Near-field weight cache, group-interleaved: entry (source src, block offset q) lives at
+// ((src / 32) * 125 + q) * 32 + src % 32, so the 32 sources of one warp read 128 contiguous
+// bytes per offset.  Exactly one of f32 / b16 is non-null when the cache is on.
+struct NearCache {
+    float* f32 = nullptr;
+    __nv_bfloat16* b16 = nullptr;
+    __host__ __device__ bool on() const { return f32 || b16; }
+};
+
+// Norm: W and the caches.  Forward / Adjoint: the operators.  Count: deposits per projection.
+// Layout: per group and ray, the number of post-block steps up to the last deposit of any lane
+// (written to len; the per-group totals to a.group_total).
+enum class Op : int { Norm = 0, Forward = 1, Adjoint = 2, Count = 3, Layout = 4 };
+
+// Per-launch operands.  Norm writes W (and the cache when it is on); Forward scatters
+// f_s / W_s * w_st into out (which must be zeroed first); Adjoint writes out[s] on tissue;
+// Count adds the deposit count to *count.
+struct OpArgs {
+    const float* in = nullptr;   // f (Forward) or the gathered image (Adjoint)
+    float* out = nullptr;
+    float* W = nullptr;
+    NearCache near;
+    FarField far;
+    unsigned long long* count = nullptr;
+    unsigned short* len = nullptr;         // Layout output
+    long long* group_total = nullptr;      // Layout output: entries per group (sum of len * 32)
+};
+
+// projector.cu
+cudaError_t setup_rays(const Grid& g, int n_rays, RayStep* d_far, RayStep* d_near, cudaStream_t s);
+// trace_near: retrace the near block (no cache).  Forward / Adjoint / Count read the stored far
+// field when a.far is on, and march the far rays otherwise.
+cudaError_t project(Op op, const ProjParams& p, const OpArgs& a, bool trace_near, cudaStream_t s);
+// Fills the ray template p.tmpl ([n_rays][tmpl_len] ints).
+cudaError_t build_template(const ProjParams& p, int* tmpl, cudaStream_t s);
+
+// em.cu ---------------------------------------------------------------------------------------
+// Device scalars of one MAP-EM run; all FP64 where the reference accumulates in FP64.
+struct EmScalars {
+    double support_sum;  // measured counts on the support
+    double sum;          // last FP64 volume sum
+    float eps;           // 1e-6 * support_sum / n_active (prc.cu:668)
+    float floor;         // 1000 * eps (prc.cu:670)
+    float lambda;        // Biggs-Andrews step length for the next prediction
+    float scale;         // count rescale of the current iteration
+    float init_scale;    // count rescale of the initial estimate
+    int pad;
+};
+
+// Grid-wide FP64 reduction scratch: block partials, and a counter the last block resets.
+struct Reduction {
+    double* partials;       // kReduceBlocks * 4
+    unsigned int* counter;  // one
+};
+constexpr int kReduceBlocks = 592;  // 148 SMs x 4
+constexpr int kEmThreads = 256;
+
+struct EmVolumes {
+    size_t n;            // voxels
+    const unsigned char* support;
+    EmScalars* scalars;
+    Reduction red;
+};
+
+// g = support ? max(g_in, 0) : 0 and f = g; with `initialize`, also the floor and count rescale.
+cudaError_t em_begin(const EmVolumes& v, const float* g_in, float* g, float* f, int n_active, bool initialize,
+                     cudaStream_t s);
+cudaError_t em_extrapolate(const EmVolumes& v, const float* f, const float* prev, float* y, cudaStream_t s);
+cudaError_t em_ratio(const EmVolumes& v, const float* g, float* est, cudaStream_t s);
+cudaError_t em_update(const EmVolumes& v, const Grid& grid, const float* start, const float* back, float* next,
+                      float beta, float gamma, cudaStream_t s);
+cudaError_t em_finish(const EmVolumes& v, float* next, float* residual, const float* h_prev, bool use_scale,
+                      cudaStream_t s);
+cudaError_t em_sum(const EmVolumes& v, const float* x, cudaStream_t s);
+cudaError_t em_mask_copy(const EmVolumes& v, const float* src, float* dst, float fill, cudaStream_t s);
+
+}  // namespace prc

@@ -1,0 +1,513 @@
+// prc_abi.cu -- the C ABI of include/prc_b200.h: one handle per density map, owning every
+// device allocation, its stream, the projector state (Projector, prc.cu:403-450) and the
+// MAP-EM state of main() (prc.cu:659-711).
+#include "../../include/prc_b200.h"
+#include "engine.h"
+
+#include <climits>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <utility>
+#include <vector>
+
+using namespace prc;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+    g_last_error = msg;
+    return code;
+}
+
+#define PRC_CUDA(call)                                                                              \
+    do {                                                                                            \
+        const cudaError_t err_ = (call);                                                            \
+        if (err_ != cudaSuccess)                                                                    \
+            return fail(err_ == cudaErrorMemoryAllocation ? PRC_ERR_MEMORY : PRC_ERR_CUDA,          \
+                        std::string("CUDA error '") + cudaGetErrorString(err_) + "' in " + #call); \
+    } while (0)
+
+}  // namespace
+
+struct prc_handle {
+    Grid g{};
+    RangeModel model;
+    prc_options opts{};
+    size_t n = 0;  // voxels
+    int n_active = 0;
+    int n_groups = 0;
+    cudaStream_t stream = nullptr;
+    int device = 0;
+
+    // projector state
+    float* rho = nullptr;
+    unsigned char* support = nullptr;
+    int* active = nullptr;
+    float* W = nullptr;
+    float* table = nullptr;
+    RayStep* far = nullptr;
+    RayStep* near_rays = nullptr;
+    NearCache cache;
+    FarField far_field;
+    int* tmpl = nullptr;
+    unsigned short* len = nullptr;
+    long long* group_base = nullptr;
+    long long* group_total = nullptr;
+    int64_t far_entries = 0;
+    int cache_mode = PRC_CACHE_NONE;
+    bool trace_near = false;
+    ProjParams params{};
+    unsigned long long* counter = nullptr;
+    float* scratch = nullptr;      // input volume of the host-memory forms
+    float* scratch_out = nullptr;  // output volume of the host-memory operator forms
+
+    // MAP-EM state
+    float* g_em = nullptr;
+    float* vol[5] = {};  // f, prev, y, h_prev, est (rotated by pointer swaps)
+    float *f = nullptr, *prev = nullptr, *y = nullptr, *h_prev = nullptr, *est = nullptr;
+    EmScalars* scalars = nullptr;
+    Reduction red{};
+    bool em_started = false;
+    int64_t bytes = 0;
+
+    std::vector<void*> allocations;
+
+    template <class T>
+    cudaError_t alloc(T** p, size_t count) {
+        void* v = nullptr;
+        const cudaError_t e = cudaMalloc(&v, count * sizeof(T) > 0 ? count * sizeof(T) : 1);
+        if (e != cudaSuccess) return e;
+        allocations.push_back(v);
+        bytes += (int64_t)(count * sizeof(T));
+        *p = static_cast<T*>(v);
+        return cudaMemsetAsync(v, 0, count * sizeof(T), stream);
+    }
+
+    cudaStream_t pick(void* s) const { return s ? static_cast<cudaStream_t>(s) : stream; }
+
+    EmVolumes em_volumes() const { return EmVolumes{n, support, scalars, red}; }
+
+    OpArgs op_args() const {
+        OpArgs a;
+        a.W = W;
+        a.near = cache;
+        a.far = far_field;
+        return a;
+    }
+};
+
+extern "C" {
+
+void prc_default_options(prc_options* o) {
+    if (!o) return;
+    o->rays = 128;
+    o->support_rho = 0.05f;
+    o->air_cap_mm = 50.0f;
+    o->exact_range = 0;
+    o->cache = PRC_CACHE_FULL;
+    o->precision = PRC_PRECISION_FP32;
+}
+
+int prc_isotope_count(void) { return kNumIsotopes; }
+
+const char* prc_isotope_name(int i) { return i >= 0 && i < kNumIsotopes ? kIsotopeTable[i].name : nullptr; }
+
+int prc_isotope_cutoff(const char* isotope, float* cutoff_mm) {
+    RangeModel m;
+    if (!isotope || !m.resolve(isotope)) return fail(PRC_ERR_ISOTOPE, std::string("Unknown isotope ") + (isotope ? isotope : "(null)"));
+    if (cutoff_mm) *cutoff_mm = m.cutoff;
+    return PRC_OK;
+}
+
+const char* prc_last_error(void) { return g_last_error.c_str(); }
+
+void prc_destroy(prc_handle* h) {
+    if (!h) return;
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    for (void* p : h->allocations) cudaFree(p);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+}
+
+static int create_impl(prc_handle* h, const float* density_host) {
+    const Grid& g = h->g;
+    // Host-side clamp, support and source list (prc.cu:598-613).
+    std::vector<float> rho(h->n);
+    std::vector<unsigned char> support(h->n);
+    std::vector<int> active;
+    active.reserve(h->n / 2);
+    for (size_t i = 0; i < h->n; ++i) {
+        const float r = density_host[i];
+        if (!std::isfinite(r)) {
+            char msg[96];
+            snprintf(msg, sizeof(msg), "Non-finite density at voxel %zu", i);
+            return fail(PRC_ERR_NONFINITE, msg);
+        }
+        rho[i] = r > kMinDensity ? r : kMinDensity;
+        support[i] = rho[i] >= g.support_rho;
+        if (support[i]) active.push_back((int)i);
+    }
+    h->n_active = (int)active.size();
+    h->n_groups = (h->n_active + kLanes - 1) / kLanes;
+
+    PRC_CUDA(cudaGetDevice(&h->device));
+    PRC_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    PRC_CUDA(h->alloc(&h->rho, h->n));
+    PRC_CUDA(h->alloc(&h->support, h->n));
+    PRC_CUDA(h->alloc(&h->active, h->n_active));
+    PRC_CUDA(h->alloc(&h->W, h->n_active));
+    PRC_CUDA(h->alloc(&h->far, h->opts.rays));
+    PRC_CUDA(h->alloc(&h->near_rays, kNearRays));
+    PRC_CUDA(h->alloc(&h->counter, 1));
+    PRC_CUDA(cudaMemcpyAsync(h->rho, rho.data(), h->n * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+    PRC_CUDA(cudaMemcpyAsync(h->support, support.data(), h->n, cudaMemcpyHostToDevice, h->stream));
+    if (h->n_active)
+        PRC_CUDA(cudaMemcpyAsync(h->active, active.data(), active.size() * sizeof(int), cudaMemcpyHostToDevice,
+                                 h->stream));
+
+    ProjParams& p = h->params;
+    p.g = g;
+    p.nxy = g.nx * g.ny;
+    p.n_active = h->n_active;
+    p.n_rays = h->opts.rays;
+    p.rho = h->rho;
+    p.active = h->active;
+    p.far = h->far;
+    p.near = h->near_rays;
+    p.n_branch = h->model.n;
+    for (int b = 0; b < 3; ++b) p.br[b] = h->model.br[b];
+    if (!h->opts.exact_range) {  // prc.cu:625-633
+        const std::vector<float> table = h->model.table();
+        PRC_CUDA(h->alloc(&h->table, table.size()));
+        PRC_CUDA(cudaMemcpyAsync(h->table, table.data(), table.size() * sizeof(float), cudaMemcpyHostToDevice,
+                                 h->stream));
+        p.table = h->table;
+        p.table_scale = h->model.table_scale();
+    }
+    PRC_CUDA(setup_rays(g, h->opts.rays, h->far, h->near_rays, h->stream));
+
+    const bool bf16 = h->opts.precision == PRC_PRECISION_BF16;
+    const size_t elem = bf16 ? 2 : 4;
+    // Near cache when it fits in a quarter of free memory (prc.cu:411-419).
+    h->trace_near = true;
+    if (h->opts.cache >= PRC_CACHE_NEAR && h->n_groups) {
+        size_t free_b = 0, total_b = 0;
+        PRC_CUDA(cudaMemGetInfo(&free_b, &total_b));
+        const size_t entries = (size_t)h->n_groups * kNear * kLanes;
+        if (entries * elem <= free_b / 4) {
+            cudaError_t e = bf16 ? h->alloc(&h->cache.b16, entries) : h->alloc(&h->cache.f32, entries);
+            if (e == cudaSuccess) h->trace_near = false, h->cache_mode = PRC_CACHE_NEAR;
+            else cudaGetLastError();  // optional: fall back to retracing
+        }
+    }
+    // Far-field coefficient field: size it with a layout pass, then let the Norm pass fill it.
+    // Template rows hold every step a ray can take inside the image plus the padding of the
+    // last packed group of 4, rounded to whole int4s.
+    const long long tmpl_len = ((long long)g.nx + g.ny + g.nz + 3 + 3) / 4 * 4;
+    if (h->opts.cache == PRC_CACHE_FULL && !h->trace_near && tmpl_len < 65535) {
+        p.tmpl_len = (int)tmpl_len;
+        PRC_CUDA(h->alloc(&h->tmpl, (size_t)h->opts.rays * tmpl_len));
+        PRC_CUDA(h->alloc(&h->len, (size_t)h->n_groups * h->opts.rays));
+        PRC_CUDA(h->alloc(&h->group_total, h->n_groups));
+        PRC_CUDA(h->alloc(&h->group_base, h->n_groups));
+        p.tmpl = h->tmpl;
+        PRC_CUDA(build_template(p, h->tmpl, h->stream));
+        OpArgs la = h->op_args();
+        la.len = h->len;
+        la.group_total = h->group_total;
+        PRC_CUDA(project(Op::Layout, p, la, true, h->stream));
+        std::vector<long long> totals(h->n_groups);
+        PRC_CUDA(cudaMemcpyAsync(totals.data(), h->group_total, totals.size() * sizeof(long long),
+                                 cudaMemcpyDeviceToHost, h->stream));
+        PRC_CUDA(cudaStreamSynchronize(h->stream));
+        long long run = 0;
+        for (long long& t : totals) {
+            const long long v = t;
+            t = run;
+            run += v;
+        }
+        size_t free_b = 0, total_b = 0;
+        PRC_CUDA(cudaMemGetInfo(&free_b, &total_b));
+        if ((size_t)run * elem <= free_b / 2) {
+            cudaError_t e = bf16 ? h->alloc(&h->far_field.b16, (size_t)run) : h->alloc(&h->far_field.f32, (size_t)run);
+            if (e == cudaSuccess) {
+                PRC_CUDA(cudaMemcpyAsync(h->group_base, totals.data(), totals.size() * sizeof(long long),
+                                         cudaMemcpyHostToDevice, h->stream));
+                p.len = h->len;
+                p.group_base = h->group_base;
+                h->far_entries = run;
+                h->cache_mode = PRC_CACHE_FULL;
+            } else {
+                cudaGetLastError();  // optional: far rays stay traced
+            }
+        }
+    }
+    OpArgs a = h->op_args();
+    PRC_CUDA(project(Op::Norm, p, a, true, h->stream));
+    PRC_CUDA(cudaStreamSynchronize(h->stream));
+    return PRC_OK;
+}
+
+int prc_create(const prc_geometry* geo, const char* isotope, const prc_options* opts_in, const float* density_host,
+               prc_handle** out) {
+    if (!out) return fail(PRC_ERR_ARGUMENT, "Invalid argument: null handle pointer");
+    *out = nullptr;
+    if (!geo || !density_host) return fail(PRC_ERR_ARGUMENT, "Invalid argument: null geometry or density");
+    prc_options o;
+    prc_default_options(&o);
+    if (opts_in) o = *opts_in;
+    // prc.cu:540-551
+    if (geo->nx <= 0 || geo->ny <= 0 || geo->nz <= 0 || !(geo->dx > 0) || !(geo->dy > 0) || !(geo->dz > 0) ||
+        !std::isfinite(geo->dx) || !std::isfinite(geo->dy) || !std::isfinite(geo->dz) || o.rays < 2 ||
+        (o.rays & 1) || o.rays > INT_MAX - 31 || !(o.support_rho >= 0) || !(o.air_cap_mm > 0) ||
+        !std::isfinite(o.support_rho) || !std::isfinite(o.air_cap_mm) ||
+        (o.precision != PRC_PRECISION_FP32 && o.precision != PRC_PRECISION_BF16) || o.cache < PRC_CACHE_NONE ||
+        o.cache > PRC_CACHE_FULL)
+        return fail(PRC_ERR_ARGUMENT, "Invalid geometry or solver parameters");
+    if (geo->nx > INT_MAX / geo->ny || geo->nx * geo->ny > INT_MAX / geo->nz)
+        return fail(PRC_ERR_LIMIT, "Volume exceeds the INT_MAX voxel index limit");
+    prc_handle* h = new prc_handle();
+    if (!h->model.resolve(isotope ? isotope : "")) {
+        delete h;
+        return fail(PRC_ERR_ISOTOPE, std::string("Unknown isotope ") + (isotope ? isotope : "(null)"));
+    }
+    h->opts = o;
+    h->g = Grid{geo->nx, geo->ny, geo->nz, geo->dx, geo->dy, geo->dz, h->model.cutoff, o.support_rho, o.air_cap_mm};
+    h->n = (size_t)geo->nx * geo->ny * geo->nz;
+    const int rc = create_impl(h, density_host);
+    if (rc != PRC_OK) {
+        const std::string msg = g_last_error;
+        prc_destroy(h);
+        g_last_error = msg;
+        return rc;
+    }
+    *out = h;
+    return PRC_OK;
+}
+
+int prc_cache_mode(const prc_handle* h, int* mode, int64_t* far_entries) {
+    if (!h) return fail(PRC_ERR_ARGUMENT, "Invalid argument");
+    if (mode) *mode = h->cache_mode;
+    if (far_entries) *far_entries = h->far_entries;
+    return PRC_OK;
+}
+
+int prc_active_count(const prc_handle* h, int64_t* n) {
+    if (!h || !n) return fail(PRC_ERR_ARGUMENT, "Invalid argument");
+    *n = h->n_active;
+    return PRC_OK;
+}
+
+int prc_cutoff(const prc_handle* h, float* c) {
+    if (!h || !c) return fail(PRC_ERR_ARGUMENT, "Invalid argument");
+    *c = h->g.cutoff;
+    return PRC_OK;
+}
+
+int prc_device_bytes(const prc_handle* h, int64_t* b) {
+    if (!h || !b) return fail(PRC_ERR_ARGUMENT, "Invalid argument");
+    *b = h->bytes;
+    return PRC_OK;
+}
+
+void* prc_stream(const prc_handle* h) { return h ? (void*)h->stream : nullptr; }
+
+int prc_forward(prc_handle* h, const float* d_in, float* d_out, void* stream) {
+    if (!h || !d_in || !d_out) return fail(PRC_ERR_ARGUMENT, "Invalid argument");
+    const cudaStream_t s = h->pick(stream);
+    PRC_CUDA(cudaMemsetAsync(d_out, 0, h->n * sizeof(float), s));
+    OpArgs a = h->op_args();
+    a.in = d_in;
+    a.out = d_out;
+    PRC_CUDA(project(Op::Forward, h->params, a, h->trace_near, s));
+    return PRC_OK;
+}
+
+int prc_adjoint(prc_handle* h, const float* d_in, float* d_out, void* stream) {
+    if (!h || !d_in || !d_out) return fail(PRC_ERR_ARGUMENT, "Invalid argument");
+    OpArgs a = h->op_args();
+    a.in = d_in;
+    a.out = d_out;
+    PRC_CUDA(project(Op::Adjoint, h->params, a, h->trace_near, h->pick(stream)));
+    return PRC_OK;
+}
+
+static int ensure_em(prc_handle* h) {
+    if (h->g_em) return PRC_OK;
+    PRC_CUDA(h->alloc(&h->g_em, h->n));
+    for (float*& v : h->vol) PRC_CUDA(h->alloc(&v, h->n));
+    PRC_CUDA(h->alloc(&h->scalars, 1));
+    PRC_CUDA(h->alloc(&h->red.partials, (size_t)kReduceBlocks * 4));
+    PRC_CUDA(h->alloc(&h->red.counter, 1));
+    return PRC_OK;
+}
+
+static int em_begin_impl(prc_handle* h, const float* d_g, bool initialize, cudaStream_t s) {
+    if (h->n_active == 0) return fail(PRC_ERR_NO_ACTIVITY, "No tissue voxels: nothing to do");
+    int rc = ensure_em(h);
+    if (rc != PRC_OK) return rc;
+    h->f = h->vol[0], h->prev = h->vol[1], h->y = h->vol[2], h->h_prev = h->vol[3], h->est = h->vol[4];
+    // the history buffers start at zero (prc.cu:661-665): prev, y and h_prev
+    PRC_CUDA(cudaMemsetAsync(h->prev, 0, h->n * sizeof(float), s));
+    PRC_CUDA(cudaMemsetAsync(h->y, 0, h->n * sizeof(float), s));
+    PRC_CUDA(cudaMemsetAsync(h->h_prev, 0, h->n * sizeof(float), s));
+    PRC_CUDA(em_begin(h->em_volumes(), d_g, h->g_em, h->f, h->n_active, initialize, s));
+    h->em_started = true;
+    return PRC_OK;
+}
+
+int prc_em_begin(prc_handle* h, const float* d_g, void* stream) {
+    if (!h || !d_g) return fail(PRC_ERR_ARGUMENT, "Invalid argument");
+    return em_begin_impl(h, d_g, true, h->pick(stream));
+}
+
+int prc_em_iterate(prc_handle* h, int n_iter, float beta, float gamma, int accelerate, void* stream) {
+    if (!h) return fail(PRC_ERR_ARGUMENT, "Invalid argument");
+    if (!h->em_started) return fail(PRC_ERR_STATE, "prc_em_iterate called before prc_em_begin");
+    if (n_iter < 0 || !(beta >= 0) || !(gamma >= 0) || !std::isfinite(beta) || !std::isfinite(gamma))
+        return fail(PRC_ERR_ARGUMENT, "Invalid geometry or solver parameters");
+    const cudaStream_t s = h->pick(stream);
+    const EmVolumes v = h->em_volumes();
+    for (int it = 0; it < n_iter; ++it) {  // prc.cu:675-700
+        const float* start = h->f;
+        if (accelerate) {
+            PRC_CUDA(em_extrapolate(v, h->f, h->prev, h->y, s));
+            start = h->y;
+        }
+        int rc = prc_forward(h, start, h->est, s);
+        if (rc != PRC_OK) return rc;
+        PRC_CUDA(em_ratio(v, h->g_em, h->est, s));
+        rc = prc_adjoint(h, h->est, h->prev, s);  // prediction has consumed prev
+        if (rc != PRC_OK) return rc;
+        PRC_CUDA(em_update(v, h->g, start, h->prev, h->est, beta, gamma, s));
+        if (beta > 0.0f || accelerate)
+            PRC_CUDA(em_finish(v, h->est, accelerate ? h->y : nullptr, h->h_prev, beta > 0.0f, s));
+        if (accelerate) {
+            std::swap(h->y, h->h_prev);
+            std::swap(h->prev, h->f);
+        }
+        std::swap(h->f, h->est);
+    }
+    return PRC_OK;
+}
+
+int prc_em_estimate(prc_handle* h, float* d_out, void* stream) {
+    if (!h || !d_out) return fail(PRC_ERR_ARGUMENT, "Invalid argument");
+    if (!h->em_started) return fail(PRC_ERR_STATE, "prc_em_estimate called before prc_em_begin");
+    PRC_CUDA(cudaMemcpyAsync(d_out, h->f, h->n * sizeof(float), cudaMemcpyDeviceToDevice, h->pick(stream)));
+    return PRC_OK;
+}
+
+int prc_em_run(prc_handle* h, const float* d_g, float* d_out, int iterations, float beta, float gamma,
+               int accelerate, void* stream) {
+    if (!h || !d_g || !d_out) return fail(PRC_ERR_ARGUMENT, "Invalid argument");
+    if (iterations < 0) return fail(PRC_ERR_ARGUMENT, "Invalid geometry or solver parameters");
+    const cudaStream_t s = h->pick(stream);
+    int rc = em_begin_impl(h, d_g, iterations > 0, s);
+    if (rc == PRC_OK) rc = prc_em_iterate(h, iterations, beta, gamma, accelerate, s);
+    if (rc == PRC_OK) rc = prc_em_estimate(h, d_out, s);
+    return rc;
+}
+
+static int ensure_scratch(prc_handle* h) {
+    if (!h->scratch) PRC_CUDA(h->alloc(&h->scratch, h->n));
+    if (!h->scratch_out) PRC_CUDA(h->alloc(&h->scratch_out, h->n));
+    return PRC_OK;
+}
+
+int prc_em_run_host(prc_handle* h, const float* g_host, float* out_host, int iterations, float beta, float gamma,
+                    int accelerate) {
+    if (!h || !g_host || !out_host) return fail(PRC_ERR_ARGUMENT, "Invalid argument");
+    int rc = ensure_scratch(h);
+    if (rc != PRC_OK) return rc;
+    PRC_CUDA(cudaMemcpyAsync(h->scratch, g_host, h->n * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+    rc = prc_em_run(h, h->scratch, h->scratch, iterations, beta, gamma, accelerate, h->stream);
+    if (rc != PRC_OK) return rc;
+    PRC_CUDA(cudaMemcpyAsync(out_host, h->scratch, h->n * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+    PRC_CUDA(cudaStreamSynchronize(h->stream));
+    return PRC_OK;
+}
+
+int prc_em_begin_host(prc_handle* h, const float* g_host) {
+    if (!h || !g_host) return fail(PRC_ERR_ARGUMENT, "Invalid argument");
+    int rc = ensure_scratch(h);
+    if (rc != PRC_OK) return rc;
+    PRC_CUDA(cudaMemcpyAsync(h->scratch, g_host, h->n * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+    rc = em_begin_impl(h, h->scratch, true, h->stream);
+    if (rc != PRC_OK) return rc;
+    PRC_CUDA(cudaStreamSynchronize(h->stream));
+    return PRC_OK;
+}
+
+int prc_em_estimate_host(prc_handle* h, float* out_host) {
+    if (!h || !out_host) return fail(PRC_ERR_ARGUMENT, "Invalid argument");
+    if (!h->em_started) return fail(PRC_ERR_STATE, "prc_em_estimate_host called before prc_em_begin");
+    PRC_CUDA(cudaMemcpyAsync(out_host, h->f, h->n * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+    PRC_CUDA(cudaStreamSynchronize(h->stream));
+    return PRC_OK;
+}
+
+int prc_forward_host(prc_handle* h, const float* in_host, float* out_host) {
+    if (!h || !in_host || !out_host) return fail(PRC_ERR_ARGUMENT, "Invalid argument");
+    int rc = ensure_scratch(h);
+    if (rc != PRC_OK) return rc;
+    float* in = h->scratch;
+    float* out = h->scratch_out;
+    PRC_CUDA(cudaMemcpyAsync(in, in_host, h->n * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+    rc = prc_forward(h, in, out, h->stream);
+    if (rc != PRC_OK) return rc;
+    PRC_CUDA(cudaMemcpyAsync(out_host, out, h->n * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+    PRC_CUDA(cudaStreamSynchronize(h->stream));
+    return PRC_OK;
+}
+
+int prc_adjoint_host(prc_handle* h, const float* in_host, float* out_host) {
+    if (!h || !in_host || !out_host) return fail(PRC_ERR_ARGUMENT, "Invalid argument");
+    int rc = ensure_scratch(h);
+    if (rc != PRC_OK) return rc;
+    float* in = h->scratch;
+    float* out = h->scratch_out;
+    PRC_CUDA(cudaMemcpyAsync(in, in_host, h->n * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+    PRC_CUDA(cudaMemsetAsync(out, 0, h->n * sizeof(float), h->stream));
+    rc = prc_adjoint(h, in, out, h->stream);
+    if (rc != PRC_OK) return rc;
+    PRC_CUDA(cudaMemcpyAsync(out_host, out, h->n * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+    PRC_CUDA(cudaStreamSynchronize(h->stream));
+    return PRC_OK;
+}
+
+int prc_sum(prc_handle* h, const float* d_x, double* sum, void* stream) {
+    if (!h || !d_x || !sum) return fail(PRC_ERR_ARGUMENT, "Invalid argument");
+    int rc = ensure_em(h);
+    if (rc != PRC_OK) return rc;
+    const cudaStream_t s = h->pick(stream);
+    PRC_CUDA(em_sum(h->em_volumes(), d_x, s));
+    PRC_CUDA(cudaMemcpyAsync(sum, &h->scalars->sum, sizeof(double), cudaMemcpyDeviceToHost, s));
+    PRC_CUDA(cudaStreamSynchronize(s));
+    return PRC_OK;
+}
+
+int prc_count_deposits(prc_handle* h, int64_t* deposits) {
+    if (!h || !deposits) return fail(PRC_ERR_ARGUMENT, "Invalid argument");
+    PRC_CUDA(cudaMemsetAsync(h->counter, 0, sizeof(unsigned long long), h->stream));
+    OpArgs a = h->op_args();
+    a.count = h->counter;
+    PRC_CUDA(project(Op::Count, h->params, a, h->trace_near, h->stream));
+    unsigned long long v = 0;
+    PRC_CUDA(cudaMemcpyAsync(&v, h->counter, sizeof(v), cudaMemcpyDeviceToHost, h->stream));
+    PRC_CUDA(cudaStreamSynchronize(h->stream));
+    *deposits = (int64_t)v;
+    return PRC_OK;
+}
+
+int prc_synchronize(prc_handle* h) {
+    if (!h) return fail(PRC_ERR_ARGUMENT, "Invalid argument");
+    PRC_CUDA(cudaStreamSynchronize(h->stream));
+    return PRC_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,305 @@
+// prc_cli.cpp -- the `prc ISOTOPE NX NY NZ DX DY DZ [options]` command line, byte-compatible
+// with jlherraiz/PRC_MLEM's executable (prc.cu:452-722): same options and defaults, same raw
+// float32 I/O, same messages and exit codes.  All validation happens before the first CUDA call
+// (the reference's CLI tests run with every GPU hidden); the device work goes through the
+// C ABI of include/prc_b200.h.
+#include "../../include/prc_b200.h"
+
+#include <algorithm>
+#include <cerrno>
+#include <chrono>
+#include <climits>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+namespace {
+
+constexpr float kMinDensity = 1.0e-3f;
+constexpr int kNearRays = 2048;
+
+double now_s() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+struct Options {  // prc.cu:452-459
+    std::string isotope, mode = "correct", input = "ACTIVITY.raw", density = "DENSITY.raw", output;
+    int nx = 0, ny = 0, nz = 0;
+    float dx = 0, dy = 0, dz = 0;
+    int rays = 128, iterations = 20, save_every = 0;
+    float beta = 0.2f, gamma = 20.0f, support_rho = 0.05f, air_cap_mm = 50.0f;
+    bool reproject = false, cache_near = true, exact_range = false, accelerate = true, bf16 = false;
+    int cache = PRC_CACHE_FULL;
+};
+
+void print_usage(const char* prog, FILE* stream = stderr) {  // prc.cu:461-484
+    fprintf(stream,
+            "Usage: %s ISOTOPE NX NY NZ DX DY DZ [options]\n"
+            "  --mode correct|forward|adjoint   (default correct)\n"
+            "  --input FILE      blurred (correct) or source (forward/adjoint) image, default ACTIVITY.raw\n"
+            "  --density FILE    density map in g/cm3, default DENSITY.raw\n"
+            "  --output FILE     default ACTIVITY_PRC_V2.raw (correct), ACTIVITY_FWD.raw, ACTIVITY_ADJ.raw\n"
+            "  --rays N          even far-field rays per voxel (default 128)\n"
+            "  --iterations N    accelerated MAP-EM iterations (default 20)\n"
+            "  --beta B          relative-difference prior strength (default 0.2; 0 = no prior)\n"
+            "                    Add --no-accel for plain Richardson-Lucy.\n"
+            "  --gamma G         RDP edge preservation, larger keeps sharper edges (default 20)\n"
+            "  --support-rho R   minimum density of voxels that can hold activity (default 0.05)\n"
+            "  --air-cap-mm L    a positron that crossed L mm of air has escaped (default 50)\n"
+            "  --save-every K    also write the estimate every K iterations\n"
+            "  --reproject       also write A f of the result (_REPROJ.raw)\n"
+            "  --exact-range     evaluate the survival function analytically, not from the table (validation)\n"
+            "  --no-cache-near   trace the near block again in every pass (less GPU memory, slower)\n"
+            "  --no-accel        plain MAP-EM without Biggs-Andrews extrapolation (validation)\n"
+            "  --cache MODE      none|near|full: weights kept on the GPU between passes (default full)\n"
+            "  --bf16-weights    store the projector weights in bfloat16 (mixed precision)\n"
+            "Isotopes:",
+            prog);
+    for (int i = 0; i < prc_isotope_count(); ++i) fprintf(stream, " %s", prc_isotope_name(i));
+    fprintf(stream, "\n");
+}
+
+[[noreturn]] void die() { exit(EXIT_FAILURE); }
+
+int parse_int(const char* text, const char* name) {  // prc.cu:486-495
+    char* end = nullptr;
+    errno = 0;
+    const long value = strtol(text, &end, 10);
+    if (errno || end == text || *end || value < INT_MIN || value > INT_MAX) {
+        fprintf(stderr, "Invalid integer for %s: %s\n", name, text);
+        die();
+    }
+    return (int)value;
+}
+
+float parse_float(const char* text, const char* name) {  // prc.cu:497-506
+    char* end = nullptr;
+    errno = 0;
+    const float value = strtof(text, &end);
+    if (errno || end == text || *end || !std::isfinite(value)) {
+        fprintf(stderr, "Invalid finite number for %s: %s\n", name, text);
+        die();
+    }
+    return value;
+}
+
+Options parse(int argc, char** argv) {  // prc.cu:508-555
+    Options o;
+    if (argc < 8) {
+        print_usage(argv[0]);
+        die();
+    }
+    o.isotope = argv[1];
+    o.nx = parse_int(argv[2], "NX"), o.ny = parse_int(argv[3], "NY"), o.nz = parse_int(argv[4], "NZ");
+    o.dx = parse_float(argv[5], "DX"), o.dy = parse_float(argv[6], "DY"), o.dz = parse_float(argv[7], "DZ");
+    for (int i = 8; i < argc; ++i) {
+        const std::string key = argv[i];
+        auto value = [&]() -> const char* {
+            if (i + 1 >= argc) {
+                fprintf(stderr, "Missing value for %s\n", key.c_str());
+                die();
+            }
+            return argv[++i];
+        };
+        if (key == "--mode") o.mode = value();
+        else if (key == "--input") o.input = value();
+        else if (key == "--density") o.density = value();
+        else if (key == "--output") o.output = value();
+        else if (key == "--rays") o.rays = parse_int(value(), key.c_str());
+        else if (key == "--iterations") o.iterations = parse_int(value(), key.c_str());
+        else if (key == "--beta") o.beta = parse_float(value(), key.c_str());
+        else if (key == "--gamma") o.gamma = parse_float(value(), key.c_str());
+        else if (key == "--support-rho") o.support_rho = parse_float(value(), key.c_str());
+        else if (key == "--air-cap-mm") o.air_cap_mm = parse_float(value(), key.c_str());
+        else if (key == "--save-every") o.save_every = parse_int(value(), key.c_str());
+        else if (key == "--reproject") o.reproject = true;
+        else if (key == "--no-cache-near") o.cache_near = false;
+        else if (key == "--cache") {
+            const std::string m = value();
+            o.cache = m == "none" ? PRC_CACHE_NONE : m == "near" ? PRC_CACHE_NEAR : m == "full" ? PRC_CACHE_FULL : -1;
+        }
+        else if (key == "--exact-range") o.exact_range = true;
+        else if (key == "--no-accel") o.accelerate = false;
+        else if (key == "--bf16-weights") o.bf16 = true;
+        else {
+            fprintf(stderr, "Unknown option %s\n", key.c_str());
+            print_usage(argv[0]);
+            die();
+        }
+    }
+    if (o.nx <= 0 || o.ny <= 0 || o.nz <= 0 || o.dx <= 0 || o.dy <= 0 || o.dz <= 0 || o.rays < 2 || (o.rays & 1) ||
+        o.rays > INT_MAX - 31 || o.iterations < 0 || o.iterations == INT_MAX || o.beta < 0 || o.gamma < 0 ||
+        o.support_rho < 0 || o.air_cap_mm <= 0 || o.save_every < 0 || o.cache < 0 ||
+        (o.mode != "correct" && o.mode != "forward" && o.mode != "adjoint")) {
+        fprintf(stderr, "Invalid geometry or solver parameters\n");
+        die();
+    }
+    if (o.nx > INT_MAX / o.ny || o.nx * o.ny > INT_MAX / o.nz) {
+        fprintf(stderr, "Volume exceeds the INT_MAX voxel index limit\n");
+        die();
+    }
+    if (o.output.empty())
+        o.output = o.mode == "correct" ? "ACTIVITY_PRC_V2.raw" : o.mode == "forward" ? "ACTIVITY_FWD.raw" : "ACTIVITY_ADJ.raw";
+    return o;
+}
+
+// "_it003" / "_REPROJ" go before the extension of the file name, never into a dotted
+// directory (prc.cu:557-562).
+std::string with_suffix(const std::string& path, const std::string& suffix) {
+    const size_t dot = path.rfind('.');
+    const size_t slash = path.find_last_of("/\\");
+    const size_t start = slash == std::string::npos ? 0 : slash + 1;
+    return dot == std::string::npos || dot <= start ? path + suffix : path.substr(0, dot) + suffix + path.substr(dot);
+}
+
+void read_raw(const std::string& path, std::vector<float>* v) {  // prc.cu:339-347
+    FILE* fp = fopen(path.c_str(), "rb");
+    if (!fp || fread(v->data(), sizeof(float), v->size(), fp) != v->size() || fgetc(fp) != EOF || ferror(fp)) {
+        fprintf(stderr, "Expected exactly %zu float32 values in %s\n", v->size(), path.c_str());
+        die();
+    }
+    fclose(fp);
+}
+
+void save_image(const std::string& path, const std::vector<float>& host) {  // prc.cu:349-360
+    for (float value : host)
+        if (!std::isfinite(value)) {
+            fprintf(stderr, "Non-finite output: %s\n", path.c_str());
+            die();
+        }
+    FILE* fp = fopen(path.c_str(), "wb");
+    if (!fp || fwrite(host.data(), sizeof(float), host.size(), fp) != host.size() || fclose(fp) != 0) {
+        fprintf(stderr, "Cannot write %s\n", path.c_str());
+        die();
+    }
+}
+
+void check(int rc) {
+    if (rc != PRC_OK) {
+        fprintf(stderr, "%s\n", prc_last_error());
+        die();
+    }
+}
+
+double host_sum(const std::vector<float>& v) {
+    double s = 0.0;
+    for (float x : v) s += x;
+    return s;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+    if (argc == 2 && (!strcmp(argv[1], "--help") || !strcmp(argv[1], "-h"))) {
+        print_usage(argv[0], stdout);
+        return EXIT_SUCCESS;
+    }
+    const Options o = parse(argc, argv);
+    float cutoff = 0.0f;
+    if (prc_isotope_cutoff(o.isotope.c_str(), &cutoff) != PRC_OK) {
+        print_usage(argv[0]);
+        return EXIT_FAILURE;
+    }
+    const size_t n = (size_t)o.nx * o.ny * o.nz;
+
+    const double t0 = now_s();
+    std::vector<float> rho(n), img(n);
+    read_raw(o.density, &rho);
+    read_raw(o.input, &img);
+    size_t n_active = 0;
+    double input_sum = 0.0, support_sum = 0.0;
+    for (size_t i = 0; i < n; ++i) {  // prc.cu:598-613
+        if (!std::isfinite(rho[i]) || !std::isfinite(img[i])) {
+            fprintf(stderr, "Non-finite density or activity at voxel %zu\n", i);
+            return EXIT_FAILURE;
+        }
+        rho[i] = std::max(rho[i], kMinDensity);
+        img[i] = std::max(img[i], 0.0f);
+        input_sum += img[i];
+        if (rho[i] >= o.support_rho) {
+            ++n_active;
+            support_sum += img[i];
+        } else {
+            img[i] = 0.0f;
+        }
+    }
+    printf("isotope %s, grid %dx%dx%d, voxel %.3fx%.3fx%.3f mm, cutoff %.3f mm (water), air cap %.1f mm\n",
+           o.isotope.c_str(), o.nx, o.ny, o.nz, o.dx, o.dy, o.dz, cutoff, o.air_cap_mm);
+    printf("tissue voxels %zu (%.1f%%), input counts in tissue %.6g of %.6g (%.2f%%)\n", n_active,
+           100.0 * n_active / n, support_sum, input_sum, input_sum > 0 ? 100.0 * support_sum / input_sum : 0.0);
+    if (support_sum == 0.0) {
+        fprintf(stderr, "No activity in voxels with density >= %g: nothing to do\n", o.support_rho);
+        return EXIT_FAILURE;
+    }
+
+    // First CUDA contact.
+    prc_geometry geo{o.nx, o.ny, o.nz, o.dx, o.dy, o.dz};
+    prc_options opts;
+    prc_default_options(&opts);
+    opts.rays = o.rays;
+    opts.support_rho = o.support_rho;
+    opts.air_cap_mm = o.air_cap_mm;
+    opts.exact_range = o.exact_range;
+    opts.cache = o.cache_near ? o.cache : PRC_CACHE_NONE;
+    opts.precision = o.bf16 ? PRC_PRECISION_BF16 : PRC_PRECISION_FP32;
+    double t = now_s();
+    prc_handle* h = nullptr;
+    check(prc_create(&geo, o.isotope.c_str(), &opts, rho.data(), &h));
+    int64_t bytes = 0, far_entries = 0;
+    int mode = 0;
+    prc_device_bytes(h, &bytes);
+    prc_cache_mode(h, &mode, &far_entries);
+    printf("normalisation (%d near-block + %d far-field rays): %.2f s, cache %s, device memory %.0f MiB\n", kNearRays,
+           o.rays, now_s() - t, mode == PRC_CACHE_FULL ? "near+far" : mode == PRC_CACHE_NEAR ? "near" : "none",
+           bytes / 1048576.0);
+
+    std::vector<float> out(n);
+    if (o.mode == "forward" || o.mode == "adjoint") {  // prc.cu:648-657
+        t = now_s();
+        check(o.mode == "forward" ? prc_forward_host(h, img.data(), out.data()) : prc_adjoint_host(h, img.data(), out.data()));
+        printf("%s: %.3f s\n", o.mode.c_str(), now_s() - t);
+        save_image(o.output, out);
+        printf("sum in %.6g, sum out %.6g, total %.2f s\n", support_sum, host_sum(out), now_s() - t0);
+        prc_destroy(h);
+        return EXIT_SUCCESS;
+    }
+
+    // MAP-EM (prc.cu:659-720)
+    printf("MAP-EM: %d iterations, beta %.4g, gamma %.3g\n", o.iterations, o.beta, o.gamma);
+    t = now_s();
+    if (o.iterations == 0) {
+        check(prc_em_run_host(h, img.data(), out.data(), 0, o.beta, o.gamma, o.accelerate));
+    } else {
+        check(prc_em_begin_host(h, img.data()));
+        t = now_s();
+        for (int it = 1; it <= o.iterations; ++it) {
+            check(prc_em_iterate(h, 1, o.beta, o.gamma, o.accelerate, nullptr));
+            if (it == 1 || it % 10 == 0 || it == o.iterations) {
+                check(prc_synchronize(h));
+                printf("iteration %d/%d: %.2f s\n", it, o.iterations, now_s() - t);
+            }
+            if (o.save_every > 0 && it % o.save_every == 0 && it < o.iterations) {
+                char tag[32];
+                snprintf(tag, sizeof(tag), "_it%03d", it);
+                check(prc_em_estimate_host(h, out.data()));
+                save_image(with_suffix(o.output, tag), out);
+            }
+        }
+        check(prc_em_estimate_host(h, out.data()));
+    }
+    const double t_iter = now_s() - t;
+    save_image(o.output, out);
+    if (o.reproject) {
+        std::vector<float> reproj(n);
+        check(prc_forward_host(h, out.data(), reproj.data()));
+        save_image(with_suffix(o.output, "_REPROJ"), reproj);
+    }
+    printf("sum blurred (tissue) %.6g, sum corrected %.6g\n", support_sum, host_sum(out));
+    printf("iterations %.2f s (%.2f s each), total %.2f s\n", t_iter, o.iterations ? t_iter / o.iterations : 0.0,
+           now_s() - t0);
+    prc_destroy(h);
+    return EXIT_SUCCESS;
+}

@@ -1,0 +1,153 @@
+"""MAP-EM parity and behaviour on a B200 (prc.cu:659-711; tests/test_solver.py:245-348): the
+corrected images match the reference executable within 1e-5 relative L2 in every fp32 form, the
+bf16-weight form stays within 1 % NRMSE of the FP64 oracle, and the solver's invariants hold."""
+import numpy as np
+import pytest
+import torch
+
+import prc_mlem_b200 as pm
+from conftest import nrmse, rel_l2
+
+pytestmark = pytest.mark.gpu
+EM_CASES = {"em_b0.1_it3": (3, 0.1, 20.0, True), "em_b0_it4_plain": (4, 0.0, 20.0, False),
+            "em_b0.2_it2_plain": (2, 0.2, 20.0, False), "em_b0.03_it6": (6, 0.03, 20.0, True),
+            "em_b0_it25": (25, 0.0, 20.0, True)}
+_cache = {}
+
+
+def projector(fixture72, cache=pm.PRC_CACHE_FULL, prec=pm.PRC_PRECISION_FP32):
+    if (cache, prec) not in _cache:
+        rho, x, y, shape, sp = fixture72
+        _cache[(cache, prec)] = pm.Projector("68Ga", rho, sp, rays=32, cache=cache, precision=prec)
+    return _cache[(cache, prec)]
+
+
+@pytest.mark.parametrize("cache", [pm.PRC_CACHE_FULL, pm.PRC_CACHE_NEAR, pm.PRC_CACHE_NONE], ids=["full", "near", "none"])
+@pytest.mark.parametrize("case", sorted(EM_CASES))
+def test_correction_matches_reference_binary(fixture72, ref_golden, oracle_mod, case, cache):
+    rho, x, y, shape, sp = fixture72
+    it, beta, gamma, accel = EM_CASES[case]
+    out = projector(fixture72, cache).correct_host(x, it, beta, gamma, accel)
+    assert rel_l2(out, ref_golden[f"fixture_{case}"]) < 1e-5
+
+
+@pytest.mark.parametrize("case", sorted(EM_CASES))
+def test_bf16_correction_within_one_percent_of_fp64(fixture72, oracle_mod, case):
+    rho, x, y, shape, sp = fixture72
+    it, beta, gamma, accel = EM_CASES[case]
+    out = projector(fixture72, pm.PRC_CACHE_FULL, pm.PRC_PRECISION_BF16).correct_host(x, it, beta, gamma, accel)
+    fp64 = oracle_mod.Problem("68Ga", rho, sp, rays=32, precision=64).correct(x, it, beta, gamma, accel)
+    assert nrmse(out, fp64) < 0.01
+
+
+def test_small_phantom_correction_matches_reference_binary(ref_golden):
+    from prc_mlem_b200 import phantoms
+    rho, truth, sp = phantoms.small_phantom(seed=1)
+    with pm.Projector("18F", rho, sp, rays=32) as P:
+        out = P.correct_host(ref_golden["small_g"], 4, 0.0, 20.0, False)
+    assert rel_l2(out, ref_golden["small_em_b0_it4_plain"]) < 1e-5
+
+
+def test_zero_iterations_preserves_supported_input_exactly(fixture72):
+    rho, x, y, shape, sp = fixture72
+    src = x.copy()
+    src[5, 4, 5] = 0
+    np.testing.assert_array_equal(projector(fixture72).correct_host(src, 0), src)
+
+
+@pytest.mark.parametrize("iterations", [1, 2])
+def test_acceleration_warmup_matches_plain(fixture72, iterations):
+    rho, x, y, shape, sp = fixture72
+    P = projector(fixture72)
+    acc = P.correct_host(x, iterations, 0.2, 20.0, True)
+    plain = P.correct_host(x, iterations, 0.2, 20.0, False)
+    np.testing.assert_allclose(acc, plain, rtol=3e-5, atol=3e-6)
+
+
+@pytest.mark.parametrize("accel", [True, False])
+def test_unregularised_rl_conserves_counts(fixture72, accel):
+    rho, x, y, shape, sp = fixture72
+    P = projector(fixture72)
+    out = P.correct_host(x, 25, 0.0, 20.0, accel)
+    assert out.min() >= 0
+    assert np.all(out[~P.support] == 0)
+    assert abs(out.sum(dtype=np.float64) / x.sum(dtype=np.float64) - 1) < 5e-6
+
+
+def test_sparse_observations_do_not_lock_supported_zeros(fixture72):
+    rho, x, y, shape, sp = fixture72
+    P = projector(fixture72)
+    sparse = x.copy()
+    sparse[np.random.default_rng(21).random(shape) < 0.5] = 0
+    out = P.correct_host(sparse, 5, 0.1, 20.0, True)
+    zeros = (sparse == 0) & P.support
+    assert np.mean(out[zeros] > 0) > 0.95
+    assert out.min() >= 0 and np.all(out[~P.support] == 0)
+    assert abs(out.sum(dtype=np.float64) / sparse.sum(dtype=np.float64) - 1) < 3e-6
+
+
+def test_activity_unit_scaling(fixture72):
+    rho, x, y, shape, sp = fixture72
+    P = projector(fixture72)
+    a = P.correct_host(x, 4, 0.1, 20.0, True)
+    b = P.correct_host(x * 1000, 4, 0.1, 20.0, True) / 1000
+    np.testing.assert_allclose(b, a, rtol=5e-5, atol=5e-6)
+
+
+def test_long_sparse_cold_reconstruction(fixture72):
+    rho, x, y, shape, sp = fixture72
+    P = projector(fixture72)
+    truth = P.support.astype(np.float32)
+    cold = np.zeros(shape, bool)
+    cold[4:8, 3:7, 3:7] = True
+    cold &= P.support
+    truth[cold] = 0
+    blurred = P.forward_host(truth)
+    sparse = (np.random.default_rng(81).poisson(2 * blurred) / 2).astype(np.float32)
+    missed = (sparse == 0) & P.support & ~cold
+    assert missed.sum() > 20
+    for accel in (True, False):
+        out = P.correct_host(sparse, 30, 0.2, 20.0, accel)
+        assert out.min() >= 0 and np.all(out[~P.support] == 0)
+        assert np.mean(out[missed] > 0) > 0.95
+        assert out[cold].mean() < out[P.support & ~cold].mean()
+        assert abs(out.sum(dtype=np.float64) / sparse.sum(dtype=np.float64) - 1) < 5e-6
+
+
+def test_acceleration_approaches_long_plain_reference_sooner(fixture72):
+    rho, x, y, shape, sp = fixture72
+    P = projector(fixture72)
+    blurred = P.forward_host(x)
+    plain = P.correct_host(blurred, 400, 0.2, 20.0, False)
+    acc = P.correct_host(blurred, 100, 0.2, 20.0, True)
+    short = P.correct_host(blurred, 100, 0.2, 20.0, False)
+    dist = lambda im: np.linalg.norm(im - plain) / np.linalg.norm(plain)
+    assert dist(acc) < 1e-3
+    assert dist(acc) < 0.5 * dist(short)
+    assert abs(acc.sum(dtype=np.float64) / blurred.sum(dtype=np.float64) - 1) < 3e-6
+
+
+def test_incremental_iterations_equal_one_run(fixture72):
+    """prc_em_iterate carries the acceleration history across calls."""
+    rho, x, y, shape, sp = fixture72
+    P = projector(fixture72)
+    d_g = torch.from_numpy(x).cuda()
+    d_a, d_b = torch.empty_like(d_g), torch.empty_like(d_g)
+    P.correct(d_g, d_a, 7, 0.1, 20.0, True)
+    P.em_begin(d_g)
+    P.em_iterate(2, 0.1, 20.0, True)
+    P.em_iterate(5, 0.1, 20.0, True)
+    P.em_estimate(d_b)
+    P.synchronize()
+    assert rel_l2(d_b.cpu().numpy(), d_a.cpu().numpy()) < 1e-6
+
+
+def test_state_errors(fixture72):
+    rho, x, y, shape, sp = fixture72
+    with pm.Projector("68Ga", rho, sp, rays=32) as P:
+        with pytest.raises(pm.PrcError) as e:
+            P.em_iterate(1, 0.1, 20.0, True)
+        assert e.value.code == 7
+        d = torch.from_numpy(x).cuda()
+        with pytest.raises(pm.PrcError):
+            P.correct(d, d, -1)
