@@ -36,16 +36,20 @@ struct ProjParams {
     int n_branch;            // analytic model (used when table == nullptr)
     Branch br[3];
     // Far-field layout (used by the stored field; null until the layout pass has run).
-    const int* tmpl;                 // [n_rays][tmpl_len]: linear target offset of the m-th step
-                                     // of ray r after it left the near block (same for every source)
-    int tmpl_len;                    // nx + ny + nz: no ray takes more steps inside the image
-    const unsigned short* len;       // [n_groups][n_rays]: stored steps of ray r in group G
-    const long long* group_base;     // [n_groups]: element offset of group G's far field
+    const int* tmpl;                 // [n_rows][tmpl_len]: linear target offset of step m of row k;
+                                     // row 0 is the 5x5x5 block, row 1 + r the post-block steps of
+                                     // far ray r (the same for every source)
+    int tmpl_len;                    // steps per row: covers every step a ray takes in the image
+    int n_rows;                      // n_rays + 1
+    const unsigned short* len;       // [n_groups][n_rows]: stored steps of row k in group G
+    const long long* group_base;     // [n_groups + 1]: element offset of group G's stream
+    const int* desc;                 // per pack: template element offset of its first step
 };
 
-// Stored far-field weights ("coefficient field"): for group G, ray r, post-block step m and
-// lane l, entry group_base[G] + (sum_{r'<r} len[G][r'] + m) * 32 + l.  Target voxels come from
-// the ray template, so no index is stored; forward and adjoint read the same field.
+// Stored weights ("coefficient field") of near block and far rays: for group G, template row k,
+// step m and lane l, the entry group_base[G] + (sum_{k'<k} len[G][k']) * 32 + (m / 4) * 128 +
+// l * 4 + m % 4.  Target voxels come from the template, so no index is stored; forward and
+// adjoint read the same field.
 struct FarField {
     float* f32 = nullptr;
     __nv_bfloat16* b16 = nullptr;
@@ -76,6 +80,7 @@ struct OpArgs {
     NearCache near;
     FarField far;
     unsigned long long* count = nullptr;
+    unsigned int* error = nullptr;         // set non-zero when a stored-field copy timed out
     unsigned short* len = nullptr;         // Layout output
     long long* group_total = nullptr;      // Layout output: entries per group (sum of len * 32)
 };
@@ -85,8 +90,12 @@ cudaError_t setup_rays(const Grid& g, int n_rays, RayStep* d_far, RayStep* d_nea
 // trace_near: retrace the near block (no cache).  Forward / Adjoint / Count read the stored far
 // field when a.far is on, and march the far rays otherwise.
 cudaError_t project(Op op, const ProjParams& p, const OpArgs& a, bool trace_near, cudaStream_t s);
-// Fills the ray template p.tmpl ([n_rays][tmpl_len] ints).
+// Fills the template p.tmpl ([n_rows][tmpl_len] ints).
 cudaError_t build_template(const ProjParams& p, int* tmpl, cudaStream_t s);
+// Fills the pack descriptors (one int per 128 stored entries) from p.len and p.group_base.
+cudaError_t build_descriptors(const ProjParams& p, int* desc, cudaStream_t s);
+// Stored steps of the near-block row (125 offsets padded to whole packs).
+int near_row_steps();
 
 // em.cu ---------------------------------------------------------------------------------------
 // Device scalars of one MAP-EM run; all FP64 where the reference accumulates in FP64.

@@ -4,6 +4,7 @@
 #include "../../include/prc_b200.h"
 #include "engine.h"
 
+#include <algorithm>
 #include <climits>
 #include <cmath>
 #include <cstdio>
@@ -57,11 +58,13 @@ struct prc_handle {
     unsigned short* len = nullptr;
     long long* group_base = nullptr;
     long long* group_total = nullptr;
+    int* desc = nullptr;
     int64_t far_entries = 0;
     int cache_mode = PRC_CACHE_NONE;
     bool trace_near = false;
     ProjParams params{};
     unsigned long long* counter = nullptr;
+    unsigned int* error = nullptr;  // device flag raised by a kernel that gave up a bounded wait
     float* scratch = nullptr;      // input volume of the host-memory forms
     float* scratch_out = nullptr;  // output volume of the host-memory operator forms
 
@@ -96,9 +99,22 @@ struct prc_handle {
         a.W = W;
         a.near = cache;
         a.far = far_field;
+        a.error = error;
         return a;
     }
 };
+
+// Reads and clears the device error flag; a raised flag means a kernel gave up a bounded wait.
+static int check_device_error(prc_handle* h) {
+    unsigned int flag = 0;
+    PRC_CUDA(cudaMemcpyAsync(&flag, h->error, sizeof(flag), cudaMemcpyDeviceToHost, h->stream));
+    PRC_CUDA(cudaStreamSynchronize(h->stream));
+    if (flag) {
+        PRC_CUDA(cudaMemsetAsync(h->error, 0, sizeof(flag), h->stream));
+        return fail(PRC_ERR_CUDA, "a stored-field copy did not complete within its bounded wait");
+    }
+    return PRC_OK;
+}
 
 extern "C" {
 
@@ -163,6 +179,7 @@ static int create_impl(prc_handle* h, const float* density_host) {
     PRC_CUDA(h->alloc(&h->far, h->opts.rays));
     PRC_CUDA(h->alloc(&h->near_rays, kNearRays));
     PRC_CUDA(h->alloc(&h->counter, 1));
+    PRC_CUDA(h->alloc(&h->error, 1));
     PRC_CUDA(cudaMemcpyAsync(h->rho, rho.data(), h->n * sizeof(float), cudaMemcpyHostToDevice, h->stream));
     PRC_CUDA(cudaMemcpyAsync(h->support, support.data(), h->n, cudaMemcpyHostToDevice, h->stream));
     if (h->n_active)
@@ -192,28 +209,19 @@ static int create_impl(prc_handle* h, const float* density_host) {
 
     const bool bf16 = h->opts.precision == PRC_PRECISION_BF16;
     const size_t elem = bf16 ? 2 : 4;
-    // Near cache when it fits in a quarter of free memory (prc.cu:411-419).
     h->trace_near = true;
-    if (h->opts.cache >= PRC_CACHE_NEAR && h->n_groups) {
-        size_t free_b = 0, total_b = 0;
-        PRC_CUDA(cudaMemGetInfo(&free_b, &total_b));
-        const size_t entries = (size_t)h->n_groups * kNear * kLanes;
-        if (entries * elem <= free_b / 4) {
-            cudaError_t e = bf16 ? h->alloc(&h->cache.b16, entries) : h->alloc(&h->cache.f32, entries);
-            if (e == cudaSuccess) h->trace_near = false, h->cache_mode = PRC_CACHE_NEAR;
-            else cudaGetLastError();  // optional: fall back to retracing
-        }
-    }
-    // Far-field coefficient field: size it with a layout pass, then let the Norm pass fill it.
-    // Template rows hold every step a ray can take inside the image plus the padding of the
-    // last packed group of 4, rounded to whole int4s.
-    const long long tmpl_len = ((long long)g.nx + g.ny + g.nz + 3 + 3) / 4 * 4;
-    if (h->opts.cache == PRC_CACHE_FULL && !h->trace_near && tmpl_len < 65535) {
+    // Stored coefficient field (near block + far rays): size it with a layout pass, then let
+    // the Norm pass fill it.  Template rows hold every step a ray can take inside the image
+    // plus the padding of the last pack, in whole int4s.
+    const long long tmpl_len =
+        std::max<long long>(near_row_steps(), ((long long)g.nx + g.ny + g.nz + 3 + 3) / 4 * 4);
+    if (h->opts.cache == PRC_CACHE_FULL && h->n_groups && tmpl_len < 65535) {
         p.tmpl_len = (int)tmpl_len;
-        PRC_CUDA(h->alloc(&h->tmpl, (size_t)h->opts.rays * tmpl_len));
-        PRC_CUDA(h->alloc(&h->len, (size_t)h->n_groups * h->opts.rays));
+        p.n_rows = h->opts.rays + 1;
+        PRC_CUDA(h->alloc(&h->tmpl, (size_t)p.n_rows * tmpl_len));
+        PRC_CUDA(h->alloc(&h->len, (size_t)h->n_groups * p.n_rows));
         PRC_CUDA(h->alloc(&h->group_total, h->n_groups));
-        PRC_CUDA(h->alloc(&h->group_base, h->n_groups));
+        PRC_CUDA(h->alloc(&h->group_base, (size_t)h->n_groups + 1));
         p.tmpl = h->tmpl;
         PRC_CUDA(build_template(p, h->tmpl, h->stream));
         OpArgs la = h->op_args();
@@ -230,26 +238,43 @@ static int create_impl(prc_handle* h, const float* density_host) {
             t = run;
             run += v;
         }
+        totals.push_back(run);  // group_base[n_groups]: end of the last group
         size_t free_b = 0, total_b = 0;
         PRC_CUDA(cudaMemGetInfo(&free_b, &total_b));
-        if ((size_t)run * elem <= free_b / 2) {
+        const size_t desc_count = (size_t)(run / (4 * kLanes));
+        if ((size_t)run * elem + desc_count * 4 <= free_b / 2) {
             cudaError_t e = bf16 ? h->alloc(&h->far_field.b16, (size_t)run) : h->alloc(&h->far_field.f32, (size_t)run);
+            if (e == cudaSuccess) e = h->alloc(&h->desc, desc_count);
             if (e == cudaSuccess) {
                 PRC_CUDA(cudaMemcpyAsync(h->group_base, totals.data(), totals.size() * sizeof(long long),
                                          cudaMemcpyHostToDevice, h->stream));
                 p.len = h->len;
                 p.group_base = h->group_base;
+                PRC_CUDA(build_descriptors(p, h->desc, h->stream));
+                p.desc = h->desc;
                 h->far_entries = run;
                 h->cache_mode = PRC_CACHE_FULL;
+                h->trace_near = false;
             } else {
-                cudaGetLastError();  // optional: far rays stay traced
+                cudaGetLastError();  // optional: fall back to the near cache
             }
+        }
+    }
+    // Near cache when the field is off and it fits in a quarter of free memory (prc.cu:411-419).
+    if (h->cache_mode != PRC_CACHE_FULL && h->opts.cache >= PRC_CACHE_NEAR && h->n_groups) {
+        size_t free_b = 0, total_b = 0;
+        PRC_CUDA(cudaMemGetInfo(&free_b, &total_b));
+        const size_t entries = (size_t)h->n_groups * kNear * kLanes;
+        if (entries * elem <= free_b / 4) {
+            cudaError_t e = bf16 ? h->alloc(&h->cache.b16, entries) : h->alloc(&h->cache.f32, entries);
+            if (e == cudaSuccess) h->trace_near = false, h->cache_mode = PRC_CACHE_NEAR;
+            else cudaGetLastError();  // optional: fall back to retracing
         }
     }
     OpArgs a = h->op_args();
     PRC_CUDA(project(Op::Norm, p, a, true, h->stream));
     PRC_CUDA(cudaStreamSynchronize(h->stream));
-    return PRC_OK;
+    return check_device_error(h);
 }
 
 int prc_create(const prc_geometry* geo, const char* isotope, const prc_options* opts_in, const float* density_host,
@@ -428,8 +453,7 @@ int prc_em_run_host(prc_handle* h, const float* g_host, float* out_host, int ite
     rc = prc_em_run(h, h->scratch, h->scratch, iterations, beta, gamma, accelerate, h->stream);
     if (rc != PRC_OK) return rc;
     PRC_CUDA(cudaMemcpyAsync(out_host, h->scratch, h->n * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
-    PRC_CUDA(cudaStreamSynchronize(h->stream));
-    return PRC_OK;
+    return check_device_error(h);
 }
 
 int prc_em_begin_host(prc_handle* h, const float* g_host) {
@@ -461,8 +485,7 @@ int prc_forward_host(prc_handle* h, const float* in_host, float* out_host) {
     rc = prc_forward(h, in, out, h->stream);
     if (rc != PRC_OK) return rc;
     PRC_CUDA(cudaMemcpyAsync(out_host, out, h->n * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
-    PRC_CUDA(cudaStreamSynchronize(h->stream));
-    return PRC_OK;
+    return check_device_error(h);
 }
 
 int prc_adjoint_host(prc_handle* h, const float* in_host, float* out_host) {
@@ -476,8 +499,7 @@ int prc_adjoint_host(prc_handle* h, const float* in_host, float* out_host) {
     rc = prc_adjoint(h, in, out, h->stream);
     if (rc != PRC_OK) return rc;
     PRC_CUDA(cudaMemcpyAsync(out_host, out, h->n * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
-    PRC_CUDA(cudaStreamSynchronize(h->stream));
-    return PRC_OK;
+    return check_device_error(h);
 }
 
 int prc_sum(prc_handle* h, const float* d_x, double* sum, void* stream) {
@@ -507,7 +529,7 @@ int prc_count_deposits(prc_handle* h, int64_t* deposits) {
 int prc_synchronize(prc_handle* h) {
     if (!h) return fail(PRC_ERR_ARGUMENT, "Invalid argument");
     PRC_CUDA(cudaStreamSynchronize(h->stream));
-    return PRC_OK;
+    return check_device_error(h);
 }
 
 }  // extern "C"

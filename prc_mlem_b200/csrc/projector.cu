@@ -141,28 +141,83 @@ __device__ __forceinline__ void march(const ProjParams& p, const RayStep& R, boo
 enum NearMode : int { kTraceNear = 0, kCacheF32 = 1, kCacheBF16 = 2 };
 enum FarMode : int { kMarch = 0, kFieldF32 = 1, kFieldBF16 = 2 };
 
-// kPack consecutive steps of one lane are stored together (one vector load per lane).
+// ---- stored coefficient field ----------------------------------------------------------------
+// Stream of one group: template row 0 is the near block (125 offsets, padded to kNearRow
+// steps), rows 1..n_rays the far rays after they leave the block.  Row k contributes len[G][k]
+// steps (a multiple of kPack, zero for rays no lane deposits on).  kPack consecutive steps of
+// one lane are stored together, so a "pack" (kPack steps x 32 lanes) is one vector load per
+// lane, and a group's packs are contiguous in stream order.  desc[pack] holds the element
+// offset of the pack's first step in the template, so every pack can be addressed without
+// walking the stream.
 constexpr int kPack = 4;
+constexpr int kNearRow = 128;  // 125 block offsets rounded up to whole packs
+// TMA ring of the field stream: kStages chunks of kChunk bytes per warp.
+constexpr int kStages = 4;
+constexpr int kChunk = 2048;
+constexpr size_t kFieldSmemBytes = size_t(kWarps) * kStages * kChunk;
+// try_wait rounds before a field copy is declared lost (each round is a bounded hardware wait).
+constexpr int kWaitRounds = 1 << 20;
 
-// Streaming (evict-first) vector load of kPack stored weights of this lane.
-template <int FAR_MODE>
-__device__ __forceinline__ void load_pack(const FarField& f, long long e, float* w) {
-    if constexpr (FAR_MODE == kFieldF32) {
-        const float4 v = __ldcs(reinterpret_cast<const float4*>(f.f32 + e));
-        w[0] = v.x, w[1] = v.y, w[2] = v.z, w[3] = v.w;
-    } else {
-        const uint2 v = __ldcs(reinterpret_cast<const uint2*>(f.b16 + e));
-        w[0] = __uint_as_float(v.x << 16), w[1] = __uint_as_float(v.x & 0xffff0000u);
-        w[2] = __uint_as_float(v.y << 16), w[3] = __uint_as_float(v.y & 0xffff0000u);
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+    return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbarrier_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+// 1D bulk copy global -> this CTA's shared memory, completion counted on an mbarrier.
+// Source and destination are 16-byte aligned and bytes is a multiple of 16.
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity) {
+    for (int i = 0; i < kWaitRounds; ++i) {
+        unsigned done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(smem_u32(bar)), "r"(parity)
+            : "memory");
+        if (done) return true;
     }
+    return false;
+}
+
+__device__ __forceinline__ int near_offset(const ProjParams& p, int q) {
+    const int dx = q % kNearSide - kNearR, dy = q / kNearSide % kNearSide - kNearR,
+              dz = q / (kNearSide * kNearSide) - kNearR;
+    return (dz * p.g.ny + dy) * p.g.nx + dx;
+}
+
+// Element index of (step m of the row whose stream block starts at row_base) for this lane.
+__device__ __forceinline__ long long pack_slot(long long row_base, int m, int lane) {
+    return row_base + (long long)(m / kPack) * (kPack * kLanes) + lane * kPack + m % kPack;
+}
+
+template <int FAR_MODE>
+__device__ __forceinline__ void store_weight(const FarField& f, long long e, float w) {
+    if constexpr (FAR_MODE == kFieldF32) f.f32[e] = w;
+    else f.b16[e] = __float2bfloat16_rn(w);
 }
 
 // One warp per group of 32 consecutive sources.  NEAR_MODE says where the 5x5x5 weights come
-// from, FAR_MODE whether far rays are marched or read from the stored field.  Norm always
-// marches and, when the caches are allocated, writes them; Layout marches to size the field.
+// from when the far rays are marched; FAR_MODE selects marching or the stored field (which
+// then also holds the near block).  Norm always marches and writes W, and the near cache or
+// the stored field when they are allocated; Layout marches to size the field.
 template <Op OP, bool EXACT, int NEAR_MODE, int FAR_MODE>
 __global__ void __launch_bounds__(kBlock) project_kernel(const ProjParams p, const OpArgs a) {
-    extern __shared__ float near_sum[];
+    extern __shared__ __align__(128) unsigned char dyn_smem[];
+    __shared__ uint64_t field_bars[kWarps][kStages];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int group = blockIdx.x * kWarps + warp;
     if (group * kLanes >= p.n_active) return;  // the whole warp leaves together
@@ -184,9 +239,6 @@ __global__ void __launch_bounds__(kBlock) project_kernel(const ProjParams p, con
     if (!__any_sync(kFull, live)) return;
     const int nx = p.g.nx, ny = p.g.ny;
     const int vx = s % nx, vy = (s / nx) % ny, vz = s / p.nxy;
-    // Norm: W must sum exactly the weights later projections use, so stored bf16 weights are
-    // rounded before they are accumulated.
-    const bool near_bf16 = OP == Op::Norm && a.near.b16, far_bf16 = OP == Op::Norm && a.far.b16;
 
     auto deposit = [&](int t, float w) {
         if constexpr (OP == Op::Norm) acc += w;
@@ -195,46 +247,58 @@ __global__ void __launch_bounds__(kBlock) project_kernel(const ProjParams p, con
         else cnt += 1;
     };
 
-    // Near block (prc.cu:193-218).
-    if constexpr (OP != Op::Layout) {
-        float* sum = near_sum + warp * (kNear * kLanes);
-        if constexpr (NEAR_MODE == kTraceNear) {
-            for (int q = 0; q < kNear; ++q) sum[q * kLanes + lane] = 0.0f;
-            for (int r = 0; r < kNearRays; ++r) {
-                const RayStep R = p.near[r];
-                march<true, EXACT>(p, R, live, s, vx, vy, vz,
-                                   [&](int, float w, int q, int) { sum[q * kLanes + lane] += w; });
-            }
-        }
-        const size_t cache_base = (size_t)group * kNear * kLanes + lane;
-        const float near_scale = (float)p.n_rays / kNearRays;
-        for (int q = 0; q < kNear; ++q) {
-            const int dx = q % kNearSide - kNearR, dy = q / kNearSide % kNearSide - kNearR,
-                      dz = q / (kNearSide * kNearSide) - kNearR;
-            float w;
-            if constexpr (NEAR_MODE == kTraceNear) {
-                const bool in = (unsigned)(vx + dx) < (unsigned)nx && (unsigned)(vy + dy) < (unsigned)ny &&
-                                (unsigned)(vz + dz) < (unsigned)p.g.nz;
-                w = in ? sum[q * kLanes + lane] * near_scale : 0.0f;
-                if constexpr (OP == Op::Norm) {
-                    if (near_bf16) w = __bfloat162float(__float2bfloat16_rn(w));
-                    if (valid && a.near.b16) a.near.b16[cache_base + (size_t)q * kLanes] = __float2bfloat16_rn(w);
-                    if (valid && a.near.f32) a.near.f32[cache_base + (size_t)q * kLanes] = w;
-                }
-            } else if constexpr (NEAR_MODE == kCacheF32) {
-                w = live ? __ldg(a.near.f32 + cache_base + (size_t)q * kLanes) : 0.0f;
-            } else {
-                w = live ? __bfloat162float(a.near.b16[cache_base + (size_t)q * kLanes]) : 0.0f;
-            }
-            if (live && w > 0.0f) deposit(s + (dz * ny + dy) * nx + dx, w);
-        }
-    }
-
-    // Far field (prc.cu:220-226).
     if constexpr (FAR_MODE == kMarch) {
-        long long fbase = 0;  // Norm: element offset of this ray's field block, plus this lane's slot
-        if constexpr (OP == Op::Norm) {
-            if (a.far.on()) fbase = p.group_base[group] + lane * kPack;
+        const bool field = OP == Op::Norm && a.far.on();
+        const long long gbase = field ? p.group_base[group] : 0;
+        // Norm: W must sum exactly the weights later projections use, so stored bf16 weights
+        // are rounded before they are accumulated.
+        const bool near_round = OP == Op::Norm && (a.near.b16 || a.far.b16);
+        const bool far_round = OP == Op::Norm && a.far.b16;
+
+        // Near block (prc.cu:193-218).
+        if constexpr (OP != Op::Layout) {
+            float* sum = reinterpret_cast<float*>(dyn_smem) + warp * (kNear * kLanes);
+            if constexpr (NEAR_MODE == kTraceNear) {
+                for (int q = 0; q < kNear; ++q) sum[q * kLanes + lane] = 0.0f;
+                for (int r = 0; r < kNearRays; ++r) {
+                    const RayStep R = p.near[r];
+                    march<true, EXACT>(p, R, live, s, vx, vy, vz,
+                                       [&](int, float w, int q, int) { sum[q * kLanes + lane] += w; });
+                }
+            }
+            const size_t cache_base = (size_t)group * kNear * kLanes + lane;
+            const float near_scale = (float)p.n_rays / kNearRays;
+            for (int q = 0; q < kNear; ++q) {
+                const int dx = q % kNearSide - kNearR, dy = q / kNearSide % kNearSide - kNearR,
+                          dz = q / (kNearSide * kNearSide) - kNearR;
+                float w;
+                if constexpr (NEAR_MODE == kTraceNear) {
+                    const bool in = (unsigned)(vx + dx) < (unsigned)nx && (unsigned)(vy + dy) < (unsigned)ny &&
+                                    (unsigned)(vz + dz) < (unsigned)p.g.nz;
+                    w = in ? sum[q * kLanes + lane] * near_scale : 0.0f;
+                    if constexpr (OP == Op::Norm) {
+                        if (near_round) w = __bfloat162float(__float2bfloat16_rn(w));
+                        if (valid && a.near.b16) a.near.b16[cache_base + (size_t)q * kLanes] = __float2bfloat16_rn(w);
+                        if (valid && a.near.f32) a.near.f32[cache_base + (size_t)q * kLanes] = w;
+                        if (field && valid) {
+                            if (a.far.f32) store_weight<kFieldF32>(a.far, pack_slot(gbase, q, lane), w);
+                            else store_weight<kFieldBF16>(a.far, pack_slot(gbase, q, lane), w);
+                        }
+                    }
+                } else if constexpr (NEAR_MODE == kCacheF32) {
+                    w = live ? __ldg(a.near.f32 + cache_base + (size_t)q * kLanes) : 0.0f;
+                } else {
+                    w = live ? __bfloat162float(a.near.b16[cache_base + (size_t)q * kLanes]) : 0.0f;
+                }
+                if (live && w > 0.0f) deposit(s + (dz * ny + dy) * nx + dx, w);
+            }
+        }
+
+        // Far field (prc.cu:220-226).
+        long long rbase = gbase + (long long)kNearRow * kLanes;  // Norm: stream block of ray r
+        if constexpr (OP == Op::Layout) {
+            if (lane == 0) a.len[(size_t)group * p.n_rows] = kNearRow;
+            acc = (float)kNearRow;
         }
         for (int r = 0; r < p.n_rays; ++r) {
             const RayStep R = p.far[r];
@@ -242,59 +306,115 @@ __global__ void __launch_bounds__(kBlock) project_kernel(const ProjParams p, con
                 int last = -1;
                 march<false, EXACT>(p, R, live, s, vx, vy, vz, [&](int, float, int, int m) { last = m; });
                 const int L = (__reduce_max_sync(kFull, last + 1) + kPack - 1) / kPack * kPack;
-                if (lane == 0) a.len[(size_t)group * p.n_rays + r] = (unsigned short)L;
+                if (lane == 0) a.len[(size_t)group * p.n_rows + 1 + r] = (unsigned short)L;
                 acc += (float)L;  // exact: totals stay far below 2^24 per group
             } else if constexpr (OP == Op::Norm) {
-                const int L = a.far.on() ? (int)p.len[(size_t)group * p.n_rays + r] : 0;
                 march<false, EXACT>(p, R, live, s, vx, vy, vz, [&](int, float w, int, int m) {
-                    if (far_bf16) w = __bfloat162float(__float2bfloat16_rn(w));
+                    if (far_round) w = __bfloat162float(__float2bfloat16_rn(w));
                     acc += w;
-                    const long long e = fbase + (long long)(m / kPack) * (kPack * kLanes) + m % kPack;
-                    if (a.far.f32) a.far.f32[e] = w;
-                    else if (a.far.b16) a.far.b16[e] = __float2bfloat16_rn(w);
+                    if (field) {
+                        if (a.far.f32) store_weight<kFieldF32>(a.far, pack_slot(rbase, m, lane), w);
+                        else store_weight<kFieldBF16>(a.far, pack_slot(rbase, m, lane), w);
+                    }
                 });
-                fbase += (long long)L * kLanes;
+                if (field) rbase += (long long)p.len[(size_t)group * p.n_rows + 1 + r] * kLanes;
             } else {
                 march<false, EXACT>(p, R, live, s, vx, vy, vz, [&](int t, float w, int, int) { deposit(t, w); });
             }
         }
     } else {
-        // Stored field: the weights of one ray for the 32 lanes are one contiguous block of
-        // len * 32 entries, packed so that each lane reads kPack consecutive steps with one
-        // vector load (16 B fp32, 8 B bf16); target voxels are the source plus the template
-        // offsets, read as int4 broadcasts.  Eight steps are loaded before any is used.  The
-        // adjoint's gathers do not wait for the weights: their index is clamped into the volume
-        // and a zero weight discards the value.
-        const int4* tmpl4 = reinterpret_cast<const int4*>(p.tmpl);
-        const unsigned short* len = p.len + (size_t)group * p.n_rays;
-        long long fbase = p.group_base[group] + lane * kPack;
+        // Stored field, streamed by TMA.  Lane 0 keeps kStages bulk copies of kChunk bytes in
+        // flight into this warp's shared-memory ring (cp.async.bulk, completion counted by an
+        // mbarrier), so the weights arrive as contiguous DRAM bursts without holding
+        // registers.  For each chunk the warp first reads the packs' descriptors and template
+        // offsets, issues every gather of the chunk (adjoint; indices clamped into the volume,
+        // a zero weight discards the value), and only then consumes the weights.
+        constexpr int kElem = FAR_MODE == kFieldF32 ? 4 : 2;
+        constexpr int kPackBytes = kPack * kLanes * kElem;
+        constexpr int kPacksPerChunk = kChunk / kPackBytes;
+        unsigned char* ring = dyn_smem + (size_t)warp * kStages * kChunk;
+        uint64_t* bars = field_bars[warp];
+        const long long e0 = p.group_base[group], e1 = p.group_base[group + 1];
+        const char* src_bytes = (FAR_MODE == kFieldF32 ? reinterpret_cast<const char*>(a.far.f32)
+                                                       : reinterpret_cast<const char*>(a.far.b16)) + e0 * kElem;
+        const int* desc = p.desc + e0 / (kPack * kLanes);
+        const long long total = (e1 - e0) * kElem;
+        const int n_packs = (int)((e1 - e0) / (kPack * kLanes));
+        const int n_chunks = (n_packs + kPacksPerChunk - 1) / kPacksPerChunk;
+        auto issue = [&](int c) {  // lane 0 only
+            const int stage = c % kStages;
+            const unsigned bytes = (unsigned)min((long long)kChunk, total - (long long)c * kChunk);
+            mbar_expect_tx(&bars[stage], bytes);
+            bulk_copy_g2s(ring + stage * kChunk, src_bytes + (long long)c * kChunk, bytes, &bars[stage]);
+        };
+        if (lane == 0) {
+            for (int k = 0; k < kStages; ++k) mbar_init(&bars[k], 1);
+            fence_mbarrier_init();
+            for (int c = 0; c < n_chunks && c < kStages; ++c) issue(c);
+        }
+        __syncwarp();
         const int n_vox = p.nxy * p.g.nz;
-        for (int r = 0; r < p.n_rays; ++r, tmpl4 += p.tmpl_len / kPack) {
-            const int L = len[r];
-            for (int m = 0; m < L; m += 2 * kPack) {
-                const bool two = m + kPack < L;
-                float w[2 * kPack];
-                load_pack<FAR_MODE>(a.far, fbase + (long long)(m / kPack) * (kPack * kLanes), w);
-                if (two) load_pack<FAR_MODE>(a.far, fbase + (long long)(m / kPack + 1) * (kPack * kLanes), w + kPack);
-                else
+        bool ok = true;
+        for (int c = 0; c < n_chunks; ++c) {
+            const int packs = min(kPacksPerChunk, n_packs - c * kPacksPerChunk);
+            int o[kPacksPerChunk * kPack];
 #pragma unroll
-                    for (int u = kPack; u < 2 * kPack; ++u) w[u] = 0.0f;
-                const int4 oa = __ldg(tmpl4 + m / kPack);
-                const int4 ob = two ? __ldg(tmpl4 + m / kPack + 1) : make_int4(0, 0, 0, 0);
-                const int o[2 * kPack] = {oa.x, oa.y, oa.z, oa.w, ob.x, ob.y, ob.z, ob.w};
-                if constexpr (OP == Op::Adjoint) {
-                    float v[2 * kPack];
+            for (int k = 0; k < kPacksPerChunk; ++k) {
+                int4 t = make_int4(0, 0, 0, 0);
+                if (k < packs) t = __ldg(reinterpret_cast<const int4*>(p.tmpl + __ldg(desc + c * kPacksPerChunk + k)));
+                o[k * kPack] = t.x, o[k * kPack + 1] = t.y, o[k * kPack + 2] = t.z, o[k * kPack + 3] = t.w;
+            }
+            float v[kPacksPerChunk * kPack];
+            if constexpr (OP == Op::Adjoint) {
 #pragma unroll
-                    for (int u = 0; u < 2 * kPack; ++u) v[u] = __ldg(a.in + min(max(s + o[u], 0), n_vox - 1));
+                for (int u = 0; u < kPacksPerChunk * kPack; ++u) v[u] = __ldg(a.in + min(max(s + o[u], 0), n_vox - 1));
+            }
+            const int stage = c % kStages;
+            if (!mbar_wait_bounded(&bars[stage], (c / kStages) & 1)) {
+                ok = false;
+                break;
+            }
+            const unsigned char* chunk = ring + stage * kChunk;
 #pragma unroll
-                    for (int u = 0; u < 2 * kPack; ++u) acc += (live && w[u] > 0.0f) ? w[u] * v[u] : 0.0f;
-                } else {
+            for (int k = 0; k < kPacksPerChunk; ++k) {
+                if (k < packs) {
+                    float w[kPack];
+                    if constexpr (FAR_MODE == kFieldF32) {
+                        const float4 x = reinterpret_cast<const float4*>(chunk + k * kPackBytes)[lane];
+                        w[0] = x.x, w[1] = x.y, w[2] = x.z, w[3] = x.w;
+                    } else {
+                        const uint2 x = reinterpret_cast<const uint2*>(chunk + k * kPackBytes)[lane];
+                        w[0] = __uint_as_float(x.x << 16), w[1] = __uint_as_float(x.x & 0xffff0000u);
+                        w[2] = __uint_as_float(x.y << 16), w[3] = __uint_as_float(x.y & 0xffff0000u);
+                    }
 #pragma unroll
-                    for (int u = 0; u < 2 * kPack; ++u)
-                        if (live && w[u] > 0.0f) deposit(s + o[u], w[u]);
+                    for (int u = 0; u < kPack; ++u) {
+                        const float wu = w[u];
+                        if constexpr (OP == Op::Adjoint) {
+                            acc += (live && wu > 0.0f) ? wu * v[k * kPack + u] : 0.0f;
+                        } else {
+                            if (live && wu > 0.0f) deposit(s + o[k * kPack + u], wu);
+                        }
+                    }
                 }
             }
-            fbase += (long long)L * kLanes;
+            __syncwarp();
+            if (lane == 0 && c + kStages < n_chunks) {
+                fence_proxy_async();  // this stage's reads precede the copy that overwrites it
+                issue(c + kStages);
+            }
+        }
+        if (!ok) {
+            // A copy did not complete in time: report it, and give the copies still in flight
+            // a bounded chance to land before this warp's shared memory is released.
+            if (lane == 0) {
+                atomicOr(a.error, 1u);
+                for (int k = 0; k < kStages; ++k) {
+                    mbar_wait_bounded(&bars[k], 0);
+                    mbar_wait_bounded(&bars[k], 1);
+                }
+            }
+            __syncwarp();
         }
     }
 
@@ -310,15 +430,17 @@ __global__ void __launch_bounds__(kBlock) project_kernel(const ProjParams p, con
     }
 }
 
-// Ray template: the linear offsets of the post-block steps of each far ray, from the same
-// uniform DDA the march performs.
+// Template rows: row 0 the near block's 125 offsets (then zeros), rows 1..n_rays the offsets of
+// the post-block steps of each far ray, from the same uniform DDA the march performs.
 __global__ void template_kernel(const ProjParams p, int* tmpl) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r == 0)
+        for (int q = 0; q < p.tmpl_len; ++q) tmpl[q] = q < kNear ? near_offset(p, q) : 0;
     if (r >= p.n_rays) return;
     const RayStep R = p.far[r];
     float tx = R.tx, ty = R.ty, tz = R.tz;
     int oi = 0, oj = 0, ok = 0, m = 0;
-    int* out = tmpl + (size_t)r * p.tmpl_len;
+    int* out = tmpl + (size_t)(r + 1) * p.tmpl_len;
     for (int step = 0; m < p.tmpl_len && step < 4 * p.tmpl_len; ++step) {
         const bool in_block = abs(oi) <= kNearR && abs(oj) <= kNearR && abs(ok) <= kNearR;
         if (!in_block) out[m++] = (ok * p.g.ny + oj) * p.g.nx + oi;
@@ -329,12 +451,24 @@ __global__ void template_kernel(const ProjParams p, int* tmpl) {
     }
 }
 
+// Pack descriptors of every group: the template element offset of each pack's first step.
+__global__ void desc_kernel(const ProjParams p, int* desc) {
+    const int group = blockIdx.x * blockDim.x + threadIdx.x;
+    if (group * kLanes >= p.n_active) return;
+    const unsigned short* len = p.len + (size_t)group * p.n_rows;
+    int* out = desc + p.group_base[group] / (kPack * kLanes);
+    for (int row = 0; row < p.n_rows; ++row)
+        for (int m = 0; m < len[row]; m += kPack) *out++ = row * p.tmpl_len + m;
+}
+
 template <Op OP, bool EXACT, int NEAR_MODE, int FAR_MODE>
 cudaError_t launch(const ProjParams& p, const OpArgs& a, cudaStream_t s) {
     const int groups = (p.n_active + kLanes - 1) / kLanes;
     const int blocks = (groups + kWarps - 1) / kWarps;
     if (blocks == 0) return cudaSuccess;
-    const size_t smem = NEAR_MODE == kTraceNear && OP != Op::Layout ? kNearSmemBytes : 0;
+    size_t smem = 0;
+    if (FAR_MODE != kMarch) smem = kFieldSmemBytes;
+    else if (NEAR_MODE == kTraceNear && OP != Op::Layout) smem = kNearSmemBytes;
     auto kernel = project_kernel<OP, EXACT, NEAR_MODE, FAR_MODE>;
     if (smem > 48 * 1024) {
         const cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -351,18 +485,10 @@ cudaError_t launch_modes(const ProjParams& p, const OpArgs& a, bool trace_near, 
             return a.near.b16 ? launch<OP, EXACT, kCacheBF16, kMarch>(p, a, s) : launch<OP, EXACT, kCacheF32, kMarch>(p, a, s);
         return launch<OP, EXACT, kTraceNear, kMarch>(p, a, s);
     } else {
-        if (trace_near || !a.near.on()) {
-            if (a.far.f32) return launch<OP, EXACT, kTraceNear, kFieldF32>(p, a, s);
-            if (a.far.b16) return launch<OP, EXACT, kTraceNear, kFieldBF16>(p, a, s);
-            return launch<OP, EXACT, kTraceNear, kMarch>(p, a, s);
-        }
-        if (a.near.b16) {
-            if (a.far.b16) return launch<OP, EXACT, kCacheBF16, kFieldBF16>(p, a, s);
-            if (a.far.f32) return launch<OP, EXACT, kCacheBF16, kFieldF32>(p, a, s);
-            return launch<OP, EXACT, kCacheBF16, kMarch>(p, a, s);
-        }
-        if (a.far.f32) return launch<OP, EXACT, kCacheF32, kFieldF32>(p, a, s);
-        if (a.far.b16) return launch<OP, EXACT, kCacheF32, kFieldBF16>(p, a, s);
+        if (a.far.f32) return launch<OP, EXACT, kTraceNear, kFieldF32>(p, a, s);
+        if (a.far.b16) return launch<OP, EXACT, kTraceNear, kFieldBF16>(p, a, s);
+        if (trace_near || !a.near.on()) return launch<OP, EXACT, kTraceNear, kMarch>(p, a, s);
+        if (a.near.b16) return launch<OP, EXACT, kCacheBF16, kMarch>(p, a, s);
         return launch<OP, EXACT, kCacheF32, kMarch>(p, a, s);
     }
 }
@@ -381,9 +507,18 @@ cudaError_t setup_rays(const Grid& g, int n_rays, RayStep* d_far, RayStep* d_nea
 }
 
 cudaError_t build_template(const ProjParams& p, int* tmpl, cudaStream_t s) {
-    template_kernel<<<(p.n_rays + 127) / 128, 128, 0, s>>>(p, tmpl);
+    template_kernel<<<(p.n_rays + 128) / 128, 128, 0, s>>>(p, tmpl);
     return cudaGetLastError();
 }
+
+cudaError_t build_descriptors(const ProjParams& p, int* desc, cudaStream_t s) {
+    const int groups = (p.n_active + kLanes - 1) / kLanes;
+    if (groups == 0) return cudaSuccess;
+    desc_kernel<<<(groups + 127) / 128, 128, 0, s>>>(p, desc);
+    return cudaGetLastError();
+}
+
+int near_row_steps() { return kNearRow; }
 
 cudaError_t project(Op op, const ProjParams& p, const OpArgs& a, bool trace_near, cudaStream_t s) {
     switch (op) {
