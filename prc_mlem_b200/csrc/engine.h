@@ -21,6 +21,13 @@ struct RayStep {
     int pad;
 };
 
+// Layout of a stored field stream (see FarField).
+struct StreamLayout {
+    const unsigned short* len = nullptr;    // [n_groups][n_rows]: stored steps of row k in group G
+    const long long* group_base = nullptr;  // [n_groups + 1]: element offset of group G's stream
+    const int* desc = nullptr;              // per pack: template element offset of its first step
+};
+
 // Everything a projector kernel needs to know about one volume.
 struct ProjParams {
     Grid g;
@@ -41,15 +48,17 @@ struct ProjParams {
                                      // far ray r (the same for every source)
     int tmpl_len;                    // steps per row: covers every step a ray takes in the image
     int n_rows;                      // n_rays + 1
-    const unsigned short* len;       // [n_groups][n_rows]: stored steps of row k in group G
-    const long long* group_base;     // [n_groups + 1]: element offset of group G's stream
-    const int* desc;                 // per pack: template element offset of its first step
+    StreamLayout src;                // source-major field: group = 32 consecutive sources
+    StreamLayout tgt;                // target-major field: group = 32 consecutive targets
+    const int* vox2src;              // voxel -> source index, -1 off the support
 };
 
 // Stored weights ("coefficient field") of near block and far rays: for group G, template row k,
 // step m and lane l, the entry group_base[G] + (sum_{k'<k} len[G][k']) * 32 + (m / 4) * 128 +
-// l * 4 + m % 4.  Target voxels come from the template, so no index is stored; forward and
-// adjoint read the same field.
+// l * 4 + m % 4.  Target voxels come from the template, so no index is stored.  The
+// source-major field (lane = source s, target s + o) serves the adjoint as a gather; the
+// target-major copy of the same weights (lane = target t, source t - o) serves the forward as a
+// gather of u = f / W.
 struct FarField {
     float* f32 = nullptr;
     __nv_bfloat16* b16 = nullptr;
@@ -78,12 +87,21 @@ struct OpArgs {
     float* out = nullptr;
     float* W = nullptr;
     NearCache near;
-    FarField far;
+    FarField far;                          // source-major stored field
+    FarField farT;                         // target-major stored field (forward as a gather)
     unsigned long long* count = nullptr;
     unsigned int* error = nullptr;         // set non-zero when a stored-field copy timed out
     unsigned short* len = nullptr;         // Layout output
     long long* group_total = nullptr;      // Layout output: entries per group (sum of len * 32)
 };
+
+// Target-major field construction (setup only).
+cudaError_t transpose_lengths(const ProjParams& p, const FarField& far, int* len_t32, cudaStream_t s);
+cudaError_t transpose_fill(const ProjParams& p, const FarField& far, const FarField& farT, const int* row_base_t,
+                           cudaStream_t s);
+// u = f / W on the support (0 where that is not positive, as prc.cu:244-248 skips the source)
+// and out = 0 off the support: the input of the gather form of the forward projection.
+cudaError_t forward_prep(const ProjParams& p, const float* W, const float* f, float* u, float* out, cudaStream_t s);
 
 // projector.cu
 cudaError_t setup_rays(const Grid& g, int n_rays, RayStep* d_far, RayStep* d_near, cudaStream_t s);
@@ -92,8 +110,8 @@ cudaError_t setup_rays(const Grid& g, int n_rays, RayStep* d_far, RayStep* d_nea
 cudaError_t project(Op op, const ProjParams& p, const OpArgs& a, bool trace_near, cudaStream_t s);
 // Fills the template p.tmpl ([n_rows][tmpl_len] ints).
 cudaError_t build_template(const ProjParams& p, int* tmpl, cudaStream_t s);
-// Fills the pack descriptors (one int per 128 stored entries) from p.len and p.group_base.
-cudaError_t build_descriptors(const ProjParams& p, int* desc, cudaStream_t s);
+// Fills the pack descriptors (one int per 128 stored entries) of a stream layout.
+cudaError_t build_descriptors(const ProjParams& p, const StreamLayout& l, int* desc, cudaStream_t s);
 // Stored steps of the near-block row (125 offsets padded to whole packs).
 int near_row_steps();
 

@@ -59,6 +59,14 @@ struct prc_handle {
     long long* group_base = nullptr;
     long long* group_total = nullptr;
     int* desc = nullptr;
+    // target-major copy of the field (forward projection as a gather)
+    FarField far_t;
+    unsigned short* len_t = nullptr;
+    long long* group_base_t = nullptr;
+    int* desc_t = nullptr;
+    int* vox2src = nullptr;
+    float* u = nullptr;  // f / W volume for the gather form of the forward projection
+    int64_t far_t_entries = 0;
     int64_t far_entries = 0;
     int cache_mode = PRC_CACHE_NONE;
     bool trace_near = false;
@@ -99,6 +107,7 @@ struct prc_handle {
         a.W = W;
         a.near = cache;
         a.far = far_field;
+        a.farT = far_t;
         a.error = error;
         return a;
     }
@@ -147,6 +156,78 @@ void prc_destroy(prc_handle* h) {
     for (void* p : h->allocations) cudaFree(p);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
+}
+
+// The target-major copy of the stored field: per target group and template row, the longest
+// step any contributing source reaches, prefix sums, then a copy of every weight.  Optional:
+// without it (not enough memory) the forward projection scatters with atomics instead.
+static int build_target_major(prc_handle* h, const std::vector<int>& active, size_t elem) {
+    ProjParams& p = h->params;
+    const size_t rows = (size_t)h->n_groups * p.n_rows;
+    std::vector<int> v2s(h->n, -1);
+    for (size_t i = 0; i < active.size(); ++i) v2s[active[i]] = (int)i;
+    PRC_CUDA(h->alloc(&h->vox2src, h->n));
+    PRC_CUDA(cudaMemcpyAsync(h->vox2src, v2s.data(), h->n * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+    p.vox2src = h->vox2src;
+    int* len32 = nullptr;
+    PRC_CUDA(cudaMalloc(&len32, rows * sizeof(int)));
+    struct Free {
+        int* p;
+        ~Free() { cudaFree(p); }
+    } free_len32{len32};
+    PRC_CUDA(cudaMemsetAsync(len32, 0, rows * sizeof(int), h->stream));
+    PRC_CUDA(transpose_lengths(p, h->far_field, len32, h->stream));
+    std::vector<int> l32(rows);
+    PRC_CUDA(cudaMemcpyAsync(l32.data(), len32, rows * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    PRC_CUDA(cudaStreamSynchronize(h->stream));
+    std::vector<unsigned short> lt(rows);
+    std::vector<int> row_base(rows);
+    std::vector<long long> gbase(h->n_groups + 1);
+    long long run = 0;
+    for (int g = 0; g < h->n_groups; ++g) {
+        gbase[g] = run;
+        int within = 0;
+        for (int k = 0; k < p.n_rows; ++k) {
+            const size_t i = (size_t)g * p.n_rows + k;
+            const int L = (l32[i] + 3) / 4 * 4;
+            lt[i] = (unsigned short)L;
+            row_base[i] = within;
+            within += L * kLanes;
+        }
+        run += within;
+    }
+    gbase[h->n_groups] = run;
+    size_t free_b = 0, total_b = 0;
+    PRC_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    const size_t desc_count = (size_t)(run / (4 * kLanes));
+    // keep room for the MAP-EM volumes and the transient row offsets
+    if ((size_t)run * elem + desc_count * 4 + rows * 6 + 16 * h->n * 4 > free_b) return PRC_OK;
+    const bool bf16 = elem == 2;
+    cudaError_t e = bf16 ? h->alloc(&h->far_t.b16, (size_t)run) : h->alloc(&h->far_t.f32, (size_t)run);
+    if (e == cudaSuccess) e = h->alloc(&h->desc_t, desc_count);
+    if (e == cudaSuccess) e = h->alloc(&h->len_t, rows);
+    if (e == cudaSuccess) e = h->alloc(&h->group_base_t, (size_t)h->n_groups + 1);
+    if (e == cudaSuccess) e = h->alloc(&h->u, h->n);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        h->far_t = FarField{};
+        return PRC_OK;  // the forward keeps its scatter form
+    }
+    int* d_row_base = nullptr;
+    PRC_CUDA(cudaMalloc(&d_row_base, rows * sizeof(int)));
+    Free free_rb{d_row_base};
+    PRC_CUDA(cudaMemcpyAsync(h->len_t, lt.data(), rows * sizeof(unsigned short), cudaMemcpyHostToDevice, h->stream));
+    PRC_CUDA(cudaMemcpyAsync(h->group_base_t, gbase.data(), gbase.size() * sizeof(long long), cudaMemcpyHostToDevice,
+                             h->stream));
+    PRC_CUDA(cudaMemcpyAsync(d_row_base, row_base.data(), rows * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+    p.tgt.len = h->len_t;
+    p.tgt.group_base = h->group_base_t;
+    PRC_CUDA(build_descriptors(p, p.tgt, h->desc_t, h->stream));
+    p.tgt.desc = h->desc_t;
+    PRC_CUDA(transpose_fill(p, h->far_field, h->far_t, d_row_base, h->stream));
+    PRC_CUDA(cudaStreamSynchronize(h->stream));
+    h->far_t_entries = run;
+    return PRC_OK;
 }
 
 static int create_impl(prc_handle* h, const float* density_host) {
@@ -248,10 +329,10 @@ static int create_impl(prc_handle* h, const float* density_host) {
             if (e == cudaSuccess) {
                 PRC_CUDA(cudaMemcpyAsync(h->group_base, totals.data(), totals.size() * sizeof(long long),
                                          cudaMemcpyHostToDevice, h->stream));
-                p.len = h->len;
-                p.group_base = h->group_base;
-                PRC_CUDA(build_descriptors(p, h->desc, h->stream));
-                p.desc = h->desc;
+                p.src.len = h->len;
+                p.src.group_base = h->group_base;
+                PRC_CUDA(build_descriptors(p, p.src, h->desc, h->stream));
+                p.src.desc = h->desc;
                 h->far_entries = run;
                 h->cache_mode = PRC_CACHE_FULL;
                 h->trace_near = false;
@@ -273,6 +354,10 @@ static int create_impl(prc_handle* h, const float* density_host) {
     }
     OpArgs a = h->op_args();
     PRC_CUDA(project(Op::Norm, p, a, true, h->stream));
+    if (h->cache_mode == PRC_CACHE_FULL) {
+        const int rc = build_target_major(h, active, elem);
+        if (rc != PRC_OK) return rc;
+    }
     PRC_CUDA(cudaStreamSynchronize(h->stream));
     return check_device_error(h);
 }
@@ -317,7 +402,7 @@ int prc_create(const prc_geometry* geo, const char* isotope, const prc_options* 
 int prc_cache_mode(const prc_handle* h, int* mode, int64_t* far_entries) {
     if (!h) return fail(PRC_ERR_ARGUMENT, "Invalid argument");
     if (mode) *mode = h->cache_mode;
-    if (far_entries) *far_entries = h->far_entries;
+    if (far_entries) *far_entries = h->far_entries + h->far_t_entries;
     return PRC_OK;
 }
 
@@ -344,10 +429,16 @@ void* prc_stream(const prc_handle* h) { return h ? (void*)h->stream : nullptr; }
 int prc_forward(prc_handle* h, const float* d_in, float* d_out, void* stream) {
     if (!h || !d_in || !d_out) return fail(PRC_ERR_ARGUMENT, "Invalid argument");
     const cudaStream_t s = h->pick(stream);
-    PRC_CUDA(cudaMemsetAsync(d_out, 0, h->n * sizeof(float), s));
     OpArgs a = h->op_args();
     a.in = d_in;
     a.out = d_out;
+    if (h->far_t.on()) {  // gather form: u = f / W, then out[t] = sum_k T_tk u[t - o_k]
+        PRC_CUDA(forward_prep(h->params, h->W, d_in, h->u, d_out, s));
+        a.in = h->u;
+        PRC_CUDA(project(Op::Forward, h->params, a, h->trace_near, s));
+        return PRC_OK;
+    }
+    PRC_CUDA(cudaMemsetAsync(d_out, 0, h->n * sizeof(float), s));
     PRC_CUDA(project(Op::Forward, h->params, a, h->trace_near, s));
     return PRC_OK;
 }

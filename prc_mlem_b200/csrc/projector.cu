@@ -152,8 +152,14 @@ enum FarMode : int { kMarch = 0, kFieldF32 = 1, kFieldBF16 = 2 };
 constexpr int kPack = 4;
 constexpr int kNearRow = 128;  // 125 block offsets rounded up to whole packs
 // TMA ring of the field stream: kStages chunks of kChunk bytes per warp.
-constexpr int kStages = 4;
-constexpr int kChunk = 2048;
+#ifndef PRC_FIELD_STAGES
+#define PRC_FIELD_STAGES 2
+#endif
+#ifndef PRC_FIELD_CHUNK
+#define PRC_FIELD_CHUNK 2048
+#endif
+constexpr int kStages = PRC_FIELD_STAGES;
+constexpr int kChunk = PRC_FIELD_CHUNK;
 constexpr size_t kFieldSmemBytes = size_t(kWarps) * kStages * kChunk;
 // try_wait rounds before a field copy is declared lost (each round is a bounded hardware wait).
 constexpr int kWaitRounds = 1 << 20;
@@ -228,9 +234,13 @@ __global__ void __launch_bounds__(kBlock) project_kernel(const ProjParams p, con
     float scale = 0.0f, acc = 0.0f;
     unsigned long long cnt = 0;
     if constexpr (OP == Op::Forward) {  // prc.cu:244-248
-        const float fs = valid ? __ldg(a.in + s) : 0.0f, ws = valid ? __ldg(a.W + src) : 0.0f;
-        scale = ws > 0.0f ? fs / ws : 0.0f;
-        live = valid && scale > 0.0f;
+        if (FAR_MODE != kMarch && a.farT.on()) {
+            live = valid;  // gather form: lanes are targets, a.in holds u = f / W
+        } else {
+            const float fs = valid ? __ldg(a.in + s) : 0.0f, ws = valid ? __ldg(a.W + src) : 0.0f;
+            scale = ws > 0.0f ? fs / ws : 0.0f;
+            live = valid && scale > 0.0f;
+        }
     } else if constexpr (OP == Op::Adjoint) {  // prc.cu:260-264
         const float ws = valid ? __ldg(a.W + src) : 0.0f;
         live = valid && ws > 0.0f;
@@ -249,7 +259,7 @@ __global__ void __launch_bounds__(kBlock) project_kernel(const ProjParams p, con
 
     if constexpr (FAR_MODE == kMarch) {
         const bool field = OP == Op::Norm && a.far.on();
-        const long long gbase = field ? p.group_base[group] : 0;
+        const long long gbase = field ? p.src.group_base[group] : 0;
         // Norm: W must sum exactly the weights later projections use, so stored bf16 weights
         // are rounded before they are accumulated.
         const bool near_round = OP == Op::Norm && (a.near.b16 || a.far.b16);
@@ -317,7 +327,7 @@ __global__ void __launch_bounds__(kBlock) project_kernel(const ProjParams p, con
                         else store_weight<kFieldBF16>(a.far, pack_slot(rbase, m, lane), w);
                     }
                 });
-                if (field) rbase += (long long)p.len[(size_t)group * p.n_rows + 1 + r] * kLanes;
+                if (field) rbase += (long long)p.src.len[(size_t)group * p.n_rows + 1 + r] * kLanes;
             } else {
                 march<false, EXACT>(p, R, live, s, vx, vy, vz, [&](int t, float w, int, int) { deposit(t, w); });
             }
@@ -329,15 +339,22 @@ __global__ void __launch_bounds__(kBlock) project_kernel(const ProjParams p, con
         // registers.  For each chunk the warp first reads the packs' descriptors and template
         // offsets, issues every gather of the chunk (adjoint; indices clamped into the volume,
         // a zero weight discards the value), and only then consumes the weights.
+        // The forward gathers u = f / W over the target-major copy when it exists (lane = target,
+        // source = target - offset); otherwise it scatters over the source-major field.
         constexpr int kElem = FAR_MODE == kFieldF32 ? 4 : 2;
         constexpr int kPackBytes = kPack * kLanes * kElem;
         constexpr int kPacksPerChunk = kChunk / kPackBytes;
+        const bool gather = OP == Op::Adjoint || (OP == Op::Forward && a.farT.on());
+        const bool transposed = OP == Op::Forward && a.farT.on();
+        const StreamLayout& lay = transposed ? p.tgt : p.src;
+        const FarField& fld = transposed ? a.farT : a.far;
+        const int sign = transposed ? -1 : 1;
         unsigned char* ring = dyn_smem + (size_t)warp * kStages * kChunk;
         uint64_t* bars = field_bars[warp];
-        const long long e0 = p.group_base[group], e1 = p.group_base[group + 1];
-        const char* src_bytes = (FAR_MODE == kFieldF32 ? reinterpret_cast<const char*>(a.far.f32)
-                                                       : reinterpret_cast<const char*>(a.far.b16)) + e0 * kElem;
-        const int* desc = p.desc + e0 / (kPack * kLanes);
+        const long long e0 = lay.group_base[group], e1 = lay.group_base[group + 1];
+        const char* src_bytes = (FAR_MODE == kFieldF32 ? reinterpret_cast<const char*>(fld.f32)
+                                                       : reinterpret_cast<const char*>(fld.b16)) + e0 * kElem;
+        const int* desc = lay.desc + e0 / (kPack * kLanes);
         const long long total = (e1 - e0) * kElem;
         const int n_packs = (int)((e1 - e0) / (kPack * kLanes));
         const int n_chunks = (n_packs + kPacksPerChunk - 1) / kPacksPerChunk;
@@ -353,7 +370,6 @@ __global__ void __launch_bounds__(kBlock) project_kernel(const ProjParams p, con
             for (int c = 0; c < n_chunks && c < kStages; ++c) issue(c);
         }
         __syncwarp();
-        const int n_vox = p.nxy * p.g.nz;
         bool ok = true;
         for (int c = 0; c < n_chunks; ++c) {
             const int packs = min(kPacksPerChunk, n_packs - c * kPacksPerChunk);
@@ -364,39 +380,42 @@ __global__ void __launch_bounds__(kBlock) project_kernel(const ProjParams p, con
                 if (k < packs) t = __ldg(reinterpret_cast<const int4*>(p.tmpl + __ldg(desc + c * kPacksPerChunk + k)));
                 o[k * kPack] = t.x, o[k * kPack + 1] = t.y, o[k * kPack + 2] = t.z, o[k * kPack + 3] = t.w;
             }
-            float v[kPacksPerChunk * kPack];
-            if constexpr (OP == Op::Adjoint) {
-#pragma unroll
-                for (int u = 0; u < kPacksPerChunk * kPack; ++u) v[u] = __ldg(a.in + min(max(s + o[u], 0), n_vox - 1));
-            }
             const int stage = c % kStages;
             if (!mbar_wait_bounded(&bars[stage], (c / kStages) & 1)) {
                 ok = false;
                 break;
             }
+            // weights of the chunk from shared memory; packs beyond the stream end read as 0
             const unsigned char* chunk = ring + stage * kChunk;
+            float w[kPacksPerChunk * kPack];
 #pragma unroll
             for (int k = 0; k < kPacksPerChunk; ++k) {
                 if (k < packs) {
-                    float w[kPack];
                     if constexpr (FAR_MODE == kFieldF32) {
                         const float4 x = reinterpret_cast<const float4*>(chunk + k * kPackBytes)[lane];
-                        w[0] = x.x, w[1] = x.y, w[2] = x.z, w[3] = x.w;
+                        w[k * kPack] = x.x, w[k * kPack + 1] = x.y, w[k * kPack + 2] = x.z, w[k * kPack + 3] = x.w;
                     } else {
                         const uint2 x = reinterpret_cast<const uint2*>(chunk + k * kPackBytes)[lane];
-                        w[0] = __uint_as_float(x.x << 16), w[1] = __uint_as_float(x.x & 0xffff0000u);
-                        w[2] = __uint_as_float(x.y << 16), w[3] = __uint_as_float(x.y & 0xffff0000u);
+                        w[k * kPack] = __uint_as_float(x.x << 16), w[k * kPack + 1] = __uint_as_float(x.x & 0xffff0000u);
+                        w[k * kPack + 2] = __uint_as_float(x.y << 16), w[k * kPack + 3] = __uint_as_float(x.y & 0xffff0000u);
                     }
+                } else {
 #pragma unroll
-                    for (int u = 0; u < kPack; ++u) {
-                        const float wu = w[u];
-                        if constexpr (OP == Op::Adjoint) {
-                            acc += (live && wu > 0.0f) ? wu * v[k * kPack + u] : 0.0f;
-                        } else {
-                            if (live && wu > 0.0f) deposit(s + o[k * kPack + u], wu);
-                        }
-                    }
+                    for (int u = 0; u < kPack; ++u) w[k * kPack + u] = 0.0f;
                 }
+            }
+            if (gather) {
+                // Only lanes with a deposit load: zero-padded steps cost no memory traffic.
+                float v[kPacksPerChunk * kPack];
+#pragma unroll
+                for (int u = 0; u < kPacksPerChunk * kPack; ++u)
+                    v[u] = (live && w[u] > 0.0f) ? __ldg(a.in + s + sign * o[u]) : 0.0f;
+#pragma unroll
+                for (int u = 0; u < kPacksPerChunk * kPack; ++u) acc += w[u] * v[u];
+            } else {
+#pragma unroll
+                for (int u = 0; u < kPacksPerChunk * kPack; ++u)
+                    if (live && w[u] > 0.0f) deposit(s + o[u], w[u]);
             }
             __syncwarp();
             if (lane == 0 && c + kStages < n_chunks) {
@@ -424,6 +443,8 @@ __global__ void __launch_bounds__(kBlock) project_kernel(const ProjParams p, con
         if (lane == 0) a.group_total[group] = (long long)acc * kLanes;
     } else if constexpr (OP == Op::Adjoint) {
         if (live) a.out[s] = acc / __ldg(a.W + src);  // prc.cu:266
+    } else if constexpr (OP == Op::Forward) {
+        if (FAR_MODE != kMarch && a.farT.on() && valid) a.out[s] = acc;
     } else if constexpr (OP == Op::Count) {
         for (int off = 16; off > 0; off >>= 1) cnt += __shfl_xor_sync(kFull, cnt, off);
         if (lane == 0) atomicAdd(a.count, cnt);
@@ -452,13 +473,69 @@ __global__ void template_kernel(const ProjParams p, int* tmpl) {
 }
 
 // Pack descriptors of every group: the template element offset of each pack's first step.
-__global__ void desc_kernel(const ProjParams p, int* desc) {
+__global__ void desc_kernel(const ProjParams p, const StreamLayout l, int* desc) {
     const int group = blockIdx.x * blockDim.x + threadIdx.x;
     if (group * kLanes >= p.n_active) return;
-    const unsigned short* len = p.len + (size_t)group * p.n_rows;
-    int* out = desc + p.group_base[group] / (kPack * kLanes);
+    const unsigned short* len = l.len + (size_t)group * p.n_rows;
+    int* out = desc + l.group_base[group] / (kPack * kLanes);
     for (int row = 0; row < p.n_rows; ++row)
         for (int m = 0; m < len[row]; m += kPack) *out++ = row * p.tmpl_len + m;
+}
+
+// Walks every stored source-major entry w > 0 of a group (lane = source s, template row k,
+// step m, target t = s + o).  FILL = false: raises len_t32[group(t)][k] to cover step m.
+// FILL = true: copies w into the target-major field at (group(t), row k, step m, lane(t)).
+template <bool FILL, int FAR_MODE>
+__global__ void __launch_bounds__(kBlock) transpose_kernel(const ProjParams p, const FarField far, const FarField farT,
+                                                           int* len_t32, const int* row_base_t) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int group = blockIdx.x * kWarps + warp;
+    if (group * kLanes >= p.n_active) return;
+    const int src = group * kLanes + lane;
+    const bool valid = src < p.n_active;
+    const int s = valid ? p.active[src] : 0;
+    const unsigned short* len = p.src.len + (size_t)group * p.n_rows;
+    long long row_base = p.src.group_base[group];
+    for (int k = 0; k < p.n_rows; ++k) {
+        const int L = len[k];
+        for (int m = 0; m < L; ++m) {
+            const long long e = pack_slot(row_base, m, lane);
+            float w = 0.0f;
+            if (valid) w = FAR_MODE == kFieldF32 ? far.f32[e] : __bfloat162float(far.b16[e]);
+            const bool dep = valid && w > 0.0f;
+            int tsrc = -1;
+            if (dep) tsrc = p.vox2src[s + p.tmpl[(size_t)k * p.tmpl_len + m]];
+            if constexpr (!FILL) {
+                const int key = dep ? (tsrc >> 5) : -1;
+                const unsigned same = __match_any_sync(kFull, key);
+                if (dep && lane == __ffs(same) - 1) atomicMax(len_t32 + (size_t)key * p.n_rows + k, m + 1);
+            } else {
+                if (dep) {
+                    const int tg = tsrc >> 5, tl = tsrc & 31;
+                    const long long et = pack_slot(p.tgt.group_base[tg] + row_base_t[(size_t)tg * p.n_rows + k], m, tl);
+                    if constexpr (FAR_MODE == kFieldF32) farT.f32[et] = far.f32[e];
+                    else farT.b16[et] = far.b16[e];
+                }
+            }
+        }
+        row_base += (long long)L * kLanes;
+    }
+}
+
+__global__ void forward_prep_kernel(const int* __restrict__ vox2src, const float* __restrict__ W,
+                                    const float* __restrict__ f, float* __restrict__ u, float* __restrict__ out,
+                                    size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const int src = vox2src[i];
+        float scale = 0.0f;
+        if (src >= 0) {
+            const float ws = W[src], fs = f[i];
+            scale = ws > 0.0f ? fs / ws : 0.0f;  // prc.cu:246
+        } else {
+            out[i] = 0.0f;
+        }
+        u[i] = scale > 0.0f ? scale : 0.0f;
+    }
 }
 
 template <Op OP, bool EXACT, int NEAR_MODE, int FAR_MODE>
@@ -511,10 +588,33 @@ cudaError_t build_template(const ProjParams& p, int* tmpl, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-cudaError_t build_descriptors(const ProjParams& p, int* desc, cudaStream_t s) {
+cudaError_t build_descriptors(const ProjParams& p, const StreamLayout& l, int* desc, cudaStream_t s) {
     const int groups = (p.n_active + kLanes - 1) / kLanes;
     if (groups == 0) return cudaSuccess;
-    desc_kernel<<<(groups + 127) / 128, 128, 0, s>>>(p, desc);
+    desc_kernel<<<(groups + 127) / 128, 128, 0, s>>>(p, l, desc);
+    return cudaGetLastError();
+}
+
+cudaError_t transpose_lengths(const ProjParams& p, const FarField& far, int* len_t32, cudaStream_t s) {
+    const int groups = (p.n_active + kLanes - 1) / kLanes;
+    if (groups == 0) return cudaSuccess;
+    if (far.f32) transpose_kernel<false, kFieldF32><<<(groups + kWarps - 1) / kWarps, kBlock, 0, s>>>(p, far, FarField{}, len_t32, nullptr);
+    else transpose_kernel<false, kFieldBF16><<<(groups + kWarps - 1) / kWarps, kBlock, 0, s>>>(p, far, FarField{}, len_t32, nullptr);
+    return cudaGetLastError();
+}
+
+cudaError_t transpose_fill(const ProjParams& p, const FarField& far, const FarField& farT, const int* row_base_t,
+                           cudaStream_t s) {
+    const int groups = (p.n_active + kLanes - 1) / kLanes;
+    if (groups == 0) return cudaSuccess;
+    if (far.f32) transpose_kernel<true, kFieldF32><<<(groups + kWarps - 1) / kWarps, kBlock, 0, s>>>(p, far, farT, nullptr, row_base_t);
+    else transpose_kernel<true, kFieldBF16><<<(groups + kWarps - 1) / kWarps, kBlock, 0, s>>>(p, far, farT, nullptr, row_base_t);
+    return cudaGetLastError();
+}
+
+cudaError_t forward_prep(const ProjParams& p, const float* W, const float* f, float* u, float* out, cudaStream_t s) {
+    const size_t n = (size_t)p.nxy * p.g.nz;
+    forward_prep_kernel<<<592, 256, 0, s>>>(p.vox2src, W, f, u, out, n);
     return cudaGetLastError();
 }
 
