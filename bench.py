@@ -54,6 +54,8 @@ def parse():
     ap.add_argument("--no-forms", action="store_true", help="skip the per-form comparison")
     ap.add_argument("--ops", type=int, default=0,
                     help="only run this many forward+adjoint pairs of the headline form (profiling)")
+    ap.add_argument("--form", choices=("fp32", "bf16", "traced"), default="fp32",
+                    help="projector form of the headline number (default: plain fp32 stored field)")
     return ap.parse_args()
 
 
@@ -132,15 +134,24 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def ncu_traffic(kernel_key: str):
-    """Per-launch DRAM bytes of the headline kernel from the committed ncu summary, if any."""
+FORMS = {"fp32": (2, 0), "bf16": (2, 1), "traced": (1, 0)}  # (PRC_CACHE_*, PRC_PRECISION_*)
+
+
+def ncu_traffic(kernel_key: str, stored_bytes: float):
+    """Per-launch DRAM bytes of the headline kernel, from the committed ncu summary.
+
+    The capture runs on a smaller torso (the full workload holds too much memory for a
+    multi-pass capture); its DRAM bytes per stored field byte are scaled to this run's field."""
     p = ROOT / "profiles" / "ncu_traffic.json"
     if not p.is_file():
         return None
     try:
-        return json.loads(p.read_text()).get(kernel_key)
+        entry = json.loads(p.read_text()).get(kernel_key)
     except (ValueError, OSError):
         return None
+    if not entry:
+        return None
+    return int(entry["dram_bytes"] / entry["stored_bytes"] * stored_bytes)
 
 
 # ------------------------------------------------------------------------------- our arm
@@ -161,8 +172,8 @@ def run_ours(args):
 
     rho, truth, spacing = make_workload(args.grid)
     t0 = time.perf_counter()
-    P = pm.Projector(ISOTOPE, rho, spacing, rays=RAYS, support_rho=SUPPORT_RHO, cache=pm.PRC_CACHE_FULL,
-                     precision=pm.PRC_PRECISION_FP32)
+    cache, prec = FORMS[args.form]
+    P = pm.Projector(ISOTOPE, rho, spacing, rays=RAYS, support_rho=SUPPORT_RHO, cache=cache, precision=prec)
     P.synchronize()
     setup_s = time.perf_counter() - t0
     stream = torch.cuda.ExternalStream(P.stream)
@@ -261,8 +272,10 @@ def run_ours(args):
     alg_bytes = 12 * n_active + 8 * deposits  # 8 B per deposit (weight + target value), 12 B per source
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / (launch_ms[top] / 1e3) / 1e9
-    mode, far_entries = P.cache_mode
-    traffic = ncu_traffic(f"{top}_fp32_field")
+    mode, far_entries, far_t_entries = P.cache_mode
+    elem = 2 if args.form == "bf16" else 4
+    stored_bytes = (far_t_entries if top == "forward" else far_entries) * elem
+    traffic = ncu_traffic(f"{top}_{args.form}", stored_bytes) if mode == 2 else None
 
     forms = None
     if not args.no_forms and rank == 0:
@@ -293,10 +306,12 @@ def run_ours(args):
         "config": {
             "workload": f"torso {nx}x{ny}x{nz} at 0.776x0.776x0.795 mm, {ISOTOPE}, rays {RAYS}, beta {BETA}, "
                         f"gamma {GAMMA:g}, accel on, {args.iterations} MAP-EM iterations per step",
-            "form": "plain projector, fp32 weights: near cache + stored far-field coefficient field",
+            "form": {"fp32": "plain projector, fp32 stored coefficient field (near block + far rays)",
+                     "bf16": "mixed precision: bf16 stored coefficient field, fp32 accumulation, fp64 sums",
+                     "traced": "plain projector, near cache + far rays re-marched every projection"}[args.form],
             "n_active": n_active,
             "deposits_per_projection": deposits,
-            "far_field_entries": far_entries,
+            "field_entries": {"source_major": far_entries, "target_major": far_t_entries},
             "voxels_per_s": round(value * n_vox, 1),
             "setup_s": round(setup_s, 4),
             "l2": "flushed (256 MB write) before every timed step; the step also streams a "
@@ -305,12 +320,14 @@ def run_ours(args):
         },
         "e2e": {"value": round(e2e_value, 3), "unit": "EM iters/s",
                 "h2d_bytes_per_step": int(g_host.nbytes), "d2h_bytes_per_step": int(g_host.nbytes)},
-        "roofline": {"bound": "hbm", "kernel": f"project_kernel {top} (stored fp32 field)",
+        "roofline": {"bound": "hbm", "kernel": f"project_kernel {top} ({args.form} form)",
                      "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
                      "traffic": traffic, "launch_ms": {k: round(v, 4) for k, v in launch_ms.items()},
                      "algorithmic_bytes": alg_bytes},
-        "gpu_launches": args.steps * (3 + 6 * args.iterations),
+        # per step: 3 initialisation kernels, then per iteration extrapolate, forward (u = f / W
+        # and the gather, or the scatter), ratio, adjoint, RDP update, finish
+        "gpu_launches": args.steps * (3 + (7 if far_t_entries else 6) * args.iterations),
         "clocks": clock_info,
     }
     if forms:
@@ -419,8 +436,42 @@ def run_reference(args):
                                f"beta {BETA}, gamma {GAMMA:g}, accel on, {args.iterations} MAP-EM iterations"},
         "cpu_baseline": info,
         "e2e": {"value": round(value, 5), "unit": "EM iters/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "reference_gpu": reference_gpu(rho, g),
     }
     print(json.dumps(line))
+
+
+def reference_gpu(rho, g, iterations=30):
+    """EM iterations/s of the reference executable itself (prc.cu compiled for sm_100a by
+    oracle/build_ref.sh) on the same workload, from its own `iterations X s` line."""
+    import re
+    import tempfile
+    exe = ROOT / "oracle" / "_ref" / "prc"
+    if not exe.is_file():
+        return {"unavailable": "oracle/_ref/prc was not built (needs the reference source)"}
+    try:
+        import torch
+        if not torch.cuda.is_available():
+            return {"unavailable": "no CUDA device"}
+    except Exception:
+        return {"unavailable": "no CUDA device"}
+    nz, ny, nx = rho.shape
+    with tempfile.TemporaryDirectory() as d:
+        d = Path(d)
+        rho.astype(np.float32).tofile(d / "rho.raw")
+        g.astype(np.float32).tofile(d / "g.raw")
+        cmd = [str(exe), ISOTOPE, str(nx), str(ny), str(nz), "0.776", "0.776", "0.795", "--input", str(d / "g.raw"),
+               "--density", str(d / "rho.raw"), "--output", str(d / "out.raw"), "--rays", str(RAYS), "--beta",
+               str(BETA), "--gamma", str(GAMMA), "--support-rho", str(SUPPORT_RHO), "--iterations", str(iterations)]
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=900)
+    m = re.search(r"iterations ([0-9.]+) s", r.stdout)
+    n = re.search(r"normalisation .*: ([0-9.]+) s", r.stdout)
+    if r.returncode != 0 or not m:
+        return {"unavailable": f"reference executable failed: {r.stderr.strip()[:200]}"}
+    secs = float(m.group(1))
+    return {"value": round(iterations / secs, 3), "unit": "EM iters/s", "iterations": iterations,
+            "iteration_seconds": secs, "setup_seconds": float(n.group(1)) if n else None,
+            "what": "prc.cu built for sm_100a, timed by its own 2-decimal clock"}
 
 
 def phantoms_poisson_without_gpu(truth):

@@ -47,8 +47,12 @@ enum {
 enum {
     PRC_CACHE_NONE = 0, /* retrace near block and far rays every projection (--no-cache-near) */
     PRC_CACHE_NEAR = 1, /* cache the near block, retrace far rays (the reference's default) */
-    PRC_CACHE_FULL = 2  /* also store the far-field weights, indexed by a shared ray template;
-                           falls back to PRC_CACHE_NEAR when they do not fit in half the free memory */
+    PRC_CACHE_FULL = 2, /* store every weight (near block and far rays) as a coefficient field
+                           indexed by a shared ray template, source-major for the adjoint and
+                           target-major for the forward projection (both gathers); falls back to
+                           PRC_CACHE_SOURCE_MAJOR, then PRC_CACHE_NEAR, when memory is short */
+    PRC_CACHE_SOURCE_MAJOR = 3 /* the source-major field only: half the memory of PRC_CACHE_FULL,
+                                  the forward projection scatters with atomics */
 };
 
 /* Volume geometry: positional arguments NX NY NZ DX DY DZ of prc.cu:515-516. */
@@ -96,8 +100,10 @@ int prc_active_count(const prc_handle* h, int64_t* n_active);
 int prc_cutoff(const prc_handle* h, float* cutoff_mm);
 /* Bytes of device memory the handle owns. */
 int prc_device_bytes(const prc_handle* h, int64_t* bytes);
-/* The cache mode in effect (PRC_CACHE_*, after any fall-back) and the far-field entries stored. */
-int prc_cache_mode(const prc_handle* h, int* mode, int64_t* far_entries);
+/* The cache mode in effect (PRC_CACHE_*, after any fall-back) and the entries of the stored
+ * field: source-major (used by the adjoint) and target-major (used by the forward projection,
+ * which falls back to an atomic scatter over the source-major field when this copy is 0). */
+int prc_cache_mode(const prc_handle* h, int* mode, int64_t* source_major_entries, int64_t* target_major_entries);
 /* The handle's stream (a cudaStream_t) as void*. */
 void* prc_stream(const prc_handle* h);
 

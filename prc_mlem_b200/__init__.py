@@ -27,6 +27,7 @@ PRC_PRECISION_BF16 = 1
 PRC_CACHE_NONE = 0
 PRC_CACHE_NEAR = 1
 PRC_CACHE_FULL = 2
+PRC_CACHE_SOURCE_MAJOR = 3
 ISOTOPES = ("11C", "13N", "15O", "18F", "64Cu", "68Ga", "82Rb", "124I")
 
 
@@ -61,7 +62,8 @@ _SIGNATURES = {
     "prc_active_count": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int64)]),
     "prc_cutoff": (ctypes.c_int, [_P, _F]),
     "prc_device_bytes": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int64)]),
-    "prc_cache_mode": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int64)]),
+    "prc_cache_mode": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int64),
+                                      ctypes.POINTER(ctypes.c_int64)]),
     "prc_stream": (_P, [_P]),
     "prc_forward": (ctypes.c_int, [_P, _P, _P, _P]),
     "prc_adjoint": (ctypes.c_int, [_P, _P, _P, _P]),
@@ -197,11 +199,11 @@ class Projector:
         return v.value
 
     @property
-    def cache_mode(self) -> tuple[int, int]:
-        """(PRC_CACHE_* in effect, stored far-field entries)."""
-        m, e = ctypes.c_int(), ctypes.c_int64()
-        _check(lib().prc_cache_mode(self._h, ctypes.byref(m), ctypes.byref(e)))
-        return m.value, e.value
+    def cache_mode(self) -> tuple[int, int, int]:
+        """(PRC_CACHE_* in effect, source-major field entries, target-major field entries)."""
+        m, e, t = ctypes.c_int(), ctypes.c_int64(), ctypes.c_int64()
+        _check(lib().prc_cache_mode(self._h, ctypes.byref(m), ctypes.byref(e), ctypes.byref(t)))
+        return m.value, e.value, t.value
 
     @property
     def stream(self) -> int:

@@ -46,6 +46,7 @@ struct ProjParams {
     const int* tmpl;                 // [n_rows][tmpl_len]: linear target offset of step m of row k;
                                      // row 0 is the 5x5x5 block, row 1 + r the post-block steps of
                                      // far ray r (the same for every source)
+    const int* tmpl_neg;             // the same offsets negated (target-major gathers: source = t - o)
     int tmpl_len;                    // steps per row: covers every step a ray takes in the image
     int n_rows;                      // n_rays + 1
     StreamLayout src;                // source-major field: group = 32 consecutive sources
@@ -108,8 +109,8 @@ cudaError_t setup_rays(const Grid& g, int n_rays, RayStep* d_far, RayStep* d_nea
 // trace_near: retrace the near block (no cache).  Forward / Adjoint / Count read the stored far
 // field when a.far is on, and march the far rays otherwise.
 cudaError_t project(Op op, const ProjParams& p, const OpArgs& a, bool trace_near, cudaStream_t s);
-// Fills the template p.tmpl ([n_rows][tmpl_len] ints).
-cudaError_t build_template(const ProjParams& p, int* tmpl, cudaStream_t s);
+// Fills the template ([n_rows][tmpl_len] ints) and its negated copy.
+cudaError_t build_template(const ProjParams& p, int* tmpl, int* tmpl_neg, cudaStream_t s);
 // Fills the pack descriptors (one int per 128 stored entries) of a stream layout.
 cudaError_t build_descriptors(const ProjParams& p, const StreamLayout& l, int* desc, cudaStream_t s);
 // Stored steps of the near-block row (125 offsets padded to whole packs).

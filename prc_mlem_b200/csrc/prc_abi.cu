@@ -55,6 +55,7 @@ struct prc_handle {
     NearCache cache;
     FarField far_field;
     int* tmpl = nullptr;
+    int* tmpl_neg = nullptr;
     unsigned short* len = nullptr;
     long long* group_base = nullptr;
     long long* group_total = nullptr;
@@ -296,15 +297,18 @@ static int create_impl(prc_handle* h, const float* density_host) {
     // plus the padding of the last pack, in whole int4s.
     const long long tmpl_len =
         std::max<long long>(near_row_steps(), ((long long)g.nx + g.ny + g.nz + 3 + 3) / 4 * 4);
-    if (h->opts.cache == PRC_CACHE_FULL && h->n_groups && tmpl_len < 65535) {
+    const bool want_field = h->opts.cache == PRC_CACHE_FULL || h->opts.cache == PRC_CACHE_SOURCE_MAJOR;
+    if (want_field && h->n_groups && tmpl_len < 65535) {
         p.tmpl_len = (int)tmpl_len;
         p.n_rows = h->opts.rays + 1;
         PRC_CUDA(h->alloc(&h->tmpl, (size_t)p.n_rows * tmpl_len));
+        PRC_CUDA(h->alloc(&h->tmpl_neg, (size_t)p.n_rows * tmpl_len));
         PRC_CUDA(h->alloc(&h->len, (size_t)h->n_groups * p.n_rows));
         PRC_CUDA(h->alloc(&h->group_total, h->n_groups));
         PRC_CUDA(h->alloc(&h->group_base, (size_t)h->n_groups + 1));
         p.tmpl = h->tmpl;
-        PRC_CUDA(build_template(p, h->tmpl, h->stream));
+        p.tmpl_neg = h->tmpl_neg;
+        PRC_CUDA(build_template(p, h->tmpl, h->tmpl_neg, h->stream));
         OpArgs la = h->op_args();
         la.len = h->len;
         la.group_total = h->group_total;
@@ -334,7 +338,7 @@ static int create_impl(prc_handle* h, const float* density_host) {
                 PRC_CUDA(build_descriptors(p, p.src, h->desc, h->stream));
                 p.src.desc = h->desc;
                 h->far_entries = run;
-                h->cache_mode = PRC_CACHE_FULL;
+                h->cache_mode = PRC_CACHE_SOURCE_MAJOR;
                 h->trace_near = false;
             } else {
                 cudaGetLastError();  // optional: fall back to the near cache
@@ -342,7 +346,7 @@ static int create_impl(prc_handle* h, const float* density_host) {
         }
     }
     // Near cache when the field is off and it fits in a quarter of free memory (prc.cu:411-419).
-    if (h->cache_mode != PRC_CACHE_FULL && h->opts.cache >= PRC_CACHE_NEAR && h->n_groups) {
+    if (h->cache_mode == PRC_CACHE_NONE && h->opts.cache >= PRC_CACHE_NEAR && h->n_groups) {
         size_t free_b = 0, total_b = 0;
         PRC_CUDA(cudaMemGetInfo(&free_b, &total_b));
         const size_t entries = (size_t)h->n_groups * kNear * kLanes;
@@ -354,9 +358,10 @@ static int create_impl(prc_handle* h, const float* density_host) {
     }
     OpArgs a = h->op_args();
     PRC_CUDA(project(Op::Norm, p, a, true, h->stream));
-    if (h->cache_mode == PRC_CACHE_FULL) {
+    if (h->cache_mode == PRC_CACHE_SOURCE_MAJOR && h->opts.cache == PRC_CACHE_FULL) {
         const int rc = build_target_major(h, active, elem);
         if (rc != PRC_OK) return rc;
+        if (h->far_t.on()) h->cache_mode = PRC_CACHE_FULL;
     }
     PRC_CUDA(cudaStreamSynchronize(h->stream));
     return check_device_error(h);
@@ -376,7 +381,7 @@ int prc_create(const prc_geometry* geo, const char* isotope, const prc_options* 
         (o.rays & 1) || o.rays > INT_MAX - 31 || !(o.support_rho >= 0) || !(o.air_cap_mm > 0) ||
         !std::isfinite(o.support_rho) || !std::isfinite(o.air_cap_mm) ||
         (o.precision != PRC_PRECISION_FP32 && o.precision != PRC_PRECISION_BF16) || o.cache < PRC_CACHE_NONE ||
-        o.cache > PRC_CACHE_FULL)
+        o.cache > PRC_CACHE_SOURCE_MAJOR)
         return fail(PRC_ERR_ARGUMENT, "Invalid geometry or solver parameters");
     if (geo->nx > INT_MAX / geo->ny || geo->nx * geo->ny > INT_MAX / geo->nz)
         return fail(PRC_ERR_LIMIT, "Volume exceeds the INT_MAX voxel index limit");
@@ -399,10 +404,11 @@ int prc_create(const prc_geometry* geo, const char* isotope, const prc_options* 
     return PRC_OK;
 }
 
-int prc_cache_mode(const prc_handle* h, int* mode, int64_t* far_entries) {
+int prc_cache_mode(const prc_handle* h, int* mode, int64_t* source_major_entries, int64_t* target_major_entries) {
     if (!h) return fail(PRC_ERR_ARGUMENT, "Invalid argument");
     if (mode) *mode = h->cache_mode;
-    if (far_entries) *far_entries = h->far_entries + h->far_t_entries;
+    if (source_major_entries) *source_major_entries = h->far_entries;
+    if (target_major_entries) *target_major_entries = h->far_t_entries;
     return PRC_OK;
 }
 

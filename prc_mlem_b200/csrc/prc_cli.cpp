@@ -54,7 +54,7 @@ void print_usage(const char* prog, FILE* stream = stderr) {  // prc.cu:461-484
             "  --exact-range     evaluate the survival function analytically, not from the table (validation)\n"
             "  --no-cache-near   trace the near block again in every pass (less GPU memory, slower)\n"
             "  --no-accel        plain MAP-EM without Biggs-Andrews extrapolation (validation)\n"
-            "  --cache MODE      none|near|full: weights kept on the GPU between passes (default full)\n"
+            "  --cache MODE      none|near|source|full: weights kept on the GPU between passes (default full)\n"
             "  --bf16-weights    store the projector weights in bfloat16 (mixed precision)\n"
             "Isotopes:",
             prog);
@@ -119,7 +119,11 @@ Options parse(int argc, char** argv) {  // prc.cu:508-555
         else if (key == "--no-cache-near") o.cache_near = false;
         else if (key == "--cache") {
             const std::string m = value();
-            o.cache = m == "none" ? PRC_CACHE_NONE : m == "near" ? PRC_CACHE_NEAR : m == "full" ? PRC_CACHE_FULL : -1;
+            o.cache = m == "none"     ? PRC_CACHE_NONE
+                      : m == "near"   ? PRC_CACHE_NEAR
+                      : m == "full"   ? PRC_CACHE_FULL
+                      : m == "source" ? PRC_CACHE_SOURCE_MAJOR
+                                      : -1;
         }
         else if (key == "--exact-range") o.exact_range = true;
         else if (key == "--no-accel") o.accelerate = false;
@@ -248,12 +252,14 @@ int main(int argc, char** argv) {
     double t = now_s();
     prc_handle* h = nullptr;
     check(prc_create(&geo, o.isotope.c_str(), &opts, rho.data(), &h));
-    int64_t bytes = 0, far_entries = 0;
+    int64_t bytes = 0, far_entries = 0, far_t_entries = 0;
     int mode = 0;
     prc_device_bytes(h, &bytes);
-    prc_cache_mode(h, &mode, &far_entries);
+    prc_cache_mode(h, &mode, &far_entries, &far_t_entries);
     printf("normalisation (%d near-block + %d far-field rays): %.2f s, cache %s, device memory %.0f MiB\n", kNearRays,
-           o.rays, now_s() - t, mode == PRC_CACHE_FULL ? "near+far" : mode == PRC_CACHE_NEAR ? "near" : "none",
+           o.rays, now_s() - t,
+           mode == PRC_CACHE_FULL ? "field (source+target major)" : mode == PRC_CACHE_SOURCE_MAJOR ? "field (source major)"
+           : mode == PRC_CACHE_NEAR ? "near" : "none",
            bytes / 1048576.0);
 
     std::vector<float> out(n);

@@ -139,7 +139,9 @@ __device__ __forceinline__ void march(const ProjParams& p, const RayStep& R, boo
 }
 
 enum NearMode : int { kTraceNear = 0, kCacheF32 = 1, kCacheBF16 = 2 };
-enum FarMode : int { kMarch = 0, kFieldF32 = 1, kFieldBF16 = 2 };
+// Far-field source: marched rays, the source-major field (adjoint; forward by scatter), or the
+// target-major field (forward by gather; the *T modes).
+enum FarMode : int { kMarch = 0, kFieldF32 = 1, kFieldBF16 = 2, kFieldF32T = 3, kFieldBF16T = 4 };
 
 // ---- stored coefficient field ----------------------------------------------------------------
 // Stream of one group: template row 0 is the near block (125 offsets, padded to kNearRow
@@ -234,7 +236,7 @@ __global__ void __launch_bounds__(kBlock) project_kernel(const ProjParams p, con
     float scale = 0.0f, acc = 0.0f;
     unsigned long long cnt = 0;
     if constexpr (OP == Op::Forward) {  // prc.cu:244-248
-        if (FAR_MODE != kMarch && a.farT.on()) {
+        if (FAR_MODE >= kFieldF32T) {
             live = valid;  // gather form: lanes are targets, a.in holds u = f / W
         } else {
             const float fs = valid ? __ldg(a.in + s) : 0.0f, ws = valid ? __ldg(a.W + src) : 0.0f;
@@ -336,28 +338,30 @@ __global__ void __launch_bounds__(kBlock) project_kernel(const ProjParams p, con
         // Stored field, streamed by TMA.  Lane 0 keeps kStages bulk copies of kChunk bytes in
         // flight into this warp's shared-memory ring (cp.async.bulk, completion counted by an
         // mbarrier), so the weights arrive as contiguous DRAM bursts without holding
-        // registers.  For each chunk the warp first reads the packs' descriptors and template
-        // offsets, issues every gather of the chunk (adjoint; indices clamped into the volume,
-        // a zero weight discards the value), and only then consumes the weights.
-        // The forward gathers u = f / W over the target-major copy when it exists (lane = target,
-        // source = target - offset); otherwise it scatters over the source-major field.
-        constexpr int kElem = FAR_MODE == kFieldF32 ? 4 : 2;
+        // registers.  A chunk is consumed in batches of kBatch packs: the packs' template
+        // offsets (one int4 broadcast each, addressed by the pack descriptors), the weights
+        // from shared memory, then one predicated gather per nonzero weight -- zero padding
+        // costs no memory traffic -- or one scatter per nonzero weight without the
+        // target-major copy.  Entries of lanes that are not sources are zero by construction.
+        constexpr bool kGatherT = OP == Op::Forward && FAR_MODE >= kFieldF32T;
+        constexpr int kBase = FAR_MODE >= kFieldF32T ? FAR_MODE - 2 : FAR_MODE;  // kFieldF32 / kFieldBF16
+        constexpr int kElem = kBase == kFieldF32 ? 4 : 2;
         constexpr int kPackBytes = kPack * kLanes * kElem;
         constexpr int kPacksPerChunk = kChunk / kPackBytes;
-        const bool gather = OP == Op::Adjoint || (OP == Op::Forward && a.farT.on());
-        const bool transposed = OP == Op::Forward && a.farT.on();
-        const StreamLayout& lay = transposed ? p.tgt : p.src;
-        const FarField& fld = transposed ? a.farT : a.far;
-        const int sign = transposed ? -1 : 1;
+        constexpr int kBatch = 4;  // packs per batch: 16 steps in flight per lane
+        const StreamLayout& lay = kGatherT ? p.tgt : p.src;
+        const FarField& fld = kGatherT ? a.farT : a.far;
+        const int* tmpl = kGatherT ? p.tmpl_neg : p.tmpl;
         unsigned char* ring = dyn_smem + (size_t)warp * kStages * kChunk;
         uint64_t* bars = field_bars[warp];
         const long long e0 = lay.group_base[group], e1 = lay.group_base[group + 1];
-        const char* src_bytes = (FAR_MODE == kFieldF32 ? reinterpret_cast<const char*>(fld.f32)
-                                                       : reinterpret_cast<const char*>(fld.b16)) + e0 * kElem;
+        const char* src_bytes = (kBase == kFieldF32 ? reinterpret_cast<const char*>(fld.f32)
+                                                    : reinterpret_cast<const char*>(fld.b16)) + e0 * kElem;
         const int* desc = lay.desc + e0 / (kPack * kLanes);
         const long long total = (e1 - e0) * kElem;
         const int n_packs = (int)((e1 - e0) / (kPack * kLanes));
         const int n_chunks = (n_packs + kPacksPerChunk - 1) / kPacksPerChunk;
+        const float* base = a.in + s;  // gather: source + offset (adjoint) or target - offset (forward)
         auto issue = [&](int c) {  // lane 0 only
             const int stage = c % kStages;
             const unsigned bytes = (unsigned)min((long long)kChunk, total - (long long)c * kChunk);
@@ -373,49 +377,44 @@ __global__ void __launch_bounds__(kBlock) project_kernel(const ProjParams p, con
         bool ok = true;
         for (int c = 0; c < n_chunks; ++c) {
             const int packs = min(kPacksPerChunk, n_packs - c * kPacksPerChunk);
-            int o[kPacksPerChunk * kPack];
-#pragma unroll
-            for (int k = 0; k < kPacksPerChunk; ++k) {
-                int4 t = make_int4(0, 0, 0, 0);
-                if (k < packs) t = __ldg(reinterpret_cast<const int4*>(p.tmpl + __ldg(desc + c * kPacksPerChunk + k)));
-                o[k * kPack] = t.x, o[k * kPack + 1] = t.y, o[k * kPack + 2] = t.z, o[k * kPack + 3] = t.w;
-            }
             const int stage = c % kStages;
             if (!mbar_wait_bounded(&bars[stage], (c / kStages) & 1)) {
                 ok = false;
                 break;
             }
-            // weights of the chunk from shared memory; packs beyond the stream end read as 0
             const unsigned char* chunk = ring + stage * kChunk;
-            float w[kPacksPerChunk * kPack];
+            const int* cdesc = desc + c * kPacksPerChunk;
+            for (int b = 0; b < packs; b += kBatch) {
+                int o[kBatch * kPack];
+                float w[kBatch * kPack];
 #pragma unroll
-            for (int k = 0; k < kPacksPerChunk; ++k) {
-                if (k < packs) {
-                    if constexpr (FAR_MODE == kFieldF32) {
-                        const float4 x = reinterpret_cast<const float4*>(chunk + k * kPackBytes)[lane];
+                for (int k = 0; k < kBatch; ++k) {
+                    const bool here = b + k < packs;
+                    const int4 t = here ? __ldg(reinterpret_cast<const int4*>(tmpl + __ldg(cdesc + b + k)))
+                                        : make_int4(0, 0, 0, 0);
+                    o[k * kPack] = t.x, o[k * kPack + 1] = t.y, o[k * kPack + 2] = t.z, o[k * kPack + 3] = t.w;
+                    if constexpr (kBase == kFieldF32) {
+                        const float4 x = here ? reinterpret_cast<const float4*>(chunk + (b + k) * kPackBytes)[lane]
+                                              : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
                         w[k * kPack] = x.x, w[k * kPack + 1] = x.y, w[k * kPack + 2] = x.z, w[k * kPack + 3] = x.w;
                     } else {
-                        const uint2 x = reinterpret_cast<const uint2*>(chunk + k * kPackBytes)[lane];
+                        const uint2 x = here ? reinterpret_cast<const uint2*>(chunk + (b + k) * kPackBytes)[lane]
+                                             : make_uint2(0u, 0u);
                         w[k * kPack] = __uint_as_float(x.x << 16), w[k * kPack + 1] = __uint_as_float(x.x & 0xffff0000u);
                         w[k * kPack + 2] = __uint_as_float(x.y << 16), w[k * kPack + 3] = __uint_as_float(x.y & 0xffff0000u);
                     }
+                }
+                if constexpr (OP == Op::Adjoint || kGatherT) {
+                    float v[kBatch * kPack];
+#pragma unroll
+                    for (int u = 0; u < kBatch * kPack; ++u) v[u] = w[u] > 0.0f ? __ldg(base + o[u]) : 0.0f;
+#pragma unroll
+                    for (int u = 0; u < kBatch * kPack; ++u) acc = fmaf(w[u], v[u], acc);
                 } else {
 #pragma unroll
-                    for (int u = 0; u < kPack; ++u) w[k * kPack + u] = 0.0f;
+                    for (int u = 0; u < kBatch * kPack; ++u)
+                        if (live && w[u] > 0.0f) deposit(s + o[u], w[u]);
                 }
-            }
-            if (gather) {
-                // Only lanes with a deposit load: zero-padded steps cost no memory traffic.
-                float v[kPacksPerChunk * kPack];
-#pragma unroll
-                for (int u = 0; u < kPacksPerChunk * kPack; ++u)
-                    v[u] = (live && w[u] > 0.0f) ? __ldg(a.in + s + sign * o[u]) : 0.0f;
-#pragma unroll
-                for (int u = 0; u < kPacksPerChunk * kPack; ++u) acc += w[u] * v[u];
-            } else {
-#pragma unroll
-                for (int u = 0; u < kPacksPerChunk * kPack; ++u)
-                    if (live && w[u] > 0.0f) deposit(s + o[u], w[u]);
             }
             __syncwarp();
             if (lane == 0 && c + kStages < n_chunks) {
@@ -444,7 +443,7 @@ __global__ void __launch_bounds__(kBlock) project_kernel(const ProjParams p, con
     } else if constexpr (OP == Op::Adjoint) {
         if (live) a.out[s] = acc / __ldg(a.W + src);  // prc.cu:266
     } else if constexpr (OP == Op::Forward) {
-        if (FAR_MODE != kMarch && a.farT.on() && valid) a.out[s] = acc;
+        if (FAR_MODE >= kFieldF32T && valid) a.out[s] = acc;
     } else if constexpr (OP == Op::Count) {
         for (int off = 16; off > 0; off >>= 1) cnt += __shfl_xor_sync(kFull, cnt, off);
         if (lane == 0) atomicAdd(a.count, cnt);
@@ -544,7 +543,7 @@ cudaError_t launch(const ProjParams& p, const OpArgs& a, cudaStream_t s) {
     const int blocks = (groups + kWarps - 1) / kWarps;
     if (blocks == 0) return cudaSuccess;
     size_t smem = 0;
-    if (FAR_MODE != kMarch) smem = kFieldSmemBytes;
+    if (FAR_MODE != kMarch) smem = kFieldSmemBytes;  // the ring; the near block is in the field
     else if (NEAR_MODE == kTraceNear && OP != Op::Layout) smem = kNearSmemBytes;
     auto kernel = project_kernel<OP, EXACT, NEAR_MODE, FAR_MODE>;
     if (smem > 48 * 1024) {
@@ -562,6 +561,8 @@ cudaError_t launch_modes(const ProjParams& p, const OpArgs& a, bool trace_near, 
             return a.near.b16 ? launch<OP, EXACT, kCacheBF16, kMarch>(p, a, s) : launch<OP, EXACT, kCacheF32, kMarch>(p, a, s);
         return launch<OP, EXACT, kTraceNear, kMarch>(p, a, s);
     } else {
+        if (OP == Op::Forward && a.farT.f32) return launch<OP, EXACT, kTraceNear, kFieldF32T>(p, a, s);
+        if (OP == Op::Forward && a.farT.b16) return launch<OP, EXACT, kTraceNear, kFieldBF16T>(p, a, s);
         if (a.far.f32) return launch<OP, EXACT, kTraceNear, kFieldF32>(p, a, s);
         if (a.far.b16) return launch<OP, EXACT, kTraceNear, kFieldBF16>(p, a, s);
         if (trace_near || !a.near.on()) return launch<OP, EXACT, kTraceNear, kMarch>(p, a, s);
@@ -583,8 +584,14 @@ cudaError_t setup_rays(const Grid& g, int n_rays, RayStep* d_far, RayStep* d_nea
     return cudaGetLastError();
 }
 
-cudaError_t build_template(const ProjParams& p, int* tmpl, cudaStream_t s) {
+__global__ void negate_kernel(const int* in, int* out, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        out[i] = -in[i];
+}
+
+cudaError_t build_template(const ProjParams& p, int* tmpl, int* tmpl_neg, cudaStream_t s) {
     template_kernel<<<(p.n_rays + 128) / 128, 128, 0, s>>>(p, tmpl);
+    negate_kernel<<<256, 256, 0, s>>>(tmpl, tmpl_neg, (size_t)p.n_rows * p.tmpl_len);
     return cudaGetLastError();
 }
 

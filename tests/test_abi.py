@@ -61,7 +61,7 @@ def test_create_rejects_bad_geometry_before_cuda(field, value):
 
 
 @pytest.mark.parametrize("field,value", [("rays", 3), ("rays", 0), ("air_cap_mm", 0.0), ("support_rho", -1.0),
-                                         ("precision", 7), ("cache", 5)])
+                                         ("precision", 7), ("cache", 5), ("cache", -1)])
 def test_create_rejects_bad_options_before_cuda(field, value):
     opts = pm.default_options()
     setattr(opts, field, value)

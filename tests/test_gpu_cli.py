@@ -33,7 +33,8 @@ def run(workdir, image, mode, *options, out="out.raw"):
     return np.fromfile(workdir / out, np.float32).reshape(12, 14, 16)
 
 
-@pytest.mark.parametrize("extra", [(), ("--cache", "near"), ("--no-cache-near",)], ids=["full", "near", "none"])
+@pytest.mark.parametrize("extra", [(), ("--cache", "source"), ("--cache", "near"), ("--no-cache-near",)],
+                         ids=["full", "source", "near", "none"])
 def test_cli_matches_reference_binary(workdir, ref_golden, extra):
     assert rel_l2(run(workdir, "x.raw", "forward", *extra), ref_golden["fixture_fwd_68Ga"]) < 1e-5
     assert rel_l2(run(workdir, "y.raw", "adjoint", *extra), ref_golden["fixture_adj_68Ga"]) < 1e-5

@@ -22,7 +22,8 @@ def projector(fixture72, cache=pm.PRC_CACHE_FULL, prec=pm.PRC_PRECISION_FP32):
     return _cache[(cache, prec)]
 
 
-@pytest.mark.parametrize("cache", [pm.PRC_CACHE_FULL, pm.PRC_CACHE_NEAR, pm.PRC_CACHE_NONE], ids=["full", "near", "none"])
+@pytest.mark.parametrize("cache", [pm.PRC_CACHE_FULL, pm.PRC_CACHE_SOURCE_MAJOR, pm.PRC_CACHE_NEAR, pm.PRC_CACHE_NONE],
+                         ids=["full", "source", "near", "none"])
 @pytest.mark.parametrize("case", sorted(EM_CASES))
 def test_correction_matches_reference_binary(fixture72, ref_golden, oracle_mod, case, cache):
     rho, x, y, shape, sp = fixture72

@@ -12,10 +12,11 @@ from conftest import GOLDEN, rel_l2
 
 pytestmark = pytest.mark.gpu
 ISOTOPES = ("11C", "13N", "15O", "18F", "64Cu", "68Ga", "82Rb", "124I")
-MODES = [(pm.PRC_CACHE_FULL, pm.PRC_PRECISION_FP32), (pm.PRC_CACHE_NEAR, pm.PRC_PRECISION_FP32),
-         (pm.PRC_CACHE_NONE, pm.PRC_PRECISION_FP32), (pm.PRC_CACHE_FULL, pm.PRC_PRECISION_BF16),
+MODES = [(pm.PRC_CACHE_FULL, pm.PRC_PRECISION_FP32), (pm.PRC_CACHE_SOURCE_MAJOR, pm.PRC_PRECISION_FP32),
+         (pm.PRC_CACHE_NEAR, pm.PRC_PRECISION_FP32), (pm.PRC_CACHE_NONE, pm.PRC_PRECISION_FP32),
+         (pm.PRC_CACHE_FULL, pm.PRC_PRECISION_BF16), (pm.PRC_CACHE_SOURCE_MAJOR, pm.PRC_PRECISION_BF16),
          (pm.PRC_CACHE_NEAR, pm.PRC_PRECISION_BF16)]
-MODE_IDS = ["full-fp32", "near-fp32", "none-fp32", "full-bf16", "near-bf16"]
+MODE_IDS = ["full-fp32", "source-fp32", "near-fp32", "none-fp32", "full-bf16", "source-bf16", "near-bf16"]
 
 
 def tol(prec):
@@ -37,7 +38,8 @@ def projector(fixture72, iso="68Ga", cache=pm.PRC_CACHE_FULL, prec=pm.PRC_PRECIS
 def test_forward_adjoint_match_reference_binary(fixture72, ref_golden, oracle_mod, iso):
     rho, x, y, shape, sp = fixture72
     P = projector(fixture72, iso)
-    assert P.cache_mode[0] == pm.PRC_CACHE_FULL
+    mode, source_entries, target_entries = P.cache_mode
+    assert mode == pm.PRC_CACHE_FULL and source_entries > 0 and target_entries > 0
     ax, aty = P.forward_host(x), P.adjoint_host(y)
     assert rel_l2(ax, ref_golden[f"fixture_fwd_{iso}"]) < 1e-5
     assert rel_l2(aty, ref_golden[f"fixture_adj_{iso}"]) < 1e-5
@@ -50,6 +52,7 @@ def test_forward_adjoint_match_reference_binary(fixture72, ref_golden, oracle_mo
 def test_cache_modes_match_reference_binary(fixture72, ref_golden, mode):
     rho, x, y, shape, sp = fixture72
     P = projector(fixture72, "68Ga", *mode)
+    assert P.cache_mode[0] == mode[0]  # no fall-back at this size
     assert rel_l2(P.forward_host(x), ref_golden["fixture_fwd_68Ga"]) < tol(mode[1])
     assert rel_l2(P.adjoint_host(y), ref_golden["fixture_adj_68Ga"]) < tol(mode[1])
 
