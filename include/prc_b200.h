@@ -156,6 +156,17 @@ int prc_sum(prc_handle* h, const float* d_x, double* sum, void* stream);
  * algorithmic-bytes accounting).  Synchronises. */
 int prc_count_deposits(prc_handle* h, int64_t* deposits);
 
+/* FP64 sum of n device floats into *d_sum (device memory), enqueued on `stream` (a
+ * cudaStream_t; NULL = the default stream).  It allocates no device memory: no counterpart in
+ * the reference; it exists for callers that cannot allocate at the point of the call (services
+ * that reserve all device memory at start-up, hot paths that must not pay cudaMalloc's
+ * synchronisation, operators inside another framework's allocator).  Its scratch is a
+ * file-scope device array of about 512 KiB that every GPU loading the library holds until
+ * exit; n is limited to 2^28 elements (PRC_ERR_LIMIT beyond).  The first call on each device
+ * looks up that array's device address, so it should come before any stream capture.  All
+ * calls share the array: calls that overlap on the GPU (other streams, other threads) race. */
+int prc_sum_static(const float* d_x, int64_t n, double* d_sum, void* stream);
+
 /* Waits for all work on the handle's stream. */
 int prc_synchronize(prc_handle* h);
 

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 #include <cuda_bf16.h>
 #include <cstdint>
+#include <string>
 
 #include "range_model.h"
 
@@ -155,5 +156,8 @@ cudaError_t em_finish(const EmVolumes& v, float* next, float* residual, const fl
                       cudaStream_t s);
 cudaError_t em_sum(const EmVolumes& v, const float* x, cudaStream_t s);
 cudaError_t em_mask_copy(const EmVolumes& v, const float* src, float* dst, float fill, cudaStream_t s);
+
+// Sets the message prc_last_error() returns on this thread (for entry points outside prc_abi.cu).
+void set_last_error(const std::string& msg);
 
 }  // namespace prc

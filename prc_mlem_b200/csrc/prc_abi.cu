@@ -34,6 +34,8 @@ int fail(int code, const std::string& msg) {
 
 }  // namespace
 
+void prc::set_last_error(const std::string& msg) { g_last_error = msg; }
+
 struct prc_handle {
     Grid g{};
     RangeModel model;
