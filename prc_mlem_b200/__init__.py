@@ -269,7 +269,9 @@ class Projector:
 
 
 def header_symbols() -> list[str]:
-    """Every function the public header declares (used to check the library's exports)."""
+    """Every function the public headers (include/*.h) declare (used to check the exports)."""
     import re
-    text = HEADER_PATH.read_text()
-    return sorted(set(re.findall(r"^\s*(?:[\w\s\*]+?)\b(prc_\w+)\s*\(", text, re.M)))
+    names = set()
+    for header in sorted(HEADER_PATH.parent.glob("*.h")):
+        names.update(re.findall(r"^\s*(?:[\w\s\*]+?)\b(prc_\w+)\s*\(", header.read_text(), re.M))
+    return sorted(names)

@@ -1,0 +1,116 @@
+"""The learned range-kernel surrogate on a B200: its tensor-core GEMM engine (tcgen05, bf16
+operands, fp32 accumulation in tensor memory) against a float64 reference."""
+import ctypes
+
+import numpy as np
+import pytest
+import torch
+
+import prc_mlem_b200 as pm
+
+pytestmark = pytest.mark.gpu
+
+
+def lib():
+    l = pm.lib()
+    l.prc_nn_gemm_bf16.argtypes = [ctypes.c_void_p] * 3 + [ctypes.c_int] * 3 + [ctypes.c_void_p] * 2
+    return l
+
+
+@pytest.mark.parametrize("M,N,K", [(128, 64, 64), (200, 96, 100), (1000, 32, 864), (33, 2048, 32), (2048, 32, 513)])
+def test_tensor_core_gemm_matches_float64(M, N, K):
+    g = torch.Generator().manual_seed(M * 7 + N * 3 + K)
+    a = torch.randn(M, K, generator=g).to(torch.bfloat16)
+    b = torch.randn(N, K, generator=g).to(torch.bfloat16)
+    expect = a.double() @ b.double().T
+    da, db = a.cuda(), b.cuda()
+    c = torch.full((M, N), float("nan"), dtype=torch.float32, device="cuda")
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    rc = lib().prc_nn_gemm_bf16(da.data_ptr(), db.data_ptr(), c.data_ptr(), M, N, K, err.data_ptr(), None)
+    assert rc == 0, pm.lib().prc_last_error()
+    torch.cuda.synchronize()
+    assert err.item() == 0
+    got = c.double().cpu()
+    scale = (a.double().abs() @ b.double().abs().T)
+    assert torch.all((got - expect).abs() <= 1e-5 * scale + 1e-6), float(((got - expect).abs() / scale).max())
+
+
+# ---- the network: forward values and gradients against the FP64 CPU oracle -----------------
+def nn_lib():
+    l = pm.lib()
+    l.prc_nn_create.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
+    l.prc_nn_destroy.argtypes = [ctypes.c_void_p]
+    l.prc_nn_param_count.restype = ctypes.c_int64
+    l.prc_nn_set_params.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+    l.prc_nn_get.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+    l.prc_nn_forward.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+    l.prc_nn_backward.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_float,
+                                  ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]
+    return l
+
+
+SHAPES = [("w1", (32, 3, 3, 3, 4)), ("b1", (32,)), ("w2", (32, 3, 3, 3, 32)), ("b2", (32,)),
+          ("w3", (32, 3, 3, 3, 32)), ("b3", (32,)), ("w4", (32, 3, 3, 3, 32)), ("b4", (32,)),
+          ("wh", (2048, 32)), ("bh", (2048,))]
+
+
+def random_params(seed):
+    rng = np.random.default_rng(seed)
+    p = {}
+    for name, shape in SHAPES:
+        fan_in = int(np.prod(shape[1:])) if name.startswith("w") else 1
+        p[name] = (rng.normal(0, 1.2 / np.sqrt(fan_in), shape) if name.startswith("w")
+                   else rng.uniform(0.0, 0.2, shape)).astype(np.float32)
+    return p
+
+
+def flat(p):
+    return np.concatenate([p[name].ravel() for name, _ in SHAPES]).astype(np.float32)
+
+
+def unflat(v):
+    out, off = {}, 0
+    for name, shape in SHAPES:
+        n = int(np.prod(shape))
+        out[name] = v[off:off + n].reshape(shape)
+        off += n
+    return out
+
+
+def test_network_forward_and_gradients_match_fp64_oracle():
+    from oracle import nn_oracle
+    l = nn_lib()
+    assert l.prc_nn_param_count() == sum(int(np.prod(s)) for _, s in SHAPES)
+    B = 6
+    rng = np.random.default_rng(3)
+    x0 = np.zeros((B, 9, 9, 9, 4), np.float32)
+    x0[..., 0] = rng.uniform(0, 1, (B, 9, 9, 9))
+    x0[np.arange(B), ..., 1 + np.arange(B) % 3] = 1.0
+    target = rng.normal(0, 1, (B, 2048)).astype(np.float32)
+    params = random_params(11)
+    h = ctypes.c_void_p()
+    assert l.prc_nn_create(64, ctypes.byref(h)) == 0
+    try:
+        v = flat(params)
+        assert l.prc_nn_set_params(h, v.ctypes.data) == 0
+        d_x = torch.from_numpy(x0).to(torch.bfloat16).cuda()
+        d_y = torch.empty(B, 2048, dtype=torch.float32, device="cuda")
+        assert l.prc_nn_forward(h, d_x.data_ptr(), B, d_y.data_ptr(), None) == 0
+        assert l.prc_nn_forward(h, d_x.data_ptr(), B, None, None) == 0
+        loss = ctypes.c_double()
+        d_t = torch.from_numpy(target).cuda()
+        assert l.prc_nn_backward(h, d_t.data_ptr(), B, 0.0, ctypes.byref(loss), None) == 0, pm.lib().prc_last_error()
+        grads = np.zeros_like(v)
+        assert l.prc_nn_get(h, 1, grads.ctypes.data) == 0
+    finally:
+        l.prc_nn_destroy(h)
+    net = nn_oracle.Net(params)
+    y_ref, _ = net.forward(x0.astype(np.float64))
+    y = d_y.cpu().numpy()
+    assert np.linalg.norm(y - y_ref) / np.linalg.norm(y_ref) < 2e-3
+    ref_loss, ref_g = net.loss_and_grads(x0.astype(np.float64), target.astype(np.float64))
+    assert abs(loss.value - ref_loss) <= 1e-3 * ref_loss
+    g = unflat(grads)
+    for name, _ in SHAPES:
+        err = np.linalg.norm(g[name] - ref_g[name]) / max(np.linalg.norm(ref_g[name]), 1e-30)
+        assert err < 2e-2, (name, err)
