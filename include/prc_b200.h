@@ -92,6 +92,20 @@ const char* prc_isotope_name(int i);
 int prc_create(const prc_geometry* geometry, const char* isotope, const prc_options* opts,
                const float* density_host, prc_handle** out);
 
+/* The same operator with the far field of every source replaced by 128 directions x 16 radial
+ * bins of range-kernel coefficients predicted by the learned surrogate `net` (a prc_net* from
+ * prc_surrogate.h; NULL = the traced radial kernels of every source, i.e. the surrogate
+ * representation without a network) from the density patch around the source.  No
+ * counterpart in the reference.  target_scale is the factor the network was trained with.
+ * With fallback_nrmse > 0 the ray tracer judges every source: where the predicted
+ * coefficients differ from the traced ones by more than fallback_nrmse (relative L2) the
+ * traced ones are used; *fallbacks (optional) receives their number.  The near block is
+ * traced exactly.  Forward, adjoint and MAP-EM then work as for prc_create.  Synchronises. */
+typedef struct prc_net prc_net;
+int prc_create_surrogate(const prc_geometry* geometry, const char* isotope, const prc_options* opts,
+                         const float* density_host, prc_net* net, float target_scale, float fallback_nrmse,
+                         int64_t* fallbacks, prc_handle** out);
+
 /* Releases every device allocation of the handle (Projector::~Projector, prc.cu:423-427). */
 void prc_destroy(prc_handle* h);
 

@@ -42,6 +42,16 @@ int prc_nn_forward(prc_net* net, const void* d_x0, int batch, float* d_y, void* 
  * *loss (host, optional) receives the MSE. */
 int prc_nn_backward(prc_net* net, const float* d_target, int batch, float lr, double* loss, void* stream);
 
+/* Training data on the device: n_vol random volumes of side^3 voxels of spacing_mm, each air
+ * plus up to 10 ellipsoids (ellipsoids: host [n_vol][10][8] = cx, cy, cz, rx, ry, rz in voxels,
+ * density, used flag) with 5 % Gaussian density jitter (seeded); per_vol (a multiple of 32)
+ * tissue sources per volume.  Outputs the sources' input patches (d_patches, [n][9][9][9][4]
+ * bf16) and their traced radial far-field kernels times target_scale (d_targets, [n][2048]
+ * fp32, direction-major), for isotope 18F, 68Ga or 82Rb.  Synchronises. */
+int prc_nn_make_samples(const char* isotope, int n_vol, int side, float spacing_mm, const float* ellipsoids,
+                        uint64_t seed, int per_vol, void* d_patches, float* d_targets, float target_scale,
+                        void* stream);
+
 #ifdef __cplusplus
 }
 #endif

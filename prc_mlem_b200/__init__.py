@@ -80,6 +80,19 @@ _SIGNATURES = {
     "prc_count_deposits": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int64)]),
     "prc_synchronize": (ctypes.c_int, [_P]),
     "prc_sum_static": (ctypes.c_int, [_P, ctypes.c_int64, _P, _P]),
+    "prc_create_surrogate": (ctypes.c_int, [ctypes.POINTER(Geometry), ctypes.c_char_p, ctypes.POINTER(Options), _P,
+                                            _P, ctypes.c_float, ctypes.c_float, ctypes.POINTER(ctypes.c_int64),
+                                            ctypes.POINTER(_P)]),
+    "prc_nn_gemm_bf16": (ctypes.c_int, [_P, _P, _P, ctypes.c_int, ctypes.c_int, ctypes.c_int, _P, _P]),
+    "prc_nn_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(_P)]),
+    "prc_nn_destroy": (None, [_P]),
+    "prc_nn_param_count": (ctypes.c_int64, []),
+    "prc_nn_set_params": (ctypes.c_int, [_P, _P]),
+    "prc_nn_get": (ctypes.c_int, [_P, ctypes.c_int, _P]),
+    "prc_nn_forward": (ctypes.c_int, [_P, _P, ctypes.c_int, _P, _P]),
+    "prc_nn_backward": (ctypes.c_int, [_P, _P, ctypes.c_int, ctypes.c_float, ctypes.POINTER(ctypes.c_double), _P]),
+    "prc_nn_make_samples": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_float, _P,
+                                           ctypes.c_uint64, ctypes.c_int, _P, _P, ctypes.c_float, _P]),
     "prc_last_error": (ctypes.c_char_p, []),
 }
 
@@ -142,7 +155,10 @@ class Projector:
 
     def __init__(self, isotope: str, density: np.ndarray, spacing, rays: int = 128, support_rho: float = 0.05,
                  air_cap_mm: float = 50.0, exact_range: bool = False, cache: int = PRC_CACHE_FULL,
-                 precision: int = PRC_PRECISION_FP32):
+                 precision: int = PRC_PRECISION_FP32, surrogate=None, target_scale: float = 1.0,
+                 fallback_nrmse: float = 0.0):
+        """surrogate: None for the plain projector; a trained network (prc_mlem_b200.surrogate.Network)
+        or the string "traced" for the radial coefficient field (prc_create_surrogate)."""
         density = _host(density)
         if density.ndim != 3:
             raise ValueError("density must be a (nz, ny, nx) array")
@@ -155,8 +171,17 @@ class Projector:
         opts.rays, opts.support_rho, opts.air_cap_mm = rays, support_rho, air_cap_mm
         opts.exact_range, opts.cache, opts.precision = int(exact_range), int(cache), int(precision)
         h = _P()
-        _check(lib().prc_create(ctypes.byref(geo), isotope.encode(), ctypes.byref(opts),
-                                density.ctypes.data, ctypes.byref(h)))
+        self.fallbacks = 0
+        if surrogate is None:
+            _check(lib().prc_create(ctypes.byref(geo), isotope.encode(), ctypes.byref(opts),
+                                    density.ctypes.data, ctypes.byref(h)))
+        else:
+            net = None if isinstance(surrogate, str) else surrogate.handle
+            fb = ctypes.c_int64()
+            _check(lib().prc_create_surrogate(ctypes.byref(geo), isotope.encode(), ctypes.byref(opts),
+                                              density.ctypes.data, net, target_scale, fallback_nrmse,
+                                              ctypes.byref(fb), ctypes.byref(h)))
+            self.fallbacks = fb.value
         self._h = h
         self.support = np.maximum(density, np.float32(1e-3)) >= np.float32(support_rho)
 

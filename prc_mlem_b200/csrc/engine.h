@@ -95,7 +95,55 @@ struct OpArgs {
     unsigned int* error = nullptr;         // set non-zero when a stored-field copy timed out
     unsigned short* len = nullptr;         // Layout output
     long long* group_total = nullptr;      // Layout output: entries per group (sum of len * 32)
+    // Surrogate fields: groups whose flag is 1 keep exact traced weights (the Norm pass fills
+    // only those), the others hold radial coefficients (surrogate_fill fills only those).
+    const unsigned char* fallback_groups = nullptr;
 };
+
+// ---- radial surrogate support -----------------------------------------------------------------
+// The surrogate summarises the far field of a source by 16 radial bins per far ray: bin b of ray
+// r gathers the deposits whose segment midpoint lies at path length t in [e_b, e_{b+1}), with
+// 12 equal bins up to the water-equivalent cutoff and 4 equal bins from there to 3.85 x cutoff
+// (the range in 0.26 g/cm3 lung).  Each (ray, bin) is deposited at one fixed step of the ray:
+// the post-block step whose midpoint is closest to the bin centre.
+constexpr int kRadialBins = 16;
+struct RadialTables {
+    unsigned char* bin_of = nullptr;  // [n_rays][tmpl_len]: bin of post-block step m of ray r
+    int* offset = nullptr;            // [n_rays][16]: linear target offset of bin b of ray r
+    int* xyz = nullptr;               // the same offset as packed (dx+512) | (dy+512) << 10 | (dz+512) << 20
+};
+cudaError_t build_radial_tables(const ProjParams& p, const RadialTables& t, cudaStream_t s);
+// Traced radial coefficients out[i][r][b] (fp32) of sources src[i] (voxel indices), sources
+// 32i..32i+31 all in volume vol_of_warp(i) = (i / 32) / warps_per_volume of rho + vol * volume
+// voxels.  n_src must be a multiple of 32.
+cudaError_t radial_kernels(const ProjParams& p, const RadialTables& t, const int* src, int n_src,
+                           int warps_per_volume, float* out, cudaStream_t s);
+// Surrogate field fill of the groups not flagged in a.fallback_groups: near block traced as in
+// the Norm pass (row 0), then 16 steps per far ray r from the coefficients
+// coef[src][r*16 + b] (bf16), dropped where the target voxel is outside the image or not
+// tissue; W_s = sum of all stored weights.
+cudaError_t surrogate_fill(const ProjParams& p, const OpArgs& a, const RadialTables& t, const __nv_bfloat16* coef,
+                           const unsigned char* support, cudaStream_t s);
+// Template rows of the surrogate field: row 0 the near block, row 1 + r the 16 bin offsets.
+cudaError_t build_surrogate_template(const ProjParams& p, const RadialTables& t, int* tmpl, int* tmpl_neg,
+                                     cudaStream_t s);
+
+}  // namespace prc
+struct prc_net;
+namespace prc {
+// Whole-volume CNN inference into bf16 coefficients coef[src][2048] (surrogate.cu).
+int surrogate_infer(prc_net* net, const float* rho, int nx, int ny, int nz, int iso, const int* active, int n_active,
+                    float inv_target_scale, __nv_bfloat16* coef, cudaStream_t s);
+// Replaces the coefficients of sources [first, first + n_src) by traced ones (times scale)
+// where their relative L2 difference exceeds threshold; counts them in *replaced.
+// Sources whose far field is poorly represented are flagged: predicted and traced coefficients
+// differ by more than `threshold` (relative L2; skipped when threshold < 0), or more than
+// `beyond` of the traced mass lies past the water-equivalent cutoff distance (rays through lung
+// or air, where the radial bins are coarse).  Without a network (threshold < 0) the traced
+// coefficients are copied into coef.  flags[first + i] is set to 1 for flagged sources.
+cudaError_t surrogate_judge(__nv_bfloat16* coef, const float* traced, int n_src, int first, float threshold,
+                            float beyond, int water_bins, unsigned char* flags, cudaStream_t s);
+int radial_water_bins();
 
 // Target-major field construction (setup only).
 cudaError_t transpose_lengths(const ProjParams& p, const FarField& far, int* len_t32, cudaStream_t s);

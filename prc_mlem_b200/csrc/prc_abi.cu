@@ -70,6 +70,8 @@ struct prc_handle {
     int* vox2src = nullptr;
     float* u = nullptr;  // f / W volume for the gather form of the forward projection
     int64_t far_t_entries = 0;
+    int64_t surrogate_fallbacks = 0;
+    char isotope[8] = {};
     int64_t far_entries = 0;
     int cache_mode = PRC_CACHE_NONE;
     bool trace_near = false;
@@ -233,7 +235,144 @@ static int build_target_major(prc_handle* h, const std::vector<int>& active, siz
     return PRC_OK;
 }
 
-static int create_impl(prc_handle* h, const float* density_host) {
+static int create_impl(prc_handle* h, const float* density_host, prc_net* net = nullptr, bool surrogate = false,
+                       float target_scale = 1.0f, float fallback_nrmse = 0.0f, int64_t* fallbacks = nullptr);
+
+// The surrogate field (prc_create_surrogate).  Same stream format as the stored field; the
+// template has 1 + 2 n_rays rows: the near block, the exact steps of every far ray, and the 16
+// radial bins of every far ray.  A group whose sources the tracer judges poorly represented
+// (fallback) stores the near block and its exact ray steps (filled by the Norm pass); every
+// other group stores the near block and 16 radial coefficients per ray (surrogate_fill).
+static int build_surrogate_field(prc_handle* h, prc_net* net, float target_scale, float fallback_nrmse,
+                                 int64_t* fallbacks) {
+    ProjParams& p = h->params;
+    const Grid& g = h->g;
+    const bool bf16 = h->opts.precision == PRC_PRECISION_BF16;
+    const int n_rays = h->opts.rays;
+    const int march_len = (int)(((long long)g.nx + g.ny + g.nz + 6) / 4 * 4);
+    if (march_len >= 65535) return fail(PRC_ERR_LIMIT, "volume too large for the surrogate field");
+    RadialTables tab;
+    PRC_CUDA(h->alloc(&tab.bin_of, (size_t)n_rays * march_len));
+    PRC_CUDA(h->alloc(&tab.offset, (size_t)n_rays * kRadialBins));
+    PRC_CUDA(h->alloc(&tab.xyz, (size_t)n_rays * kRadialBins));
+    ProjParams pm = p;
+    pm.tmpl_len = march_len;
+    PRC_CUDA(build_radial_tables(pm, tab, h->stream));
+    __nv_bfloat16* coef = nullptr;
+    const size_t n_coef = (size_t)h->n_active * n_rays * kRadialBins;
+    PRC_CUDA(cudaMalloc(&coef, n_coef * sizeof(__nv_bfloat16)));
+    struct FreeDev {
+        void* p;
+        ~FreeDev() { cudaFree(p); }
+    } free_coef{coef};
+    static const char* kIsos[3] = {"18F", "68Ga", "82Rb"};
+    int iso = -1;
+    for (int i = 0; i < 3; ++i)
+        if (std::strcmp(h->isotope, kIsos[i]) == 0) iso = i;
+    if (net && (iso < 0 || n_rays != 128))
+        return fail(PRC_ERR_ARGUMENT, "the surrogate network covers 18F, 68Ga and 82Rb with 128 far rays");
+    if (net) {
+        const int rc = surrogate_infer(net, h->rho, g.nx, g.ny, g.nz, iso, h->active, h->n_active,
+                                       1.0f / target_scale, coef, h->stream);
+        if (rc != PRC_OK) return rc;
+    }
+    // The tracer: judge of the predictions, and the coefficients themselves without a network.
+    unsigned char* flags = nullptr;
+    PRC_CUDA(cudaMalloc(&flags, h->n_active));
+    FreeDev free_flags{flags};
+    PRC_CUDA(cudaMemsetAsync(flags, 0, h->n_active, h->stream));
+    if (!net || fallback_nrmse > 0.0f) {
+        const int chunk = 65536;  // sources per traced batch (multiple of 32)
+        float* traced = nullptr;
+        int* srcs = nullptr;
+        PRC_CUDA(cudaMalloc(&traced, (size_t)chunk * n_rays * kRadialBins * sizeof(float)));
+        FreeDev free_traced{traced};
+        PRC_CUDA(cudaMalloc(&srcs, (size_t)chunk * sizeof(int)));
+        FreeDev free_srcs{srcs};
+        std::vector<int> host_src(chunk);
+        std::vector<int> act(h->n_active);
+        PRC_CUDA(cudaMemcpy(act.data(), h->active, act.size() * sizeof(int), cudaMemcpyDeviceToHost));
+        // sources with more than this share of their far mass beyond the water range fall back
+        const float beyond = fallback_nrmse > 0.0f ? 0.02f : 2.0f;
+        for (int first = 0; first < h->n_active; first += chunk) {
+            const int n = std::min(chunk, h->n_active - first);
+            const int padded = (n + kLanes - 1) / kLanes * kLanes;
+            for (int i = 0; i < padded; ++i) host_src[i] = act[first + std::min(i, n - 1)];
+            PRC_CUDA(cudaMemcpyAsync(srcs, host_src.data(), padded * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+            PRC_CUDA(radial_kernels(pm, tab, srcs, padded, 1 << 30, traced, h->stream));
+            PRC_CUDA(surrogate_judge(coef, traced, n, first, net ? fallback_nrmse : -1.0f, beyond,
+                                     radial_water_bins(), flags, h->stream));
+            PRC_CUDA(cudaStreamSynchronize(h->stream));
+        }
+    }
+    std::vector<unsigned char> src_flags(h->n_active);
+    PRC_CUDA(cudaMemcpy(src_flags.data(), flags, src_flags.size(), cudaMemcpyDeviceToHost));
+    std::vector<unsigned char> group_fb(h->n_groups, 0);
+    int64_t fb_sources = 0;
+    for (int i = 0; i < h->n_active; ++i)
+        if (src_flags[i]) group_fb[i / kLanes] = 1;
+    for (int gi = 0; gi < h->n_groups; ++gi)
+        if (group_fb[gi]) fb_sources += std::min(kLanes, h->n_active - gi * kLanes);
+    h->surrogate_fallbacks = fb_sources;
+    if (fallbacks) *fallbacks = fb_sources;
+    unsigned char* d_group_fb = nullptr;
+    PRC_CUDA(h->alloc(&d_group_fb, h->n_groups));
+    PRC_CUDA(cudaMemcpyAsync(d_group_fb, group_fb.data(), group_fb.size(), cudaMemcpyHostToDevice, h->stream));
+
+    // Stream layout: exact lengths from a layout pass for fallback groups, 16 bins otherwise.
+    p.n_rows = 1 + 2 * n_rays;
+    p.tmpl_len = std::max(near_row_steps(), march_len);
+    const size_t rows = (size_t)h->n_groups * p.n_rows;
+    PRC_CUDA(h->alloc(&h->len, rows));
+    PRC_CUDA(h->alloc(&h->group_total, h->n_groups));
+    PRC_CUDA(h->alloc(&h->tmpl, (size_t)p.n_rows * p.tmpl_len));
+    PRC_CUDA(h->alloc(&h->tmpl_neg, (size_t)p.n_rows * p.tmpl_len));
+    p.tmpl = h->tmpl;
+    p.tmpl_neg = h->tmpl_neg;
+    PRC_CUDA(build_surrogate_template(p, tab, h->tmpl, h->tmpl_neg, h->stream));
+    OpArgs la = h->op_args();
+    la.len = h->len;
+    la.group_total = h->group_total;
+    PRC_CUDA(project(Op::Layout, p, la, true, h->stream));
+    std::vector<unsigned short> len(rows);
+    PRC_CUDA(cudaMemcpyAsync(len.data(), h->len, rows * sizeof(unsigned short), cudaMemcpyDeviceToHost, h->stream));
+    PRC_CUDA(cudaStreamSynchronize(h->stream));
+    std::vector<long long> base(h->n_groups + 1);
+    long long run = 0;
+    for (int gi = 0; gi < h->n_groups; ++gi) {
+        unsigned short* l = &len[(size_t)gi * p.n_rows];
+        l[0] = (unsigned short)near_row_steps();
+        for (int r = 0; r < n_rays; ++r) {
+            if (!group_fb[gi]) l[1 + r] = 0;
+            l[1 + n_rays + r] = group_fb[gi] ? 0 : kRadialBins;
+        }
+        base[gi] = run;
+        for (int k = 0; k < p.n_rows; ++k) run += (long long)l[k] * kLanes;
+    }
+    base[h->n_groups] = run;
+    PRC_CUDA(h->alloc(&h->group_base, base.size()));
+    PRC_CUDA(h->alloc(&h->desc, (size_t)(run / (4 * kLanes))));
+    PRC_CUDA(bf16 ? h->alloc(&h->far_field.b16, (size_t)run) : h->alloc(&h->far_field.f32, (size_t)run));
+    PRC_CUDA(cudaMemcpyAsync(h->len, len.data(), rows * sizeof(unsigned short), cudaMemcpyHostToDevice, h->stream));
+    PRC_CUDA(cudaMemcpyAsync(h->group_base, base.data(), base.size() * sizeof(long long), cudaMemcpyHostToDevice,
+                             h->stream));
+    p.src.len = h->len;
+    p.src.group_base = h->group_base;
+    PRC_CUDA(build_descriptors(p, p.src, h->desc, h->stream));
+    p.src.desc = h->desc;
+    OpArgs a = h->op_args();
+    a.fallback_groups = d_group_fb;
+    PRC_CUDA(project(Op::Norm, p, a, true, h->stream));  // exact weights of the fallback groups
+    PRC_CUDA(surrogate_fill(p, a, tab, coef, h->support, h->stream));
+    PRC_CUDA(cudaStreamSynchronize(h->stream));
+    h->far_entries = run;
+    h->cache_mode = PRC_CACHE_SOURCE_MAJOR;
+    h->trace_near = false;
+    return PRC_OK;
+}
+
+static int create_impl(prc_handle* h, const float* density_host, prc_net* net, bool surrogate, float target_scale,
+                       float fallback_nrmse, int64_t* fallbacks) {
     const Grid& g = h->g;
     // Host-side clamp, support and source list (prc.cu:598-613).
     std::vector<float> rho(h->n);
@@ -294,6 +433,15 @@ static int create_impl(prc_handle* h, const float* density_host) {
     const bool bf16 = h->opts.precision == PRC_PRECISION_BF16;
     const size_t elem = bf16 ? 2 : 4;
     h->trace_near = true;
+    if (surrogate) {
+        int rc = build_surrogate_field(h, net, target_scale, fallback_nrmse, fallbacks);
+        if (rc != PRC_OK) return rc;
+        rc = build_target_major(h, active, elem);
+        if (rc != PRC_OK) return rc;
+        if (h->far_t.on()) h->cache_mode = PRC_CACHE_FULL;
+        PRC_CUDA(cudaStreamSynchronize(h->stream));
+        return check_device_error(h);
+    }
     // Stored coefficient field (near block + far rays): size it with a layout pass, then let
     // the Norm pass fill it.  Template rows hold every step a ray can take inside the image
     // plus the padding of the last pack, in whole int4s.
@@ -369,8 +517,9 @@ static int create_impl(prc_handle* h, const float* density_host) {
     return check_device_error(h);
 }
 
-int prc_create(const prc_geometry* geo, const char* isotope, const prc_options* opts_in, const float* density_host,
-               prc_handle** out) {
+static int create_common(const prc_geometry* geo, const char* isotope, const prc_options* opts_in,
+                         const float* density_host, prc_net* net, bool surrogate, float target_scale,
+                         float fallback_nrmse, int64_t* fallbacks, prc_handle** out) {
     if (!out) return fail(PRC_ERR_ARGUMENT, "Invalid argument: null handle pointer");
     *out = nullptr;
     if (!geo || !density_host) return fail(PRC_ERR_ARGUMENT, "Invalid argument: null geometry or density");
@@ -383,7 +532,7 @@ int prc_create(const prc_geometry* geo, const char* isotope, const prc_options* 
         (o.rays & 1) || o.rays > INT_MAX - 31 || !(o.support_rho >= 0) || !(o.air_cap_mm > 0) ||
         !std::isfinite(o.support_rho) || !std::isfinite(o.air_cap_mm) ||
         (o.precision != PRC_PRECISION_FP32 && o.precision != PRC_PRECISION_BF16) || o.cache < PRC_CACHE_NONE ||
-        o.cache > PRC_CACHE_SOURCE_MAJOR)
+        o.cache > PRC_CACHE_SOURCE_MAJOR || !(target_scale > 0) || !(fallback_nrmse >= 0))
         return fail(PRC_ERR_ARGUMENT, "Invalid geometry or solver parameters");
     if (geo->nx > INT_MAX / geo->ny || geo->nx * geo->ny > INT_MAX / geo->nz)
         return fail(PRC_ERR_LIMIT, "Volume exceeds the INT_MAX voxel index limit");
@@ -392,10 +541,11 @@ int prc_create(const prc_geometry* geo, const char* isotope, const prc_options* 
         delete h;
         return fail(PRC_ERR_ISOTOPE, std::string("Unknown isotope ") + (isotope ? isotope : "(null)"));
     }
+    std::strncpy(h->isotope, isotope, sizeof(h->isotope) - 1);
     h->opts = o;
     h->g = Grid{geo->nx, geo->ny, geo->nz, geo->dx, geo->dy, geo->dz, h->model.cutoff, o.support_rho, o.air_cap_mm};
     h->n = (size_t)geo->nx * geo->ny * geo->nz;
-    const int rc = create_impl(h, density_host);
+    const int rc = create_impl(h, density_host, net, surrogate, target_scale, fallback_nrmse, fallbacks);
     if (rc != PRC_OK) {
         const std::string msg = g_last_error;
         prc_destroy(h);
@@ -404,6 +554,17 @@ int prc_create(const prc_geometry* geo, const char* isotope, const prc_options* 
     }
     *out = h;
     return PRC_OK;
+}
+
+int prc_create(const prc_geometry* geo, const char* isotope, const prc_options* opts, const float* density_host,
+               prc_handle** out) {
+    return create_common(geo, isotope, opts, density_host, nullptr, false, 1.0f, 0.0f, nullptr, out);
+}
+
+int prc_create_surrogate(const prc_geometry* geo, const char* isotope, const prc_options* opts,
+                         const float* density_host, prc_net* net, float target_scale, float fallback_nrmse,
+                         int64_t* fallbacks, prc_handle** out) {
+    return create_common(geo, isotope, opts, density_host, net, true, target_scale, fallback_nrmse, fallbacks, out);
 }
 
 int prc_cache_mode(const prc_handle* h, int* mode, int64_t* source_major_entries, int64_t* target_major_entries) {

@@ -249,6 +249,7 @@ __global__ void __launch_bounds__(kBlock) project_kernel(const ProjParams p, con
         if (valid && !live) a.out[s] = 0.0f;
     }
     if (!__any_sync(kFull, live)) return;
+    if (OP == Op::Norm && a.fallback_groups && !a.fallback_groups[group]) return;  // a surrogate group
     const int nx = p.g.nx, ny = p.g.ny;
     const int vx = s % nx, vy = (s / nx) % ny, vz = s / p.nxy;
 
@@ -537,6 +538,149 @@ __global__ void forward_prep_kernel(const int* __restrict__ vox2src, const float
     }
 }
 
+// ---- radial surrogate ------------------------------------------------------------------------
+// kWaterBins equal bins up to the cutoff, the rest equal up to 3.85 x cutoff.
+#ifndef PRC_RADIAL_WATER_BINS
+#define PRC_RADIAL_WATER_BINS 12
+#endif
+constexpr int kWaterBins = PRC_RADIAL_WATER_BINS;
+__device__ __forceinline__ float radial_edge(int b, float cutoff) {
+    return b <= kWaterBins ? cutoff * b / kWaterBins
+                           : cutoff * (1.0f + 2.85f * (b - kWaterBins) / (kRadialBins - kWaterBins));
+}
+__device__ __forceinline__ int radial_bin(float t, float cutoff) {
+    int b = t < cutoff ? (int)(t / cutoff * kWaterBins)
+                       : kWaterBins + (int)((t / cutoff - 1.0f) / 2.85f * (kRadialBins - kWaterBins));
+    return b < 0 ? 0 : (b > kRadialBins - 1 ? kRadialBins - 1 : b);
+}
+
+// Per far ray: the bin of every post-block step, and for every bin the step whose midpoint is
+// closest to the bin centre (its target offset, plain and packed by component).
+__global__ void radial_setup_kernel(const ProjParams p, RadialTables tab) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= p.n_rays) return;
+    const RayStep R = p.far[r];
+    float tx = R.tx, ty = R.ty, tz = R.tz, t = 0.0f;
+    int oi = 0, oj = 0, ok = 0, m = 0;
+    float best[kRadialBins];
+    int best_off[kRadialBins], best_xyz[kRadialBins];
+    for (int b = 0; b < kRadialBins; ++b) best[b] = 3.0e38f, best_off[b] = 0, best_xyz[b] = 512 | (512 << 10) | (512 << 20);
+    const float cutoff = p.g.cutoff;
+    for (int step = 0; m < p.tmpl_len && step < 4 * p.tmpl_len; ++step) {
+        const bool in_block = abs(oi) <= kNearR && abs(oj) <= kNearR && abs(ok) <= kNearR;
+        const float t_next = fminf(tx, fminf(ty, tz));
+        if (!in_block) {
+            const float mid = 0.5f * (t + t_next);
+            tab.bin_of[(size_t)r * p.tmpl_len + m] = (unsigned char)radial_bin(mid, cutoff);
+            for (int b = 0; b < kRadialBins; ++b) {
+                const float centre = 0.5f * (radial_edge(b, cutoff) + radial_edge(b + 1, cutoff));
+                if (fabsf(mid - centre) < best[b] && abs(oi) < 512 && abs(oj) < 512 && abs(ok) < 512) {
+                    best[b] = fabsf(mid - centre);
+                    best_off[b] = (ok * p.g.ny + oj) * p.g.nx + oi;
+                    best_xyz[b] = (oi + 512) | ((oj + 512) << 10) | ((ok + 512) << 20);
+                }
+            }
+            ++m;
+        }
+        t = t_next;
+        if (t_next == tx) oi += R.di, tx += R.dtx;
+        else if (t_next == ty) oj += R.dj, ty += R.dty;
+        else ok += R.dk, tz += R.dtz;
+    }
+    for (int b = 0; b < kRadialBins; ++b) {
+        tab.offset[r * kRadialBins + b] = best_off[b];
+        tab.xyz[r * kRadialBins + b] = best_xyz[b];
+    }
+}
+
+template <bool EXACT>
+__global__ void __launch_bounds__(kBlock) radial_kernel_kernel(ProjParams p, const RadialTables tab, const int* src,
+                                                               int n_src, int warps_per_volume, float* out) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int w = blockIdx.x * kWarps + warp;
+    if (w * kLanes >= n_src) return;
+    p.rho += (size_t)(w / warps_per_volume) * p.nxy * p.g.nz;
+    const int i = w * kLanes + lane;
+    const int s = src[i];
+    const int vx = s % p.g.nx, vy = (s / p.g.nx) % p.g.ny, vz = s / p.nxy;
+    for (int r = 0; r < p.n_rays; ++r) {
+        float c[kRadialBins];
+#pragma unroll
+        for (int b = 0; b < kRadialBins; ++b) c[b] = 0.0f;
+        const unsigned char* bins = tab.bin_of + (size_t)r * p.tmpl_len;
+        march<false, EXACT>(p, p.far[r], true, s, vx, vy, vz, [&](int, float wdep, int, int m) {
+            const int b = bins[m];
+#pragma unroll
+            for (int k = 0; k < kRadialBins; ++k)
+                if (k == b) c[k] += wdep;
+        });
+        float4* o = reinterpret_cast<float4*>(out + ((size_t)i * p.n_rays + r) * kRadialBins);
+#pragma unroll
+        for (int k = 0; k < kRadialBins / 4; ++k) o[k] = make_float4(c[4 * k], c[4 * k + 1], c[4 * k + 2], c[4 * k + 3]);
+    }
+}
+
+// Surrogate field fill (see engine.h); the near block exactly as the Norm pass traces it.
+template <bool EXACT, int FAR_MODE>
+__global__ void __launch_bounds__(kBlock) surrogate_fill_kernel(const ProjParams p, const OpArgs a,
+                                                                const RadialTables tab, const __nv_bfloat16* coef,
+                                                                const unsigned char* support) {
+    extern __shared__ __align__(128) unsigned char dyn_smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int group = blockIdx.x * kWarps + warp;
+    if (group * kLanes >= p.n_active) return;
+    if (a.fallback_groups && a.fallback_groups[group]) return;  // exact weights, filled by the Norm pass
+    const int src = group * kLanes + lane;
+    const bool valid = src < p.n_active;
+    const int s = valid ? p.active[src] : 0;
+    const int nx = p.g.nx, ny = p.g.ny, nz = p.g.nz;
+    const int vx = s % nx, vy = (s / nx) % ny, vz = s / p.nxy;
+    const FarField& f = a.far;
+    const long long gbase = p.src.group_base[group];
+    float acc = 0.0f;
+    float* sum = reinterpret_cast<float*>(dyn_smem) + warp * (kNear * kLanes);
+    for (int q = 0; q < kNear; ++q) sum[q * kLanes + lane] = 0.0f;
+    for (int r = 0; r < kNearRays; ++r)
+        march<true, EXACT>(p, p.near[r], valid, s, vx, vy, vz,
+                           [&](int, float w, int q, int) { sum[q * kLanes + lane] += w; });
+    const float near_scale = (float)p.n_rays / kNearRays;
+    for (int q = 0; q < kNear; ++q) {
+        const int dx = q % kNearSide - kNearR, dy = q / kNearSide % kNearSide - kNearR,
+                  dz = q / (kNearSide * kNearSide) - kNearR;
+        const bool in = (unsigned)(vx + dx) < (unsigned)nx && (unsigned)(vy + dy) < (unsigned)ny &&
+                        (unsigned)(vz + dz) < (unsigned)nz;
+        float w = in ? sum[q * kLanes + lane] * near_scale : 0.0f;
+        if (FAR_MODE == kFieldBF16) w = __bfloat162float(__float2bfloat16_rn(w));
+        acc += w;
+        if (valid) store_weight<FAR_MODE>(f, pack_slot(gbase, q, lane), w);
+    }
+    long long rbase = gbase + (long long)kNearRow * kLanes;
+    for (int r = 0; r < p.n_rays; ++r) {
+        for (int b = 0; b < kRadialBins; ++b) {
+            const int xyz = tab.xyz[r * kRadialBins + b];
+            const int dx = (xyz & 1023) - 512, dy = ((xyz >> 10) & 1023) - 512, dz = ((xyz >> 20) & 1023) - 512;
+            const bool in = (unsigned)(vx + dx) < (unsigned)nx && (unsigned)(vy + dy) < (unsigned)ny &&
+                            (unsigned)(vz + dz) < (unsigned)nz;
+            float w = 0.0f;
+            if (valid && in && support[s + tab.offset[r * kRadialBins + b]])
+                w = fmaxf(__bfloat162float(coef[(size_t)src * (p.n_rays * kRadialBins) + r * kRadialBins + b]), 0.0f);
+            if (FAR_MODE == kFieldBF16) w = __bfloat162float(__float2bfloat16_rn(w));
+            acc += w;
+            if (valid) store_weight<FAR_MODE>(f, pack_slot(rbase, b, lane), w);
+        }
+        rbase += (long long)kRadialBins * kLanes;
+    }
+    if (valid) a.W[src] = acc;
+}
+
+// Rows 1 + n_rays + r of the template: the 16 bin offsets of far ray r (rows 0..n_rays are the
+// near block and the exact ray steps, from template_kernel).
+__global__ void surrogate_template_kernel(const ProjParams p, const int* offset, int* tmpl) {
+    const int r = blockIdx.x;
+    for (int j = threadIdx.x; j < p.tmpl_len; j += blockDim.x)
+        tmpl[(size_t)(1 + p.n_rays + r) * p.tmpl_len + j] = j < kRadialBins ? offset[r * kRadialBins + j] : 0;
+}
+
 template <Op OP, bool EXACT, int NEAR_MODE, int FAR_MODE>
 cudaError_t launch(const ProjParams& p, const OpArgs& a, cudaStream_t s) {
     const int groups = (p.n_active + kLanes - 1) / kLanes;
@@ -626,6 +770,44 @@ cudaError_t forward_prep(const ProjParams& p, const float* W, const float* f, fl
 }
 
 int near_row_steps() { return kNearRow; }
+int radial_water_bins() { return kWaterBins; }
+
+cudaError_t build_radial_tables(const ProjParams& p, const RadialTables& t, cudaStream_t s) {
+    radial_setup_kernel<<<(p.n_rays + 127) / 128, 128, 0, s>>>(p, t);
+    return cudaGetLastError();
+}
+
+cudaError_t radial_kernels(const ProjParams& p, const RadialTables& t, const int* src, int n_src,
+                           int warps_per_volume, float* out, cudaStream_t s) {
+    const int warps = n_src / kLanes;
+    if (warps == 0) return cudaSuccess;
+    if (p.table) radial_kernel_kernel<false><<<(warps + kWarps - 1) / kWarps, kBlock, 0, s>>>(p, t, src, n_src, warps_per_volume, out);
+    else radial_kernel_kernel<true><<<(warps + kWarps - 1) / kWarps, kBlock, 0, s>>>(p, t, src, n_src, warps_per_volume, out);
+    return cudaGetLastError();
+}
+
+cudaError_t surrogate_fill(const ProjParams& p, const OpArgs& a, const RadialTables& t, const __nv_bfloat16* coef,
+                           const unsigned char* support, cudaStream_t s) {
+    const int groups = (p.n_active + kLanes - 1) / kLanes;
+    if (groups == 0) return cudaSuccess;
+    const int blocks = (groups + kWarps - 1) / kWarps;
+    auto launch_fill = [&](auto kernel) {
+        cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kNearSmemBytes);
+        if (e != cudaSuccess) return e;
+        kernel<<<blocks, kBlock, kNearSmemBytes, s>>>(p, a, t, coef, support);
+        return cudaGetLastError();
+    };
+    if (a.far.f32) return p.table ? launch_fill(surrogate_fill_kernel<false, kFieldF32>) : launch_fill(surrogate_fill_kernel<true, kFieldF32>);
+    return p.table ? launch_fill(surrogate_fill_kernel<false, kFieldBF16>) : launch_fill(surrogate_fill_kernel<true, kFieldBF16>);
+}
+
+cudaError_t build_surrogate_template(const ProjParams& p, const RadialTables& t, int* tmpl, int* tmpl_neg,
+                                     cudaStream_t s) {
+    template_kernel<<<(p.n_rays + 128) / 128, 128, 0, s>>>(p, tmpl);
+    surrogate_template_kernel<<<p.n_rays, 128, 0, s>>>(p, t.offset, tmpl);
+    negate_kernel<<<256, 256, 0, s>>>(tmpl, tmpl_neg, (size_t)p.n_rows * p.tmpl_len);
+    return cudaGetLastError();
+}
 
 cudaError_t project(Op op, const ProjParams& p, const OpArgs& a, bool trace_near, cudaStream_t s) {
     switch (op) {

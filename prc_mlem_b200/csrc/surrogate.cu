@@ -465,3 +465,295 @@ int prc_nn_backward(prc_net* n, const float* d_target, int batch, float lr, doub
 }
 
 }  // extern "C"
+
+// ================================================================================================
+// Training data and whole-volume inference.
+// ================================================================================================
+namespace {
+
+constexpr int kPatch = 9, kPatch3 = 729, kHalo = 4;
+constexpr int kEllipsoids = 10;  // parameter slots per volume
+constexpr float kAir = 0.0012f;
+
+__device__ __forceinline__ uint32_t hash32(uint64_t x) {
+    x ^= x >> 33;
+    x *= 0xff51afd7ed558ccdULL;
+    x ^= x >> 33;
+    x *= 0xc4ceb9fe1a85ec53ULL;
+    x ^= x >> 33;
+    return (uint32_t)x;
+}
+__device__ __forceinline__ float unit(uint64_t key) { return (hash32(key) >> 8) * (1.0f / 16777216.0f); }
+
+// Volume v: air, then up to 10 ellipsoids (cx, cy, cz, rx, ry, rz [voxels], density, used) painted
+// in order, then 5 % Gaussian multiplicative jitter (Box-Muller on a hash of the voxel).
+__global__ void paint_kernel(float* rho, int n, const float* ell, int n_vol, uint64_t seed) {
+    const size_t per = (size_t)n * n * n;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < per * n_vol; i += (size_t)gridDim.x * blockDim.x) {
+        const int v = (int)(i / per);
+        const int j = (int)(i % per);
+        const float x = j % n, y = (j / n) % n, z = j / (n * n);
+        float r = kAir;
+        const float* e = ell + (size_t)v * kEllipsoids * 8;
+        for (int k = 0; k < kEllipsoids; ++k, e += 8) {
+            if (e[7] == 0.0f) continue;
+            const float dx = (x - e[0]) / e[3], dy = (y - e[1]) / e[4], dz = (z - e[2]) / e[5];
+            if (dx * dx + dy * dy + dz * dz <= 1.0f) r = e[6];
+        }
+        const float u1 = fmaxf(unit(seed * 0x9E3779B97F4A7C15ULL + 2 * i), 1e-7f), u2 = unit(seed * 0x9E3779B97F4A7C15ULL + 2 * i + 1);
+        const float g = sqrtf(-2.0f * logf(u1)) * cospif(2.0f * u2);
+        rho[i] = fmaxf(r * (1.0f + 0.05f * g), prc::kMinDensity);
+    }
+}
+
+// Sample i of volume v: a hashed random voxel, re-drawn (at most 64 times) until it is tissue.
+__global__ void pick_kernel(const float* rho, int n, int n_vol, int per_vol, float support_rho, uint64_t seed,
+                            int* src) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_vol * per_vol) return;
+    const int v = i / per_vol;
+    const int n3 = n * n * n;
+    int pick = 0;
+    for (int t = 0; t < 64; ++t) {
+        pick = (int)(hash32(seed * 1315423911ULL + (uint64_t)i * 64 + t) % (uint32_t)n3);
+        if (rho[(size_t)v * n3 + pick] >= support_rho) break;
+    }
+    src[i] = pick;
+}
+
+// Patch of sample i: density / 2 (air beyond the volume) and the one-hot isotope.
+__global__ void patch_kernel(const float* rho, int n, int per_vol, const int* src, int n_src, int iso, bf16* out) {
+    const size_t total = (size_t)n_src * kPatch3;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+        const int smp = (int)(i / kPatch3), q = (int)(i % kPatch3);
+        const int v = smp / per_vol, s = src[smp];
+        const int x = s % n + q % kPatch - kHalo, y = (s / n) % n + (q / kPatch) % kPatch - kHalo,
+                  z = s / (n * n) + q / (kPatch * kPatch) - kHalo;
+        const bool in = (unsigned)x < (unsigned)n && (unsigned)y < (unsigned)n && (unsigned)z < (unsigned)n;
+        const float r = in ? rho[(size_t)v * n * n * n + ((size_t)z * n + y) * n + x] : kAir;
+        bf16* o = out + i * kIn;
+        o[0] = __float2bfloat16_rn(0.5f * r);
+        for (int c = 0; c < 3; ++c) o[1 + c] = __float2bfloat16_rn(c == iso ? 1.0f : 0.0f);
+    }
+}
+
+__global__ void scale_kernel(float* x, size_t n, float s) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) x[i] *= s;
+}
+
+// Whole-volume inference.  The input lives on the volume padded by kHalo voxels of air on every
+// side; every layer is a 'same' 3x3x3 convolution on that padded grid (zero beyond it), which
+// equals the valid convolutions of training on the 9^3 patch of every voxel of the volume.
+struct ConvSame {
+    const bf16* x;
+    const bf16* w;
+    const float* bias;
+    bf16* out;
+    int pz, py, px, cin;
+    __device__ bf16 a(int m, int k) const {
+        int z, y, x0, kz, ky, kx;
+        z = m / (py * px);
+        y = (m / px) % py;
+        x0 = m % px;
+        decode3(k / cin, 3, kz, ky, kx);
+        const int zz = z + kz - 1, yy = y + ky - 1, xx = x0 + kx - 1;
+        if ((unsigned)zz >= (unsigned)pz || (unsigned)yy >= (unsigned)py || (unsigned)xx >= (unsigned)px)
+            return __float2bfloat16(0.0f);
+        return x[(((size_t)zz * py + yy) * px + xx) * cin + k % cin];
+    }
+    __device__ bf16 b(int n, int k) const { return w[(size_t)n * 27 * cin + k]; }
+    __device__ void store(int m, int n, float v) const {
+        out[(size_t)m * kC + n] = __float2bfloat16_rn(fmaxf(v + bias[n], 0.0f));
+    }
+};
+
+// Head on the tissue voxels: coef[src][n] = bf16(max(scale * (a4 . wh[n] + bh[n]), 0)).
+struct HeadActive {
+    const bf16* a4;
+    const int* active;
+    const bf16* wh;
+    const float* bh;
+    bf16* coef;
+    int nx, ny, py, px;
+    float scale;
+    __device__ bf16 a(int m, int k) const {
+        const int s = active[m];
+        const int x = s % nx + kHalo, y = (s / nx) % ny + kHalo, z = s / (nx * ny) + kHalo;
+        return a4[(((size_t)z * py + y) * px + x) * kC + k];
+    }
+    __device__ bf16 b(int n, int k) const { return wh[(size_t)n * kC + k]; }
+    __device__ void store(int m, int n, float v) const {
+        coef[(size_t)m * kOut + n] = __float2bfloat16_rn(fmaxf(scale * (v + bh[n]), 0.0f));
+    }
+};
+
+__global__ void padded_input_kernel(const float* rho, int nx, int ny, int nz, int iso, bf16* out) {
+    const int px = nx + 2 * kHalo, py = ny + 2 * kHalo, pz = nz + 2 * kHalo;
+    const size_t total = (size_t)px * py * pz;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+        const int x = (int)(i % px) - kHalo, y = (int)((i / px) % py) - kHalo, z = (int)(i / ((size_t)px * py)) - kHalo;
+        const bool in = (unsigned)x < (unsigned)nx && (unsigned)y < (unsigned)ny && (unsigned)z < (unsigned)nz;
+        const float r = in ? rho[((size_t)z * ny + y) * nx + x] : kAir;
+        bf16* o = out + i * kIn;
+        o[0] = __float2bfloat16_rn(0.5f * r);
+        for (int c = 0; c < 3; ++c) o[1 + c] = __float2bfloat16_rn(c == iso ? 1.0f : 0.0f);
+    }
+}
+
+// Judge (see surrogate_judge in engine.h); one warp per source.
+__global__ void judge_kernel(bf16* coef, const float* traced, int n_src, int first, float threshold, float beyond,
+                             int water_bins, unsigned char* flags) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (warp >= n_src) return;
+    bf16* c = coef + (size_t)(first + warp) * kOut;
+    const float* t = traced + (size_t)warp * kOut;
+    float num = 0.0f, den = 0.0f, mass = 0.0f, far = 0.0f;
+    for (int k = lane; k < kOut; k += 32) {
+        const float tv = t[k];
+        if (threshold >= 0.0f) {
+            const float d = __bfloat162float(c[k]) - tv;
+            num += d * d;
+        } else {
+            c[k] = __float2bfloat16_rn(tv);
+        }
+        den += tv * tv;
+        mass += tv;
+        if ((k & 15) >= water_bins) far += tv;
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+        num += __shfl_xor_sync(0xffffffffu, num, off);
+        den += __shfl_xor_sync(0xffffffffu, den, off);
+        mass += __shfl_xor_sync(0xffffffffu, mass, off);
+        far += __shfl_xor_sync(0xffffffffu, far, off);
+    }
+    const bool bad = (threshold >= 0.0f && num > threshold * threshold * den) || far > beyond * mass;
+    if (lane == 0) flags[first + warp] = bad ? 1 : 0;
+}
+
+}  // namespace
+
+namespace prc {
+
+// Whole-volume inference of `net` on the clamped density rho (device, nx*ny*nz) for isotope
+// index iso; coef[src][2048] for the sources of `active` (device), scaled back by 1 / target
+// scale.  Scratch: two padded activation volumes (allocated and freed here).
+int surrogate_infer(prc_net* net, const float* rho, int nx, int ny, int nz, int iso, const int* active, int n_active,
+                    float inv_target_scale, bf16* coef, cudaStream_t s) {
+    const int px = nx + 2 * kHalo, py = ny + 2 * kHalo, pz = nz + 2 * kHalo;
+    const size_t pv = (size_t)px * py * pz;
+    bf16 *buf0 = nullptr, *buf1 = nullptr;
+    NN_CUDA(cudaMalloc(&buf0, pv * kC * sizeof(bf16)), "surrogate inference");
+    cudaError_t e = cudaMalloc(&buf1, pv * kC * sizeof(bf16));
+    if (e != cudaSuccess) {
+        cudaFree(buf0);
+        return nn_fail(e, "surrogate inference");
+    }
+    struct Free {
+        bf16* a;
+        bf16* b;
+        ~Free() {
+            cudaFree(a);
+            cudaFree(b);
+        }
+    } free_bufs{buf0, buf1};
+    padded_input_kernel<<<1024, 256, 0, s>>>(rho, nx, ny, nz, iso, buf0);
+    bf16* in = buf0;
+    bf16* out = buf1;
+    for (int l = 0; l < 4; ++l) {
+        const int cin = l == 0 ? kIn : kC;
+        ConvSame c{in, net->wb[l], net->b[l], out, pz, py, px, cin};
+        NN_CUDA((run_problem<32>(c, (int)pv, kC, 27 * cin, 1, net->error, s)), "surrogate inference");
+        bf16* t = in;
+        in = out;
+        out = t;
+    }
+    HeadActive h{in, active, net->wb[4], net->b[4], coef, nx, ny, py, px, inv_target_scale};
+    NN_CUDA((run_problem<256>(h, n_active, kOut, kC, 1, net->error, s)), "surrogate inference");
+    NN_CUDA(cudaStreamSynchronize(s), "surrogate inference");
+    unsigned int err = 0;
+    NN_CUDA(cudaMemcpy(&err, net->error, sizeof(err), cudaMemcpyDeviceToHost), "surrogate inference");
+    if (err) return prc::set_last_error("a tensor-core MMA wait gave up"), PRC_ERR_CUDA;
+    return PRC_OK;
+}
+
+cudaError_t surrogate_judge(bf16* coef, const float* traced, int n_src, int first, float threshold, float beyond,
+                            int water_bins, unsigned char* flags, cudaStream_t s) {
+    judge_kernel<<<(n_src * 32 + 255) / 256, 256, 0, s>>>(coef, traced, n_src, first, threshold, beyond, water_bins,
+                                                          flags);
+    return cudaGetLastError();
+}
+
+}  // namespace prc
+
+extern "C" int prc_nn_make_samples(const char* isotope, int n_vol, int side, float spacing_mm, const float* ellipsoids,
+                                   uint64_t seed, int per_vol, void* d_patches, float* d_targets, float target_scale,
+                                   void* stream) {
+    using namespace prc;
+    static const char* kIsos[3] = {"18F", "68Ga", "82Rb"};
+    int iso = -1;
+    for (int i = 0; i < 3; ++i)
+        if (isotope && std::string(isotope) == kIsos[i]) iso = i;
+    if (iso < 0 || n_vol <= 0 || side < 8 || per_vol <= 0 || per_vol % kLanes || !ellipsoids || !d_patches ||
+        !d_targets || !(spacing_mm > 0))
+        return set_last_error("Invalid argument: isotope must be 18F, 68Ga or 82Rb; per_vol a multiple of 32"),
+               PRC_ERR_ARGUMENT;
+    const cudaStream_t s = static_cast<cudaStream_t>(stream);
+    RangeModel model;
+    model.resolve(kIsos[iso]);
+    Grid g{side, side, side, spacing_mm, spacing_mm, spacing_mm, model.cutoff, 0.05f, 50.0f};
+    const int n_rays = 128;
+    const int tmpl_len = ((3 * side + 6) / 4) * 4;
+    const size_t n3 = (size_t)side * side * side;
+    std::vector<void*> allocs;
+    auto alloc = [&](size_t bytes) {
+        void* p = nullptr;
+        if (cudaMalloc(&p, bytes) != cudaSuccess) return (void*)nullptr;
+        allocs.push_back(p);
+        return p;
+    };
+    struct FreeAll {
+        std::vector<void*>& v;
+        ~FreeAll() {
+            for (void* p : v) cudaFree(p);
+        }
+    } free_all{allocs};
+    float* rho = (float*)alloc(n3 * n_vol * sizeof(float));
+    float* ell = (float*)alloc((size_t)n_vol * kEllipsoids * 8 * sizeof(float));
+    int* src = (int*)alloc((size_t)n_vol * per_vol * sizeof(int));
+    RayStep* far = (RayStep*)alloc(n_rays * sizeof(RayStep));
+    RayStep* near = (RayStep*)alloc(kNearRays * sizeof(RayStep));
+    float* table = (float*)alloc((kRangeBins + 1) * sizeof(float));
+    RadialTables tab;
+    tab.bin_of = (unsigned char*)alloc((size_t)n_rays * tmpl_len);
+    tab.offset = (int*)alloc(n_rays * kRadialBins * sizeof(int));
+    tab.xyz = (int*)alloc(n_rays * kRadialBins * sizeof(int));
+    for (void* p : allocs)
+        if (!p) return set_last_error("Device allocation failed in prc_nn_make_samples"), PRC_ERR_MEMORY;
+    if (allocs.size() != 9) return set_last_error("Device allocation failed in prc_nn_make_samples"), PRC_ERR_MEMORY;
+    const std::vector<float> t = model.table();
+    NN_CUDA(cudaMemcpyAsync(table, t.data(), t.size() * sizeof(float), cudaMemcpyHostToDevice, s), "make_samples");
+    NN_CUDA(cudaMemcpyAsync(ell, ellipsoids, (size_t)n_vol * kEllipsoids * 8 * sizeof(float), cudaMemcpyHostToDevice, s),
+            "make_samples");
+    NN_CUDA(setup_rays(g, n_rays, far, near, s), "make_samples");
+    ProjParams p{};
+    p.g = g;
+    p.nxy = side * side;
+    p.n_rays = n_rays;
+    p.rho = rho;
+    p.far = far;
+    p.near = near;
+    p.table = table;
+    p.table_scale = model.table_scale();
+    p.n_branch = model.n;
+    for (int b = 0; b < 3; ++b) p.br[b] = model.br[b];
+    p.tmpl_len = tmpl_len;
+    NN_CUDA(build_radial_tables(p, tab, s), "make_samples");
+    paint_kernel<<<2048, 256, 0, s>>>(rho, side, ell, n_vol, seed);
+    pick_kernel<<<(n_vol * per_vol + 255) / 256, 256, 0, s>>>(rho, side, n_vol, per_vol, g.support_rho, seed, src);
+    NN_CUDA(radial_kernels(p, tab, src, n_vol * per_vol, per_vol / kLanes, d_targets, s), "make_samples");
+    scale_kernel<<<1024, 256, 0, s>>>(d_targets, (size_t)n_vol * per_vol * kOut, target_scale);
+    patch_kernel<<<2048, 256, 0, s>>>(rho, side, per_vol, src, n_vol * per_vol, iso, static_cast<bf16*>(d_patches));
+    NN_CUDA(cudaGetLastError(), "make_samples");
+    NN_CUDA(cudaStreamSynchronize(s), "make_samples");
+    return PRC_OK;
+}
