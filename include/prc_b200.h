@@ -181,6 +181,34 @@ int prc_count_deposits(prc_handle* h, int64_t* deposits);
  * calls share the array: calls that overlap on the GPU (other streams, other threads) race. */
 int prc_sum_static(const float* d_x, int64_t n, double* d_sum, void* stream);
 
+/* ---- batched frames (dynamic PET) ---------------------------------------------------------
+ * No counterpart in the reference.  Many volumes of different grids and isotopes corrected
+ * together: every MAP-EM phase of every frame runs as one launch (the projector's blocks map to
+ * (frame, group); the image updates take one grid row per frame, each with its own FP64
+ * reductions), and the whole schedule of a run is captured once into a CUDA graph and replayed.
+ * Each frame chooses its projector form as prc_create does (stored field while memory lasts,
+ * then the near cache); with `net`, frames of 18F, 68Ga and 82Rb use the learned surrogate
+ * (prc_create_surrogate with target_scale and fallback_nrmse).  The first run autotunes the
+ * projector's warps per block (2, 4 or 8) on one forward projection of every frame. */
+typedef struct prc_frame {
+    prc_geometry geometry;
+    const char* isotope;
+    const float* density_host;
+} prc_frame;
+typedef struct prc_batch prc_batch;
+int prc_batch_create(int n_frames, const prc_frame* frames, const prc_options* opts, prc_net* net,
+                     float target_scale, float fallback_nrmse, prc_batch** out);
+void prc_batch_destroy(prc_batch* b);
+/* d_g[i], d_out[i]: device volumes of frame i.  Enqueued on prc_batch_stream(b); a graph is
+ * captured on the first call and re-captured when the pointers or parameters change. */
+int prc_batch_em_run(prc_batch* b, const float* const* d_g, float* const* d_out, int iterations, float beta,
+                     float gamma, int accelerate);
+int prc_batch_synchronize(prc_batch* b);
+void* prc_batch_stream(const prc_batch* b);
+/* The handle of frame i (owned by the batch), and the autotuned warps per block. */
+int prc_batch_frame(prc_batch* b, int i, prc_handle** out);
+int prc_batch_warps(const prc_batch* b);
+
 /* Waits for all work on the handle's stream. */
 int prc_synchronize(prc_handle* h);
 

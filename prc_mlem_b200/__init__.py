@@ -83,6 +83,14 @@ _SIGNATURES = {
     "prc_create_surrogate": (ctypes.c_int, [ctypes.POINTER(Geometry), ctypes.c_char_p, ctypes.POINTER(Options), _P,
                                             _P, ctypes.c_float, ctypes.c_float, ctypes.POINTER(ctypes.c_int64),
                                             ctypes.POINTER(_P)]),
+"prc_batch_create": (ctypes.c_int, [ctypes.c_int, _P, ctypes.POINTER(Options), _P, ctypes.c_float,
+                                        ctypes.c_float, ctypes.POINTER(_P)]),
+    "prc_batch_destroy": (None, [_P]),
+    "prc_batch_em_run": (ctypes.c_int, [_P, _P, _P, ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_int]),
+    "prc_batch_synchronize": (ctypes.c_int, [_P]),
+    "prc_batch_stream": (_P, [_P]),
+    "prc_batch_frame": (ctypes.c_int, [_P, ctypes.c_int, ctypes.POINTER(_P)]),
+    "prc_batch_warps": (ctypes.c_int, [_P]),
     "prc_nn_gemm_bf16": (ctypes.c_int, [_P, _P, _P, ctypes.c_int, ctypes.c_int, ctypes.c_int, _P, _P]),
     "prc_nn_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(_P)]),
     "prc_nn_destroy": (None, [_P]),
@@ -95,6 +103,10 @@ _SIGNATURES = {
                                            ctypes.c_uint64, ctypes.c_int, _P, _P, ctypes.c_float, _P]),
     "prc_last_error": (ctypes.c_char_p, []),
 }
+
+class Frame(ctypes.Structure):
+    _fields_ = [("geometry", Geometry), ("isotope", ctypes.c_char_p), ("density_host", ctypes.c_void_p)]
+
 
 _lib_handle = None
 
@@ -291,6 +303,67 @@ class Projector:
         _check(lib().prc_em_run_host(self._h, g.ctypes.data, out.ctypes.data, iterations, beta, gamma,
                                      int(accelerate)))
         return out
+
+
+class Batch:
+    """Many frames (density maps of any grid, isotope) corrected together: one launch per MAP-EM
+    phase for all frames, the schedule captured into a CUDA graph (prc_batch_*).
+
+    frames: list of (isotope, density (nz, ny, nx), spacing (dx, dy, dz)).
+    """
+
+    def __init__(self, frames, rays: int = 128, support_rho: float = 0.05, cache: int = PRC_CACHE_FULL,
+                 precision: int = PRC_PRECISION_FP32, surrogate=None, target_scale: float = 1.0,
+                 fallback_nrmse: float = 0.0):
+        self._keep = []
+        arr = (Frame * len(frames))()
+        self.shapes = []
+        for i, (iso, rho, spacing) in enumerate(frames):
+            rho = _host(rho)
+            nz, ny, nx = rho.shape
+            self._keep.append(rho)
+            self.shapes.append(rho.shape)
+            iso_b = iso.encode()
+            self._keep.append(iso_b)
+            arr[i] = Frame(Geometry(nx, ny, nz, *[float(s) for s in spacing]), iso_b, rho.ctypes.data)
+        opts = default_options()
+        opts.rays, opts.support_rho, opts.cache, opts.precision = rays, support_rho, int(cache), int(precision)
+        h = _P()
+        _check(lib().prc_batch_create(len(frames), ctypes.cast(arr, _P), ctypes.byref(opts),
+                                      None if surrogate is None else surrogate.handle, target_scale,
+                                      fallback_nrmse, ctypes.byref(h)))
+        self._h = h
+        self._keep = []
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().prc_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def stream(self) -> int:
+        return lib().prc_batch_stream(self._h) or 0
+
+    @property
+    def warps(self) -> int:
+        return lib().prc_batch_warps(self._h)
+
+    def correct(self, d_gs, d_outs, iterations: int, beta: float = 0.2, gamma: float = 20.0,
+                accelerate: bool = True) -> None:
+        """Enqueues a MAP-EM run of every frame (device tensors, one per frame)."""
+        n = len(d_gs)
+        g = (ctypes.c_void_p * n)(*[_ptr(x) for x in d_gs])
+        o = (ctypes.c_void_p * n)(*[_ptr(x) for x in d_outs])
+        _check(lib().prc_batch_em_run(self._h, g, o, iterations, beta, gamma, int(accelerate)))
+
+    def synchronize(self) -> None:
+        _check(lib().prc_batch_synchronize(self._h))
 
 
 def header_symbols() -> list[str]:

@@ -72,9 +72,9 @@ __device__ __forceinline__ void grid_reduce(double (&v)[NV], const Reduction& r,
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < (n); i += (size_t)gridDim.x * blockDim.x)
 
 // g = support ? max(g_in, 0) : 0 (prc.cu:604-612); f = g; support_sum, eps and the floor.
-__global__ void begin_kernel(const float* __restrict__ g_in, const unsigned char* __restrict__ support,
-                             float* __restrict__ g, float* __restrict__ f, size_t n, int n_active, EmScalars* sc,
-                             Reduction r) {
+__device__ __forceinline__ void begin_body(const float* __restrict__ g_in, const unsigned char* __restrict__ support,
+                                           float* __restrict__ g, float* __restrict__ f, size_t n, int n_active,
+                                           EmScalars* sc, Reduction r) {
     double v[1] = {0.0};
     GRID_STRIDE(i, n) {
         const float x = support[i] ? fmaxf(g_in[i], 0.0f) : 0.0f;
@@ -93,8 +93,8 @@ __global__ void begin_kernel(const float* __restrict__ g_in, const unsigned char
 }
 
 // initialize_kernel (prc.cu:311-314) fused with the FP64 sum that sets the initial rescale.
-__global__ void floor_kernel(float* __restrict__ f, const unsigned char* __restrict__ support, size_t n,
-                             EmScalars* sc, Reduction r) {
+__device__ __forceinline__ void floor_body(float* __restrict__ f, const unsigned char* __restrict__ support, size_t n,
+                                           EmScalars* sc, Reduction r) {
     const float fl = sc->floor;
     double v[1] = {0.0};
     GRID_STRIDE(i, n) {
@@ -107,14 +107,14 @@ __global__ void floor_kernel(float* __restrict__ f, const unsigned char* __restr
 }
 
 // finish_kernel without a residual (prc.cu:325-332, called at prc.cu:671).
-__global__ void init_scale_kernel(float* __restrict__ f, size_t n, const EmScalars* sc) {
+__device__ __forceinline__ void init_scale_body(float* __restrict__ f, size_t n, const EmScalars* sc) {
     const float scale = sc->init_scale;
     GRID_STRIDE(i, n) f[i] = __fmul_rn(f[i], scale);
 }
 
 // Biggs-Andrews prediction, kept above f/2 (prc.cu:318-321).
-__global__ void extrapolate_kernel(const float* __restrict__ f, const float* __restrict__ prev,
-                                   float* __restrict__ y, size_t n, const EmScalars* sc) {
+__device__ __forceinline__ void extrapolate_body(const float* __restrict__ f, const float* __restrict__ prev,
+                                                 float* __restrict__ y, size_t n, const EmScalars* sc) {
     const float lambda = sc->lambda;
     GRID_STRIDE(i, n) {
         const float fi = f[i];
@@ -123,8 +123,8 @@ __global__ void extrapolate_kernel(const float* __restrict__ f, const float* __r
 }
 
 // EM ratio g / max(A y, eps) on the support (prc.cu:270-274).
-__global__ void ratio_kernel(const float* __restrict__ g, float* __restrict__ est,
-                             const unsigned char* __restrict__ support, size_t n, const EmScalars* sc) {
+__device__ __forceinline__ void ratio_body(const float* __restrict__ g, float* __restrict__ est,
+                                           const unsigned char* __restrict__ support, size_t n, const EmScalars* sc) {
     const float eps = sc->eps;
     GRID_STRIDE(i, n) est[i] = support[i] ? g[i] / fmaxf(est[i], eps) : 0.0f;
 }
@@ -136,9 +136,9 @@ __device__ __forceinline__ bool in_grid(const Grid& g, int i, int j, int k) {
 // RDP MAP-EM update over the 26 tissue neighbours (prc.cu:279-309), with the FP64 sum of the
 // new estimate that drives the count rescale (prc.cu:688-691) when SUM is set.
 template <bool SUM>
-__global__ void update_kernel(const float* __restrict__ f, const float* __restrict__ back,
-                              const unsigned char* __restrict__ support, float* __restrict__ next, Grid g,
-                              float beta, float gamma, EmScalars* sc, Reduction r) {
+__device__ __forceinline__ void update_body(const float* __restrict__ f, const float* __restrict__ back,
+                                            const unsigned char* __restrict__ support, float* __restrict__ next,
+                                            const Grid& g, float beta, float gamma, EmScalars* sc, Reduction r) {
     const float eps = sc->eps;
     const size_t n = (size_t)g.nx * g.ny * g.nz;
     double v[1] = {0.0};
@@ -187,9 +187,9 @@ __global__ void update_kernel(const float* __restrict__ f, const float* __restri
 // Count rescale and, when accelerating, the step h = next - y and the two FP64 inner products
 // that give lambda = clamp(<h, h_prev> / <h_prev, h_prev>, 0, 1) (prc.cu:325-332, 693-696).
 template <bool RESIDUAL>
-__global__ void finish_kernel(float* __restrict__ next, float* __restrict__ residual,
-                              const float* __restrict__ h_prev, size_t n, bool use_scale, EmScalars* sc,
-                              Reduction r) {
+__device__ __forceinline__ void finish_body(float* __restrict__ next, float* __restrict__ residual,
+                                            const float* __restrict__ h_prev, size_t n, bool use_scale, EmScalars* sc,
+                                            Reduction r) {
     const float scale = use_scale ? sc->scale : 1.0f;
     double v[2] = {0.0, 0.0};
     GRID_STRIDE(i, n) {
@@ -208,6 +208,59 @@ __global__ void finish_kernel(float* __restrict__ next, float* __restrict__ resi
             const double hh = t[1];
             sc->lambda = hh > 0.0 ? (float)fmin(1.0, fmax(0.0, t[0] / hh)) : 0.0f;
         });
+}
+
+__global__ void begin_kernel(const float* g_in, const unsigned char* support, float* g, float* f, size_t n,
+                             int n_active, EmScalars* sc, Reduction r) {
+    begin_body(g_in, support, g, f, n, n_active, sc, r);
+}
+__global__ void floor_kernel(float* f, const unsigned char* support, size_t n, EmScalars* sc, Reduction r) {
+    floor_body(f, support, n, sc, r);
+}
+__global__ void init_scale_kernel(float* f, size_t n, const EmScalars* sc) { init_scale_body(f, n, sc); }
+__global__ void extrapolate_kernel(const float* f, const float* prev, float* y, size_t n, const EmScalars* sc) {
+    extrapolate_body(f, prev, y, n, sc);
+}
+__global__ void ratio_kernel(const float* g, float* est, const unsigned char* support, size_t n, const EmScalars* sc) {
+    ratio_body(g, est, support, n, sc);
+}
+template <bool SUM>
+__global__ void update_kernel(const float* f, const float* back, const unsigned char* support, float* next, Grid g,
+                              float beta, float gamma, EmScalars* sc, Reduction r) {
+    update_body<SUM>(f, back, support, next, g, beta, gamma, sc, r);
+}
+template <bool RESIDUAL>
+__global__ void finish_kernel(float* next, float* residual, const float* h_prev, size_t n, bool use_scale,
+                              EmScalars* sc, Reduction r) {
+    finish_body<RESIDUAL>(next, residual, h_prev, n, use_scale, sc, r);
+}
+
+// Batched forms: blockIdx.y selects the volume; its grid reductions use its own scratch.
+__global__ void begin_batch_kernel(const EmItem* items, bool initialize_phase, int phase) {
+    const EmItem& it = items[blockIdx.y];
+    if (phase == 0) begin_body(it.g_in, it.v.support, it.g, it.f, it.v.n, it.n_active, it.v.scalars, it.v.red);
+    else if (phase == 1) floor_body(it.f, it.v.support, it.v.n, it.v.scalars, it.v.red);
+    else init_scale_body(it.f, it.v.n, it.v.scalars);
+    (void)initialize_phase;
+}
+__global__ void extrapolate_batch_kernel(const EmItem* items) {
+    const EmItem& it = items[blockIdx.y];
+    extrapolate_body(it.f, it.prev, it.y, it.v.n, it.v.scalars);
+}
+__global__ void ratio_batch_kernel(const EmItem* items) {
+    const EmItem& it = items[blockIdx.y];
+    ratio_body(it.g, it.est, it.v.support, it.v.n, it.v.scalars);
+}
+template <bool SUM>
+__global__ void update_batch_kernel(const EmItem* items, float beta, float gamma, bool accelerate) {
+    const EmItem& it = items[blockIdx.y];
+    update_body<SUM>(accelerate ? it.y : it.f, it.prev, it.v.support, it.est, it.grid, beta, gamma, it.v.scalars,
+                     it.v.red);
+}
+template <bool RESIDUAL>
+__global__ void finish_batch_kernel(const EmItem* items, bool use_scale) {
+    const EmItem& it = items[blockIdx.y];
+    finish_body<RESIDUAL>(it.est, RESIDUAL ? it.y : nullptr, it.h_prev, it.v.n, use_scale, it.v.scalars, it.v.red);
 }
 
 __global__ void sum_kernel(const float* __restrict__ x, size_t n, EmScalars* sc, Reduction r) {
@@ -262,6 +315,31 @@ cudaError_t em_finish(const EmVolumes& v, float* next, float* residual, const fl
     else
         finish_kernel<false><<<kReduceBlocks, kEmThreads, 0, s>>>(next, nullptr, nullptr, v.n, use_scale, v.scalars,
                                                                   v.red);
+    return cudaGetLastError();
+}
+
+cudaError_t em_batch_phase(EmPhase phase, const EmItem* d_items, int n_items, int blocks, float beta, float gamma,
+                           bool accelerate, cudaStream_t s) {
+    if (n_items == 0) return cudaSuccess;
+    if (blocks > kReduceBlocks) blocks = kReduceBlocks;
+    const dim3 grid(blocks, n_items);
+    switch (phase) {
+        case EmPhase::Begin:
+            begin_batch_kernel<<<grid, kEmThreads, 0, s>>>(d_items, true, 0);
+            begin_batch_kernel<<<grid, kEmThreads, 0, s>>>(d_items, true, 1);
+            begin_batch_kernel<<<grid, kEmThreads, 0, s>>>(d_items, true, 2);
+            break;
+        case EmPhase::Extrapolate: extrapolate_batch_kernel<<<grid, kEmThreads, 0, s>>>(d_items); break;
+        case EmPhase::Ratio: ratio_batch_kernel<<<grid, kEmThreads, 0, s>>>(d_items); break;
+        case EmPhase::Update:
+            if (beta > 0.0f) update_batch_kernel<true><<<grid, kEmThreads, 0, s>>>(d_items, beta, gamma, accelerate);
+            else update_batch_kernel<false><<<grid, kEmThreads, 0, s>>>(d_items, beta, gamma, accelerate);
+            break;
+        case EmPhase::Finish:
+            if (accelerate) finish_batch_kernel<true><<<grid, kEmThreads, 0, s>>>(d_items, beta > 0.0f);
+            else finish_batch_kernel<false><<<grid, kEmThreads, 0, s>>>(d_items, beta > 0.0f);
+            break;
+    }
     return cudaGetLastError();
 }
 

@@ -145,6 +145,42 @@ cudaError_t surrogate_judge(__nv_bfloat16* coef, const float* traced, int n_src,
                             float beyond, int water_bins, unsigned char* flags, cudaStream_t s);
 int radial_water_bins();
 
+// ---- batched projection over many volumes (one launch for all) --------------------------------
+enum BatchMode : int {
+    kBatchTraceMarch = 0,      // near block and far rays traced every pass
+    kBatchCacheF32March = 1,   // near cache (fp32 / bf16), far rays traced
+    kBatchCacheBF16March = 2,
+    kBatchFieldF32 = 3,        // stored field, source-major (adjoint gather / forward scatter)
+    kBatchFieldBF16 = 4,
+    kBatchFieldF32T = 5,       // stored field, target-major (forward gather of u = f / W)
+    kBatchFieldBF16T = 6
+};
+struct BatchItem {
+    ProjParams p;
+    OpArgs a;
+    int mode;
+    int first_block;  // blocks [first_block, first_block + blocks) of the launch belong to this item
+    int blocks;
+    int pad;
+};
+// Dynamic shared memory per warp a mode needs.
+size_t batch_smem_per_warp(int mode);
+cudaError_t project_batch(Op op, const BatchItem* d_items, int n_items, int total_blocks, int warps, size_t smem,
+                          cudaStream_t s);
+// Batched forward preparation: gather items get u = f / W (and 0 off the support of out),
+// scatter items get out = 0.
+struct PrepItem {
+    const int* vox2src;
+    const float* W;
+    const float* f;
+    float* u;
+    float* out;
+    long long n;
+    int gather;
+    int pad;
+};
+cudaError_t forward_prep_batch(const PrepItem* d_items, int n_items, cudaStream_t s);
+
 // Target-major field construction (setup only).
 cudaError_t transpose_lengths(const ProjParams& p, const FarField& far, int* len_t32, cudaStream_t s);
 cudaError_t transpose_fill(const ProjParams& p, const FarField& far, const FarField& farT, const int* row_base_t,
@@ -203,6 +239,26 @@ cudaError_t em_update(const EmVolumes& v, const Grid& grid, const float* start, 
 cudaError_t em_finish(const EmVolumes& v, float* next, float* residual, const float* h_prev, bool use_scale,
                       cudaStream_t s);
 cudaError_t em_sum(const EmVolumes& v, const float* x, cudaStream_t s);
+
+// One volume of a batched MAP-EM phase: its scratch and the buffers of the current iteration
+// (start = accelerate ? y : f, the adjoint lands in prev, the new estimate in est).
+struct EmItem {
+    EmVolumes v;
+    Grid grid;
+    int n_active;
+    int pad;
+    const float* g_in;
+    float* g;
+    float* f;
+    float* prev;
+    float* y;
+    float* h_prev;
+    float* est;
+};
+enum class EmPhase : int { Begin = 0, Extrapolate = 1, Ratio = 2, Update = 3, Finish = 4 };
+// One launch (three for Begin) covering every item; blocks per item at most kReduceBlocks.
+cudaError_t em_batch_phase(EmPhase phase, const EmItem* d_items, int n_items, int blocks, float beta, float gamma,
+                           bool accelerate, cudaStream_t s);
 cudaError_t em_mask_copy(const EmVolumes& v, const float* src, float* dst, float fill, cudaStream_t s);
 
 // Sets the message prc_last_error() returns on this thread (for entry points outside prc_abi.cu).

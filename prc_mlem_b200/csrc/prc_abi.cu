@@ -793,3 +793,359 @@ int prc_synchronize(prc_handle* h) {
 }
 
 }  // extern "C"
+
+// ================================================================================================
+// Batched frames: one handle per frame (each with its own projector form, chosen by memory),
+// every MAP-EM phase of every frame in one launch, the whole schedule captured into a CUDA graph.
+// ================================================================================================
+struct prc_batch {
+    std::vector<prc_handle*> frames;
+    cudaStream_t stream = nullptr;
+    int warps = kWarpsDefault;
+    bool tuned = false;
+    void* d_tables = nullptr;
+    size_t table_bytes = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    // what the captured graph was built for
+    std::vector<const float*> key_g;
+    std::vector<float*> key_out;
+    int key_iters = -1, key_accel = -1;
+    float key_beta = -1.0f, key_gamma = -1.0f;
+    static constexpr int kWarpsDefault = 4;
+};
+
+namespace {
+
+int batch_mode(const prc_handle* h, Op op) {
+    if (op == Op::Forward && h->far_t.on()) return h->far_t.b16 ? kBatchFieldBF16T : kBatchFieldF32T;
+    if (h->far_field.on()) return h->far_field.b16 ? kBatchFieldBF16 : kBatchFieldF32;
+    if (!h->trace_near && h->cache.on()) return h->cache.b16 ? kBatchCacheBF16March : kBatchCacheF32March;
+    return kBatchTraceMarch;
+}
+
+void release_graph(prc_batch* b) {
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->exec = nullptr;
+    b->graph = nullptr;
+}
+
+// The enqueued schedule of one batched MAP-EM run, built on the host.
+struct BatchPlan {
+    std::vector<unsigned char> host;  // all tables, uploaded at once
+    struct Launch {
+        int kind;  // 0 EM phase, 1 projector, 2 forward prep, 3 memset (frame, buffer), 4 copy-out (frame)
+        EmPhase phase;
+        Op op;
+        size_t offset;  // of its table in `host`
+        int n_items;
+        int total_blocks;
+        size_t smem;
+        int frame;
+        float* ptr;
+    };
+    std::vector<Launch> launches;
+    template <class T>
+    size_t add(const std::vector<T>& v) {
+        const size_t off = (host.size() + 255) / 256 * 256;
+        host.resize(off + v.size() * sizeof(T));
+        std::memcpy(host.data() + off, v.data(), v.size() * sizeof(T));
+        return off;
+    }
+};
+
+BatchPlan plan_batch(prc_batch* b, const float* const* d_g, float* const* d_out, int iterations, float beta,
+                     float gamma, bool accel, int warps, bool forward_only) {
+    BatchPlan plan;
+    const int n = (int)b->frames.size();
+    struct Bufs {
+        float *f, *prev, *y, *h_prev, *est;
+    };
+    std::vector<Bufs> bufs(n);
+    for (int i = 0; i < n; ++i) {
+        prc_handle* h = b->frames[i];
+        bufs[i] = {h->vol[0], h->vol[1], h->vol[2], h->vol[3], h->vol[4]};
+    }
+    auto em_items = [&]() {
+        std::vector<EmItem> items(n);
+        for (int i = 0; i < n; ++i) {
+            prc_handle* h = b->frames[i];
+            EmItem& it = items[i];
+            it.v = h->em_volumes();
+            it.grid = h->g;
+            it.n_active = h->n_active;
+            it.g_in = d_g ? d_g[i] : nullptr;
+            it.g = h->g_em;
+            it.f = bufs[i].f, it.prev = bufs[i].prev, it.y = bufs[i].y, it.h_prev = bufs[i].h_prev,
+            it.est = bufs[i].est;
+        }
+        return items;
+    };
+    auto em_launch = [&](EmPhase ph, size_t off) {
+        BatchPlan::Launch l{};
+        l.kind = 0, l.phase = ph, l.offset = off, l.n_items = n;
+        plan.launches.push_back(l);
+    };
+    auto projector_launch = [&](Op op, const std::vector<const float*>& in, const std::vector<float*>& out) {
+        std::vector<BatchItem> items(n);
+        int blocks = 0;
+        size_t smem = 0;
+        for (int i = 0; i < n; ++i) {
+            prc_handle* h = b->frames[i];
+            BatchItem& it = items[i];
+            it.p = h->params;
+            it.a = h->op_args();
+            it.a.in = in[i];
+            it.a.out = out[i];
+            it.mode = batch_mode(h, op);
+            const int groups = (h->n_active + kLanes - 1) / kLanes;
+            it.blocks = (groups + warps - 1) / warps;
+            it.first_block = blocks;
+            blocks += it.blocks;
+            smem = std::max(smem, batch_smem_per_warp(it.mode) * warps);
+        }
+        BatchPlan::Launch l{};
+        l.kind = 1, l.op = op, l.offset = plan.add(items), l.n_items = n, l.total_blocks = blocks, l.smem = smem;
+        plan.launches.push_back(l);
+    };
+    auto forward = [&](const std::vector<const float*>& in, const std::vector<float*>& out) {
+        std::vector<PrepItem> prep(n);
+        std::vector<const float*> pin(n);
+        for (int i = 0; i < n; ++i) {
+            prc_handle* h = b->frames[i];
+            const bool gather = h->far_t.on();
+            prep[i] = PrepItem{h->vox2src, h->W, in[i], h->u, out[i], (long long)h->n, gather ? 1 : 0, 0};
+            pin[i] = gather ? h->u : in[i];
+        }
+        BatchPlan::Launch l{};
+        l.kind = 2, l.offset = plan.add(prep), l.n_items = n;
+        plan.launches.push_back(l);
+        projector_launch(Op::Forward, pin, out);
+    };
+    if (forward_only) {  // one forward projection of every frame (autotuning)
+        std::vector<const float*> in(n);
+        std::vector<float*> out(n);
+        for (int i = 0; i < n; ++i) in[i] = d_g[i], out[i] = b->frames[i]->vol[4];
+        forward(in, out);
+        return plan;
+    }
+    // initialisation (prc_em_begin for every frame)
+    for (int i = 0; i < n; ++i)
+        for (float* p : {bufs[i].prev, bufs[i].y, bufs[i].h_prev}) {
+            BatchPlan::Launch l{};
+            l.kind = 3, l.frame = i, l.ptr = p;
+            plan.launches.push_back(l);
+        }
+    em_launch(EmPhase::Begin, plan.add(em_items()));
+    for (int it = 0; it < iterations; ++it) {
+        const size_t items = plan.add(em_items());
+        std::vector<const float*> start(n), est_in(n);
+        std::vector<float*> est(n), prev(n);
+        for (int i = 0; i < n; ++i) {
+            start[i] = accel ? bufs[i].y : bufs[i].f;
+            est[i] = bufs[i].est;
+            est_in[i] = bufs[i].est;
+            prev[i] = bufs[i].prev;
+        }
+        if (accel) em_launch(EmPhase::Extrapolate, items);
+        forward(start, est);
+        em_launch(EmPhase::Ratio, items);
+        projector_launch(Op::Adjoint, est_in, prev);
+        em_launch(EmPhase::Update, items);
+        if (beta > 0.0f || accel) em_launch(EmPhase::Finish, items);
+        for (int i = 0; i < n; ++i) {  // prc.cu:697-700
+            if (accel) {
+                std::swap(bufs[i].y, bufs[i].h_prev);
+                std::swap(bufs[i].prev, bufs[i].f);
+            }
+            std::swap(bufs[i].f, bufs[i].est);
+        }
+    }
+    for (int i = 0; i < n; ++i) {
+        BatchPlan::Launch l{};
+        l.kind = 4, l.frame = i, l.ptr = bufs[i].f;
+        plan.launches.push_back(l);
+    }
+    (void)d_out;
+    return plan;
+}
+
+int enqueue_plan(prc_batch* b, const BatchPlan& plan, float* const* d_out, float beta, float gamma, bool accel,
+                 int warps) {
+    const unsigned char* base = static_cast<const unsigned char*>(b->d_tables);
+    const int em_blocks = std::max(1, std::min(kReduceBlocks, 4096 / std::max(1, (int)b->frames.size())));
+    for (const BatchPlan::Launch& l : plan.launches) {
+        cudaError_t e = cudaSuccess;
+        switch (l.kind) {
+            case 0:
+                e = em_batch_phase(l.phase, reinterpret_cast<const EmItem*>(base + l.offset), l.n_items, em_blocks, beta,
+                                   gamma, accel, b->stream);
+                break;
+            case 1:
+                e = project_batch(l.op, reinterpret_cast<const BatchItem*>(base + l.offset), l.n_items, l.total_blocks,
+                                  warps, l.smem, b->stream);
+                break;
+            case 2:
+                e = forward_prep_batch(reinterpret_cast<const PrepItem*>(base + l.offset), l.n_items, b->stream);
+                break;
+            case 3:
+                e = cudaMemsetAsync(l.ptr, 0, b->frames[l.frame]->n * sizeof(float), b->stream);
+                break;
+            case 4:
+                e = cudaMemcpyAsync(d_out[l.frame], l.ptr, b->frames[l.frame]->n * sizeof(float),
+                                    cudaMemcpyDeviceToDevice, b->stream);
+                break;
+        }
+        if (e != cudaSuccess) return fail(PRC_ERR_CUDA, std::string("CUDA error '") + cudaGetErrorString(e) +
+                                                            "' in the batched MAP-EM schedule");
+    }
+    return PRC_OK;
+}
+
+int upload_plan(prc_batch* b, const BatchPlan& plan) {
+    if (plan.host.size() > b->table_bytes) {
+        if (b->d_tables) cudaFree(b->d_tables);
+        b->d_tables = nullptr;
+        PRC_CUDA(cudaMalloc(&b->d_tables, plan.host.size()));
+        b->table_bytes = plan.host.size();
+    }
+    PRC_CUDA(cudaMemcpyAsync(b->d_tables, plan.host.data(), plan.host.size(), cudaMemcpyHostToDevice, b->stream));
+    PRC_CUDA(cudaStreamSynchronize(b->stream));
+    return PRC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void prc_batch_destroy(prc_batch* b) {
+    if (!b) return;
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    release_graph(b);
+    if (b->d_tables) cudaFree(b->d_tables);
+    for (prc_handle* h : b->frames) prc_destroy(h);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+}
+
+int prc_batch_create(int n_frames, const prc_frame* frames, const prc_options* opts, prc_net* net, float target_scale,
+                     float fallback_nrmse, prc_batch** out) {
+    if (!out || n_frames <= 0 || !frames) return fail(PRC_ERR_ARGUMENT, "Invalid argument");
+    *out = nullptr;
+    if (opts && opts->exact_range) return fail(PRC_ERR_ARGUMENT, "Invalid geometry or solver parameters: batched "
+                                                                   "frames use the survival table");
+    prc_batch* b = new prc_batch();
+    cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete b;
+        return fail(PRC_ERR_CUDA, "cudaStreamCreate failed");
+    }
+    static const char* kNet[3] = {"18F", "68Ga", "82Rb"};
+    for (int i = 0; i < n_frames; ++i) {
+        const prc_frame& f = frames[i];
+        bool learned = false;
+        for (const char* iso : kNet) learned = learned || (net && f.isotope && std::strcmp(f.isotope, iso) == 0);
+        prc_handle* h = nullptr;
+        const int rc = learned ? prc_create_surrogate(&f.geometry, f.isotope, opts, f.density_host, net, target_scale,
+                                                      fallback_nrmse, nullptr, &h)
+                               : prc_create(&f.geometry, f.isotope, opts, f.density_host, &h);
+        if (rc != PRC_OK) {
+            const std::string msg = g_last_error;
+            prc_batch_destroy(b);
+            g_last_error = "frame " + std::to_string(i) + ": " + msg;
+            return rc;
+        }
+        b->frames.push_back(h);
+        const int em = ensure_em(h);
+        if (em != PRC_OK) {
+            const std::string msg = g_last_error;
+            prc_batch_destroy(b);
+            g_last_error = "frame " + std::to_string(i) + ": " + msg;
+            return em;
+        }
+    }
+    *out = b;
+    return PRC_OK;
+}
+
+int prc_batch_em_run(prc_batch* b, const float* const* d_g, float* const* d_out, int iterations, float beta,
+                     float gamma, int accelerate) {
+    if (!b || !d_g || !d_out || iterations < 1 || !(beta >= 0) || !(gamma >= 0))
+        return fail(PRC_ERR_ARGUMENT, "Invalid argument");
+    for (prc_handle* h : b->frames)
+        if (h->n_active == 0) return fail(PRC_ERR_NO_ACTIVITY, "No tissue voxels in a frame: nothing to do");
+    const int n = (int)b->frames.size();
+    if (!b->tuned) {
+        // autotune the projector's warps per block on one forward projection of every frame
+        float best = 3.0e38f;
+        int best_w = prc_batch::kWarpsDefault;
+        cudaEvent_t e0, e1;
+        PRC_CUDA(cudaEventCreate(&e0));
+        PRC_CUDA(cudaEventCreate(&e1));
+        for (int w : {2, 4, 8}) {
+            BatchPlan plan = plan_batch(b, d_g, d_out, 0, beta, gamma, accelerate != 0, w, true);
+            int rc = upload_plan(b, plan);
+            if (rc == PRC_OK) rc = enqueue_plan(b, plan, d_out, beta, gamma, accelerate != 0, w);  // warm-up
+            PRC_CUDA(cudaEventRecord(e0, b->stream));
+            if (rc == PRC_OK) rc = enqueue_plan(b, plan, d_out, beta, gamma, accelerate != 0, w);
+            PRC_CUDA(cudaEventRecord(e1, b->stream));
+            PRC_CUDA(cudaEventSynchronize(e1));
+            if (rc != PRC_OK) return rc;
+            float ms = 0.0f;
+            PRC_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            if (ms < best) best = ms, best_w = w;
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        b->warps = best_w;
+        b->tuned = true;
+    }
+    const std::vector<const float*> key_g(d_g, d_g + n);
+    const std::vector<float*> key_out(d_out, d_out + n);
+    const bool same = b->exec && key_g == b->key_g && key_out == b->key_out && b->key_iters == iterations &&
+                      b->key_beta == beta && b->key_gamma == gamma && b->key_accel == accelerate;
+    if (!same) {
+        release_graph(b);
+        BatchPlan plan = plan_batch(b, d_g, d_out, iterations, beta, gamma, accelerate != 0, b->warps, false);
+        int rc = upload_plan(b, plan);
+        if (rc != PRC_OK) return rc;
+        PRC_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+        rc = enqueue_plan(b, plan, d_out, beta, gamma, accelerate != 0, b->warps);
+        cudaGraph_t graph = nullptr;
+        const cudaError_t ce = cudaStreamEndCapture(b->stream, &graph);
+        if (rc != PRC_OK) {
+            if (graph) cudaGraphDestroy(graph);
+            return rc;
+        }
+        PRC_CUDA(ce);
+        b->graph = graph;
+        PRC_CUDA(cudaGraphInstantiate(&b->exec, b->graph, 0));
+        b->key_g = key_g, b->key_out = key_out, b->key_iters = iterations, b->key_beta = beta;
+        b->key_gamma = gamma, b->key_accel = accelerate;
+    }
+    PRC_CUDA(cudaGraphLaunch(b->exec, b->stream));
+    return PRC_OK;
+}
+
+int prc_batch_synchronize(prc_batch* b) {
+    if (!b) return fail(PRC_ERR_ARGUMENT, "Invalid argument");
+    PRC_CUDA(cudaStreamSynchronize(b->stream));
+    for (prc_handle* h : b->frames) {
+        const int rc = check_device_error(h);
+        if (rc != PRC_OK) return rc;
+    }
+    return PRC_OK;
+}
+
+void* prc_batch_stream(const prc_batch* b) { return b ? (void*)b->stream : nullptr; }
+
+int prc_batch_frame(prc_batch* b, int i, prc_handle** out) {
+    if (!b || !out || i < 0 || i >= (int)b->frames.size()) return fail(PRC_ERR_ARGUMENT, "Invalid argument");
+    *out = b->frames[i];
+    return PRC_OK;
+}
+
+int prc_batch_warps(const prc_batch* b) { return b ? b->warps : 0; }
+
+}  // extern "C"

@@ -27,8 +27,10 @@ namespace prc {
 namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
-constexpr int kWarps = 4;  // groups per block
+constexpr int kWarps = 4;  // groups per block (default launch)
 constexpr int kBlock = kWarps * kLanes;
+constexpr int kMaxWarps = 8;  // largest block of a (batched, autotuned) launch
+constexpr int kMaxBlock = kMaxWarps * kLanes;
 constexpr size_t kNearSmemBytes = size_t(kWarps) * kNear * kLanes * sizeof(float);
 
 // Direction and sub-voxel start (voxel units) of ray k of n.  Rays 2m and 2m+1 are mirror
@@ -222,12 +224,13 @@ __device__ __forceinline__ void store_weight(const FarField& f, long long e, flo
 // from when the far rays are marched; FAR_MODE selects marching or the stored field (which
 // then also holds the near block).  Norm always marches and writes W, and the near cache or
 // the stored field when they are allocated; Layout marches to size the field.
+// The work of one warp (group `group`, warp `warp` of its block): dyn_smem is the block's
+// dynamic shared memory (near tiles or field rings are indexed by warp), bars the warp's
+// kStages mbarriers.
 template <Op OP, bool EXACT, int NEAR_MODE, int FAR_MODE>
-__global__ void __launch_bounds__(kBlock) project_kernel(const ProjParams p, const OpArgs a) {
-    extern __shared__ __align__(128) unsigned char dyn_smem[];
-    __shared__ uint64_t field_bars[kWarps][kStages];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int group = blockIdx.x * kWarps + warp;
+__device__ __forceinline__ void project_group(const ProjParams& p, const OpArgs& a, int group, int warp,
+                                              unsigned char* dyn_smem, uint64_t* bars) {
+    const int lane = threadIdx.x & 31;
     if (group * kLanes >= p.n_active) return;  // the whole warp leaves together
     const int src = group * kLanes + lane;
     const bool valid = src < p.n_active;
@@ -354,7 +357,6 @@ __global__ void __launch_bounds__(kBlock) project_kernel(const ProjParams p, con
         const FarField& fld = kGatherT ? a.farT : a.far;
         const int* tmpl = kGatherT ? p.tmpl_neg : p.tmpl;
         unsigned char* ring = dyn_smem + (size_t)warp * kStages * kChunk;
-        uint64_t* bars = field_bars[warp];
         const long long e0 = lay.group_base[group], e1 = lay.group_base[group + 1];
         const char* src_bytes = (kBase == kFieldF32 ? reinterpret_cast<const char*>(fld.f32)
                                                     : reinterpret_cast<const char*>(fld.b16)) + e0 * kElem;
@@ -448,6 +450,45 @@ __global__ void __launch_bounds__(kBlock) project_kernel(const ProjParams p, con
     } else if constexpr (OP == Op::Count) {
         for (int off = 16; off > 0; off >>= 1) cnt += __shfl_xor_sync(kFull, cnt, off);
         if (lane == 0) atomicAdd(a.count, cnt);
+    }
+}
+
+template <Op OP, bool EXACT, int NEAR_MODE, int FAR_MODE>
+__global__ void __launch_bounds__(kMaxBlock) project_kernel(const ProjParams p, const OpArgs a) {
+    extern __shared__ __align__(128) unsigned char dyn_smem[];
+    __shared__ uint64_t field_bars[kMaxWarps][kStages];
+    const int warp = threadIdx.x >> 5;
+    project_group<OP, EXACT, NEAR_MODE, FAR_MODE>(p, a, blockIdx.x * (blockDim.x >> 5) + warp, warp, dyn_smem,
+                                                  field_bars[warp]);
+}
+
+// Batched launch over many volumes: block b belongs to the item (volume) whose first_block is
+// the largest one <= b; every item carries its own parameters and projector form.
+template <Op OP>
+__global__ void __launch_bounds__(kMaxBlock) project_batch_kernel(const BatchItem* items, int n_items) {
+    extern __shared__ __align__(128) unsigned char dyn_smem[];
+    __shared__ uint64_t field_bars[kMaxWarps][kStages];
+    int lo = 0, hi = n_items - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (items[mid].first_block <= (int)blockIdx.x) lo = mid;
+        else hi = mid - 1;
+    }
+    const ProjParams p = items[lo].p;
+    const OpArgs a = items[lo].a;
+    const int mode = items[lo].mode;
+    const int warp = threadIdx.x >> 5;
+    const int group = ((int)blockIdx.x - items[lo].first_block) * (blockDim.x >> 5) + warp;
+    uint64_t* bars = field_bars[warp];
+    switch (mode) {
+        case kBatchTraceMarch: project_group<OP, false, kTraceNear, kMarch>(p, a, group, warp, dyn_smem, bars); break;
+        case kBatchCacheF32March: project_group<OP, false, kCacheF32, kMarch>(p, a, group, warp, dyn_smem, bars); break;
+        case kBatchCacheBF16March: project_group<OP, false, kCacheBF16, kMarch>(p, a, group, warp, dyn_smem, bars); break;
+        case kBatchFieldF32: project_group<OP, false, kTraceNear, kFieldF32>(p, a, group, warp, dyn_smem, bars); break;
+        case kBatchFieldBF16: project_group<OP, false, kTraceNear, kFieldBF16>(p, a, group, warp, dyn_smem, bars); break;
+        case kBatchFieldF32T: project_group<OP, false, kTraceNear, kFieldF32T>(p, a, group, warp, dyn_smem, bars); break;
+        case kBatchFieldBF16T: project_group<OP, false, kTraceNear, kFieldBF16T>(p, a, group, warp, dyn_smem, bars); break;
+        default: break;
     }
 }
 
@@ -681,6 +722,25 @@ __global__ void surrogate_template_kernel(const ProjParams p, const int* offset,
         tmpl[(size_t)(1 + p.n_rays + r) * p.tmpl_len + j] = j < kRadialBins ? offset[r * kRadialBins + j] : 0;
 }
 
+__global__ void forward_prep_batch_kernel(const PrepItem* items) {
+    const PrepItem it = items[blockIdx.y];
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < it.n; i += (long long)gridDim.x * blockDim.x) {
+        if (!it.gather) {
+            it.out[i] = 0.0f;
+            continue;
+        }
+        const int src = it.vox2src[i];
+        float scale = 0.0f;
+        if (src >= 0) {
+            const float ws = it.W[src], fs = it.f[i];
+            scale = ws > 0.0f ? fs / ws : 0.0f;  // prc.cu:246
+        } else {
+            it.out[i] = 0.0f;
+        }
+        it.u[i] = scale > 0.0f ? scale : 0.0f;
+    }
+}
+
 template <Op OP, bool EXACT, int NEAR_MODE, int FAR_MODE>
 cudaError_t launch(const ProjParams& p, const OpArgs& a, cudaStream_t s) {
     const int groups = (p.n_active + kLanes - 1) / kLanes;
@@ -770,6 +830,35 @@ cudaError_t forward_prep(const ProjParams& p, const float* W, const float* f, fl
 }
 
 int near_row_steps() { return kNearRow; }
+
+size_t batch_smem_per_warp(int mode) {
+    if (mode == kBatchTraceMarch) return (size_t)kNear * kLanes * sizeof(float);
+    if (mode >= kBatchFieldF32) return (size_t)kStages * kChunk;
+    return 0;
+}
+
+cudaError_t project_batch(Op op, const BatchItem* d_items, int n_items, int total_blocks, int warps, size_t smem,
+                          cudaStream_t s) {
+    if (total_blocks == 0 || n_items == 0) return cudaSuccess;
+    if (warps < 1 || warps > kMaxWarps) return cudaErrorInvalidValue;
+    auto go = [&](auto kernel) {
+        if (smem > 48 * 1024) {
+            const cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess) return e;
+        }
+        kernel<<<total_blocks, warps * kLanes, smem, s>>>(d_items, n_items);
+        return cudaGetLastError();
+    };
+    if (op == Op::Forward) return go(project_batch_kernel<Op::Forward>);
+    if (op == Op::Adjoint) return go(project_batch_kernel<Op::Adjoint>);
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t forward_prep_batch(const PrepItem* d_items, int n_items, cudaStream_t s) {
+    if (n_items == 0) return cudaSuccess;
+    forward_prep_batch_kernel<<<dim3(128, n_items), 256, 0, s>>>(d_items);
+    return cudaGetLastError();
+}
 int radial_water_bins() { return kWaterBins; }
 
 cudaError_t build_radial_tables(const ProjParams& p, const RadialTables& t, cudaStream_t s) {
