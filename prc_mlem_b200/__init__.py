@@ -365,6 +365,22 @@ class Batch:
     def synchronize(self) -> None:
         _check(lib().prc_batch_synchronize(self._h))
 
+    def frame_handle(self, i: int) -> int:
+        h = _P()
+        _check(lib().prc_batch_frame(self._h, i, ctypes.byref(h)))
+        return h.value
+
+    def forward(self, i: int, d_in, d_out) -> None:
+        """Forward projection of frame i with its own projector (its handle's stream)."""
+        h = self.frame_handle(i)
+        _check(lib().prc_forward(h, _ptr(d_in), _ptr(d_out), None))
+        _check(lib().prc_synchronize(h))
+
+    def cache_mode(self, i: int):
+        m, e, t = ctypes.c_int(), ctypes.c_int64(), ctypes.c_int64()
+        _check(lib().prc_cache_mode(self.frame_handle(i), ctypes.byref(m), ctypes.byref(e), ctypes.byref(t)))
+        return m.value, e.value, t.value
+
 
 def header_symbols() -> list[str]:
     """Every function the public headers (include/*.h) declare (used to check the exports)."""

@@ -236,7 +236,8 @@ static int build_target_major(prc_handle* h, const std::vector<int>& active, siz
 }
 
 static int create_impl(prc_handle* h, const float* density_host, prc_net* net = nullptr, bool surrogate = false,
-                       float target_scale = 1.0f, float fallback_nrmse = 0.0f, int64_t* fallbacks = nullptr);
+                       float target_scale = 1.0f, float fallback_nrmse = 0.0f, int64_t* fallbacks = nullptr,
+                       bool batch_member = false);
 
 // The surrogate field (prc_create_surrogate).  Same stream format as the stored field; the
 // template has 1 + 2 n_rays rows: the near block, the exact steps of every far ray, and the 16
@@ -372,7 +373,7 @@ static int build_surrogate_field(prc_handle* h, prc_net* net, float target_scale
 }
 
 static int create_impl(prc_handle* h, const float* density_host, prc_net* net, bool surrogate, float target_scale,
-                       float fallback_nrmse, int64_t* fallbacks) {
+                       float fallback_nrmse, int64_t* fallbacks, bool batch_member) {
     const Grid& g = h->g;
     // Host-side clamp, support and source list (prc.cu:598-613).
     std::vector<float> rho(h->n);
@@ -500,7 +501,10 @@ static int create_impl(prc_handle* h, const float* density_host, prc_net* net, b
         size_t free_b = 0, total_b = 0;
         PRC_CUDA(cudaMemGetInfo(&free_b, &total_b));
         const size_t entries = (size_t)h->n_groups * kNear * kLanes;
-        if (entries * elem <= free_b / 4) {
+        // a batch member keeps a near cache whenever it fits: retracing 2048 near rays per
+        // source every pass would dominate the whole batch
+        const size_t limit = batch_member ? (free_b > ((size_t)1 << 30) ? free_b - ((size_t)1 << 30) : 0) : free_b / 4;
+        if (entries * elem <= limit) {
             cudaError_t e = bf16 ? h->alloc(&h->cache.b16, entries) : h->alloc(&h->cache.f32, entries);
             if (e == cudaSuccess) h->trace_near = false, h->cache_mode = PRC_CACHE_NEAR;
             else cudaGetLastError();  // optional: fall back to retracing
@@ -519,7 +523,7 @@ static int create_impl(prc_handle* h, const float* density_host, prc_net* net, b
 
 static int create_common(const prc_geometry* geo, const char* isotope, const prc_options* opts_in,
                          const float* density_host, prc_net* net, bool surrogate, float target_scale,
-                         float fallback_nrmse, int64_t* fallbacks, prc_handle** out) {
+                         float fallback_nrmse, int64_t* fallbacks, prc_handle** out, bool batch_member = false) {
     if (!out) return fail(PRC_ERR_ARGUMENT, "Invalid argument: null handle pointer");
     *out = nullptr;
     if (!geo || !density_host) return fail(PRC_ERR_ARGUMENT, "Invalid argument: null geometry or density");
@@ -545,7 +549,7 @@ static int create_common(const prc_geometry* geo, const char* isotope, const prc
     h->opts = o;
     h->g = Grid{geo->nx, geo->ny, geo->nz, geo->dx, geo->dy, geo->dz, h->model.cutoff, o.support_rho, o.air_cap_mm};
     h->n = (size_t)geo->nx * geo->ny * geo->nz;
-    const int rc = create_impl(h, density_host, net, surrogate, target_scale, fallback_nrmse, fallbacks);
+    const int rc = create_impl(h, density_host, net, surrogate, target_scale, fallback_nrmse, fallbacks, batch_member);
     if (rc != PRC_OK) {
         const std::string msg = g_last_error;
         prc_destroy(h);
@@ -1042,27 +1046,90 @@ int prc_batch_create(int n_frames, const prc_frame* frames, const prc_options* o
         return fail(PRC_ERR_CUDA, "cudaStreamCreate failed");
     }
     static const char* kNet[3] = {"18F", "68Ga", "82Rb"};
+    // While the frames build their projectors (each stored field takes at most half of the free
+    // memory it sees), hold back what they will still need: every frame's MAP-EM volumes and
+    // scratch plus 8 GiB for the caller's data until all are built, and each frame's near cache
+    // (estimated for half its voxels) until that frame is built.
+    auto hold = [](size_t bytes) -> void* {
+        void* p = nullptr;
+        if (cudaMalloc(&p, bytes) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        return p;
+    };
+    size_t em_bytes = (size_t)8 << 30;
+    std::vector<void*> near_hold(n_frames, nullptr);
+    for (int i = 0; i < n_frames; ++i) {
+        const prc_geometry& g = frames[i].geometry;
+        const size_t n = (size_t)std::max(g.nx, 0) * std::max(g.ny, 0) * std::max(g.nz, 0);
+        em_bytes += n * sizeof(float) * 12;
+    }
+    void* held = hold(em_bytes);
+    for (int i = 0; i < n_frames; ++i) {
+        const prc_geometry& g = frames[i].geometry;
+        const size_t n = (size_t)std::max(g.nx, 0) * std::max(g.ny, 0) * std::max(g.nz, 0);
+        near_hold[i] = hold(n / 2 * kNear * sizeof(float));
+    }
+    // First every frame builds its source-major field (half the memory of both copies) or, when
+    // even that does not fit, its near cache; target-major copies are added afterwards.
+    prc_options member;
+    prc_default_options(&member);
+    if (opts) member = *opts;
+    const bool want_full = member.cache == PRC_CACHE_FULL;
+    if (want_full) member.cache = PRC_CACHE_SOURCE_MAJOR;
     for (int i = 0; i < n_frames; ++i) {
         const prc_frame& f = frames[i];
+        if (near_hold[i]) cudaFree(near_hold[i]), near_hold[i] = nullptr;
         bool learned = false;
         for (const char* iso : kNet) learned = learned || (net && f.isotope && std::strcmp(f.isotope, iso) == 0);
         prc_handle* h = nullptr;
-        const int rc = learned ? prc_create_surrogate(&f.geometry, f.isotope, opts, f.density_host, net, target_scale,
-                                                      fallback_nrmse, nullptr, &h)
-                               : prc_create(&f.geometry, f.isotope, opts, f.density_host, &h);
+        const int rc = create_common(&f.geometry, f.isotope, &member, f.density_host, learned ? net : nullptr, learned,
+                                     target_scale, fallback_nrmse, nullptr, &h, true);
         if (rc != PRC_OK) {
             const std::string msg = g_last_error;
+            if (held) cudaFree(held);
+            for (void* p : near_hold)
+                if (p) cudaFree(p);
             prc_batch_destroy(b);
             g_last_error = "frame " + std::to_string(i) + ": " + msg;
             return rc;
         }
         b->frames.push_back(h);
-        const int em = ensure_em(h);
+    }
+    if (held) cudaFree(held);
+    for (int i = 0; i < n_frames; ++i) {
+        const int em = ensure_em(b->frames[i]);
         if (em != PRC_OK) {
             const std::string msg = g_last_error;
             prc_batch_destroy(b);
             g_last_error = "frame " + std::to_string(i) + ": " + msg;
             return em;
+        }
+    }
+    if (want_full) {  // target-major copies (forward as a gather), smallest fields first, while they fit
+        std::vector<int> order(n_frames);
+        for (int i = 0; i < n_frames; ++i) order[i] = i;
+        std::sort(order.begin(), order.end(),
+                  [&](int x, int y) { return b->frames[x]->far_entries < b->frames[y]->far_entries; });
+        for (int i : order) {
+            prc_handle* h = b->frames[i];
+            if (!h->far_field.on()) continue;
+            // keep 8 GiB plus every frame's data and result volumes for the caller
+            size_t free_b2 = 0, total_b2 = 0;
+            if (cudaMemGetInfo(&free_b2, &total_b2) != cudaSuccess) break;
+            size_t caller = (size_t)8 << 30;
+            for (prc_handle* o : b->frames) caller += 3 * o->n * sizeof(float);
+            const size_t need = (size_t)((double)h->far_entries * (h->far_field.b16 ? 2 : 4) * 1.05) + caller;
+            if (free_b2 < need) continue;
+            std::vector<int> act(h->n_active);
+            if (cudaMemcpy(act.data(), h->active, act.size() * sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) break;
+            const int rc = build_target_major(h, act, h->far_field.b16 ? 2 : 4);
+            if (rc != PRC_OK) {
+                prc_batch_destroy(b);
+                return rc;
+            }
+            if (h->far_t.on()) h->cache_mode = PRC_CACHE_FULL;
         }
     }
     *out = b;
