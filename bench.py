@@ -125,6 +125,19 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def aggregate(total_ms: float, steps: int, iterations: int, world: int, device=None) -> tuple[float, float]:
+    """Whole-job throughput of the replicas: every rank corrected its own frame; the time is the
+    maximum over ranks (an all-reduce MAX, the only collective), the units are all ranks'
+    iterations.  Returns (max-over-ranks milliseconds, iterations per second)."""
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        t = torch.tensor([total_ms], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    return total_ms, world * steps * iterations / (total_ms / 1e3)
+
+
 def make_workload(grid):
     from prc_mlem_b200 import phantoms
     rho, truth, spacing = phantoms.torso_phantom(seed=2, shape=tuple(grid))
@@ -226,13 +239,8 @@ def run_ours(args):
         times.append(e0.elapsed_time(e1))
     barrier()
     clock_info = clocks.stop()
-    total_ms = sum(times)
-    if world > 1:
-        t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms, value = aggregate(sum(times), args.steps, args.iterations, world, device="cuda")
     iters_total = world * args.steps * args.iterations
-    value = iters_total / (total_ms / 1e3)
 
     # end to end through the public API from pinned host buffers
     g_pin = torch.from_numpy(g_host).pin_memory()
@@ -249,12 +257,7 @@ def run_ours(args):
             raise RuntimeError(pm.lib().prc_last_error().decode())
         if i >= args.warmup:
             e2e_ms.append(e0.elapsed_time(e1))
-    e2e_total = sum(e2e_ms)
-    if world > 1:
-        t = torch.tensor([e2e_total], dtype=torch.float64, device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_total = float(t.item())
-    e2e_value = iters_total / (e2e_total / 1e3)
+    e2e_total, e2e_value = aggregate(sum(e2e_ms), args.steps, args.iterations, world, device="cuda")
     corrected = out_pin.numpy().copy()
 
     # dominant kernel: time single launches of the stored-field forward and adjoint
@@ -354,10 +357,22 @@ def compare_forms(args, rho, spacing, d_g, stream, l2_flush, value_fp32, correct
     """EM iters/s of the other projector forms on the same data, and their agreement."""
     import torch
     import prc_mlem_b200 as pm
+    from prc_mlem_b200 import surrogate as sg
     out = {"fp32_field": {"iters_per_s": round(value_fp32, 3)}}
-    for name, cache, prec in (("bf16_field", pm.PRC_CACHE_FULL, pm.PRC_PRECISION_BF16),
-                              ("traced", pm.PRC_CACHE_NEAR, pm.PRC_PRECISION_FP32)):
-        Q = pm.Projector(ISOTOPE, rho, spacing, rays=RAYS, support_rho=SUPPORT_RHO, cache=cache, precision=prec)
+    net = sg.load_trained()
+    forms = [("bf16_field", dict(cache=pm.PRC_CACHE_FULL, precision=pm.PRC_PRECISION_BF16)),
+             ("traced", dict(cache=pm.PRC_CACHE_NEAR, precision=pm.PRC_PRECISION_FP32)),
+             ("radial_traced_bf16", dict(precision=pm.PRC_PRECISION_BF16, surrogate="traced"))]
+    if net is not None:
+        forms += [("learned_bf16", dict(precision=pm.PRC_PRECISION_BF16, surrogate=net,
+                                        target_scale=sg.TARGET_SCALE)),
+                  ("learned_judged_bf16", dict(precision=pm.PRC_PRECISION_BF16, surrogate=net,
+                                               target_scale=sg.TARGET_SCALE, fallback_nrmse=0.3))]
+    for name, kw in forms:
+        t_setup = time.perf_counter()
+        Q = pm.Projector(ISOTOPE, rho, spacing, rays=RAYS, support_rho=SUPPORT_RHO, **kw)
+        Q.synchronize()
+        t_setup = time.perf_counter() - t_setup
         s = torch.cuda.ExternalStream(Q.stream)
         d_out = torch.empty_like(d_g)
         steps = max(1, min(args.steps, 3))
@@ -376,7 +391,9 @@ def compare_forms(args, rho, spacing, d_g, stream, l2_flush, value_fp32, correct
         v = args.iterations * steps / (sum(ts) / 1e3)
         img = d_out.cpu().numpy()
         out[name] = {"iters_per_s": round(v, 3), "nrmse_vs_fp32_field": nrmse(img, corrected_fp32),
-                     "device_gb": round(Q.device_bytes / 1e9, 3)}
+                     "device_gb": round(Q.device_bytes / 1e9, 3), "setup_s": round(t_setup, 3)}
+        if "surrogate" in kw:
+            out[name]["exact_fallback_share"] = round(Q.fallbacks / Q.n_active, 4)
         Q.close()
     return out
 
