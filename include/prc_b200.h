@@ -209,8 +209,15 @@ void* prc_batch_stream(const prc_batch* b);
 int prc_batch_frame(prc_batch* b, int i, prc_handle** out);
 int prc_batch_warps(const prc_batch* b);
 
-/* Waits for all work on the handle's stream. */
+/* Waits for all work on the handle's stream; reports PRC_ERR_CUDA if a kernel gave up a
+ * bounded wait since the last check. */
 int prc_synchronize(prc_handle* h);
+
+/* Failure-detection self-test (no counterpart in the reference): launches a kernel whose
+ * mbarrier wait nothing completes, bounded to `rounds` try_wait rounds (1 .. 2^20); the kernel
+ * gives up, raises the handle's error flag and returns, so this returns PRC_ERR_CUDA with the
+ * bounded-wait message while the CUDA context stays usable. */
+int prc_wait_selftest(prc_handle* h, int rounds);
 
 /* Message of the most recent failure on this thread ("" if none). */
 const char* prc_last_error(void);

@@ -79,6 +79,7 @@ _SIGNATURES = {
     "prc_sum": (ctypes.c_int, [_P, _P, ctypes.POINTER(ctypes.c_double), _P]),
     "prc_count_deposits": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int64)]),
     "prc_synchronize": (ctypes.c_int, [_P]),
+    "prc_wait_selftest": (ctypes.c_int, [_P, ctypes.c_int]),
     "prc_sum_static": (ctypes.c_int, [_P, ctypes.c_int64, _P, _P]),
     "prc_create_surrogate": (ctypes.c_int, [ctypes.POINTER(Geometry), ctypes.c_char_p, ctypes.POINTER(Options), _P,
                                             _P, ctypes.c_float, ctypes.c_float, ctypes.POINTER(ctypes.c_int64),

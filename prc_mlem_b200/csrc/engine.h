@@ -181,6 +181,9 @@ struct PrepItem {
 };
 cudaError_t forward_prep_batch(const PrepItem* d_items, int n_items, cudaStream_t s);
 
+// Self-test of the bounded mbarrier wait: a wait that nothing completes, `rounds` rounds.
+cudaError_t wait_selftest(int rounds, unsigned int* error, cudaStream_t s);
+
 // Target-major field construction (setup only).
 cudaError_t transpose_lengths(const ProjParams& p, const FarField& far, int* len_t32, cudaStream_t s);
 cudaError_t transpose_fill(const ProjParams& p, const FarField& far, const FarField& farT, const int* row_base_t,

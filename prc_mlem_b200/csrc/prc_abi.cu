@@ -790,6 +790,12 @@ int prc_count_deposits(prc_handle* h, int64_t* deposits) {
     return PRC_OK;
 }
 
+int prc_wait_selftest(prc_handle* h, int rounds) {
+    if (!h || rounds < 1 || rounds > (1 << 20)) return fail(PRC_ERR_ARGUMENT, "Invalid argument");
+    PRC_CUDA(wait_selftest(rounds, h->error, h->stream));
+    return prc_synchronize(h);
+}
+
 int prc_synchronize(prc_handle* h) {
     if (!h) return fail(PRC_ERR_ARGUMENT, "Invalid argument");
     PRC_CUDA(cudaStreamSynchronize(h->stream));

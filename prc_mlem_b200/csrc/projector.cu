@@ -190,8 +190,8 @@ __device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, unsign
                  "l"(src), "r"(bytes), "r"(smem_u32(bar))
                  : "memory");
 }
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity) {
-    for (int i = 0; i < kWaitRounds; ++i) {
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity, int rounds = kWaitRounds) {
+    for (int i = 0; i < rounds; ++i) {
         unsigned done;
         asm volatile(
             "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
@@ -835,6 +835,23 @@ size_t batch_smem_per_warp(int mode) {
     if (mode == kBatchTraceMarch) return (size_t)kNear * kLanes * sizeof(float);
     if (mode >= kBatchFieldF32) return (size_t)kStages * kChunk;
     return 0;
+}
+
+// The bounded-wait path of the field stream exercised on purpose: one thread waits on an
+// mbarrier that nothing completes (a transaction count that no copy delivers), gives up after
+// `rounds` try_wait rounds, raises the error flag like a field-stream warp does, and returns.
+__global__ void wait_selftest_kernel(int rounds, unsigned int* error) {
+    __shared__ uint64_t bar;
+    if (threadIdx.x != 0) return;
+    mbar_init(&bar, 1);
+    fence_mbarrier_init();
+    mbar_expect_tx(&bar, 16);  // arrival done, 16 bytes expected that never come
+    if (!mbar_wait_bounded(&bar, 0, rounds)) atomicOr(error, 1u);
+}
+
+cudaError_t wait_selftest(int rounds, unsigned int* error, cudaStream_t s) {
+    wait_selftest_kernel<<<1, 32, 0, s>>>(rounds, error);
+    return cudaGetLastError();
 }
 
 cudaError_t project_batch(Op op, const BatchItem* d_items, int n_items, int total_blocks, int warps, size_t smem,

@@ -143,3 +143,15 @@ def test_sum_is_fp64(fixture72):
     P = projector(fixture72)
     d = torch.from_numpy(x).cuda()
     assert abs(P.sum(d) - x.sum(dtype=np.float64)) < 1e-9 * x.sum(dtype=np.float64)
+
+
+def test_bounded_wait_reports_and_the_context_survives(fixture72):
+    """A field-stream wait that nothing completes gives up after its bound, raises the error
+    flag, and the handle keeps working (the failure is reported on the host, no GPU fault)."""
+    rho, x, y, shape, sp = fixture72
+    with pm.Projector("68Ga", rho, sp, rays=32) as P:
+        rc = pm.lib().prc_wait_selftest(P._h, 2000)
+        assert rc == 5  # PRC_ERR_CUDA
+        assert b"bounded wait" in pm.lib().prc_last_error()
+        P.synchronize()  # the flag was cleared when reported
+        assert rel_l2(P.forward_host(x), projector(fixture72).forward_host(x)) < 1e-6
