@@ -347,6 +347,9 @@ __device__ __forceinline__ void project_group(const ProjParams& p, const OpArgs&
         // from shared memory, then one predicated gather per nonzero weight -- zero padding
         // costs no memory traffic -- or one scatter per nonzero weight without the
         // target-major copy.  Entries of lanes that are not sources are zero by construction.
+        // The template offsets are fetched one batch ahead and the descriptors two batches
+        // ahead, so the descriptor -> template -> gather chain exposes one memory latency per
+        // batch instead of three.
         constexpr bool kGatherT = OP == Op::Forward && FAR_MODE >= kFieldF32T;
         constexpr int kBase = FAR_MODE >= kFieldF32T ? FAR_MODE - 2 : FAR_MODE;  // kFieldF32 / kFieldBF16
         constexpr int kElem = kBase == kFieldF32 ? 4 : 2;
@@ -364,7 +367,10 @@ __device__ __forceinline__ void project_group(const ProjParams& p, const OpArgs&
         const long long total = (e1 - e0) * kElem;
         const int n_packs = (int)((e1 - e0) / (kPack * kLanes));
         const int n_chunks = (n_packs + kPacksPerChunk - 1) / kPacksPerChunk;
-        const float* base = a.in + s;  // gather: source + offset (adjoint) or target - offset (forward)
+        // Gathered voxel: source + offset (adjoint) or target - offset (forward).  A 32-bit index
+        // (one wide multiply-add per address); the sum wraps only on padding steps (w = 0),
+        // whose loads are predicated off, since voxel indices stay below INT_MAX.
+        auto gather_index = [&](int o) { return (int)((unsigned)s + (unsigned)o); };
         auto issue = [&](int c) {  // lane 0 only
             const int stage = c % kStages;
             const unsigned bytes = (unsigned)min((long long)kChunk, total - (long long)c * kChunk);
@@ -377,6 +383,14 @@ __device__ __forceinline__ void project_group(const ProjParams& p, const OpArgs&
             for (int c = 0; c < n_chunks && c < kStages; ++c) issue(c);
         }
         __syncwarp();
+        static_assert(kPacksPerChunk % kBatch == 0, "batches stay inside a chunk");
+        auto desc_at = [&](int P) { return P < n_packs ? __ldg(desc + P) : 0; };
+        int4 tn[kBatch];
+        int dq[kBatch];
+#pragma unroll
+        for (int k = 0; k < kBatch; ++k) tn[k] = __ldg(reinterpret_cast<const int4*>(tmpl + desc_at(k)));
+#pragma unroll
+        for (int k = 0; k < kBatch; ++k) dq[k] = desc_at(kBatch + k);
         bool ok = true;
         for (int c = 0; c < n_chunks; ++c) {
             const int packs = min(kPacksPerChunk, n_packs - c * kPacksPerChunk);
@@ -386,15 +400,21 @@ __device__ __forceinline__ void project_group(const ProjParams& p, const OpArgs&
                 break;
             }
             const unsigned char* chunk = ring + stage * kChunk;
-            const int* cdesc = desc + c * kPacksPerChunk;
             for (int b = 0; b < packs; b += kBatch) {
+                const int P0 = c * kPacksPerChunk + b;
                 int o[kBatch * kPack];
                 float w[kBatch * kPack];
+                int4 tc[kBatch];
+#pragma unroll
+                for (int k = 0; k < kBatch; ++k) tc[k] = tn[k];
+#pragma unroll
+                for (int k = 0; k < kBatch; ++k) tn[k] = __ldg(reinterpret_cast<const int4*>(tmpl + dq[k]));
+#pragma unroll
+                for (int k = 0; k < kBatch; ++k) dq[k] = desc_at(P0 + 2 * kBatch + k);
 #pragma unroll
                 for (int k = 0; k < kBatch; ++k) {
                     const bool here = b + k < packs;
-                    const int4 t = here ? __ldg(reinterpret_cast<const int4*>(tmpl + __ldg(cdesc + b + k)))
-                                        : make_int4(0, 0, 0, 0);
+                    const int4 t = tc[k];
                     o[k * kPack] = t.x, o[k * kPack + 1] = t.y, o[k * kPack + 2] = t.z, o[k * kPack + 3] = t.w;
                     if constexpr (kBase == kFieldF32) {
                         const float4 x = here ? reinterpret_cast<const float4*>(chunk + (b + k) * kPackBytes)[lane]
@@ -410,7 +430,7 @@ __device__ __forceinline__ void project_group(const ProjParams& p, const OpArgs&
                 if constexpr (OP == Op::Adjoint || kGatherT) {
                     float v[kBatch * kPack];
 #pragma unroll
-                    for (int u = 0; u < kBatch * kPack; ++u) v[u] = w[u] > 0.0f ? __ldg(base + o[u]) : 0.0f;
+                    for (int u = 0; u < kBatch * kPack; ++u) v[u] = w[u] > 0.0f ? __ldg(a.in + gather_index(o[u])) : 0.0f;
 #pragma unroll
                     for (int u = 0; u < kBatch * kPack; ++u) acc = fmaf(w[u], v[u], acc);
                 } else {
