@@ -53,6 +53,8 @@ def parse():
     ap.add_argument("--iterations", type=int, default=ITERS)
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-forms", action="store_true", help="skip the per-form comparison")
+    ap.add_argument("--no-oracle-check", action="store_true",
+                    help="skip the FP64-oracle NRMSE of every form on a crop of the workload")
     ap.add_argument("--ops", type=int, default=0,
                     help="only run this many forward+adjoint pairs of the headline form (profiling)")
     ap.add_argument("--form", choices=("fp32", "bf16", "traced"), default="fp32",
@@ -296,6 +298,7 @@ def run_ours(args):
             torch.distributed.destroy_process_group()
         return
     cpu = None if args.no_cpu_baseline else cpu_baseline(rho, spacing, g_host, sample_seconds=15.0)
+    check = None if args.no_oracle_check else oracle_check(rho, spacing, g_host, args)
     nz, ny, nx = args.grid
     n_vox = nx * ny * nz
     line = {
@@ -342,6 +345,8 @@ def run_ours(args):
         line["forms"] = forms
     if cpu:
         line["cpu_baseline"] = cpu
+    if check:
+        line["fp64_oracle_check"] = check
     print(json.dumps(line))
     if world > 1:
         torch.distributed.destroy_process_group()
@@ -359,16 +364,7 @@ def compare_forms(args, rho, spacing, d_g, stream, l2_flush, value_fp32, correct
     import prc_mlem_b200 as pm
     from prc_mlem_b200 import surrogate as sg
     out = {"fp32_field": {"iters_per_s": round(value_fp32, 3)}}
-    net = sg.load_trained()
-    forms = [("bf16_field", dict(cache=pm.PRC_CACHE_FULL, precision=pm.PRC_PRECISION_BF16)),
-             ("traced", dict(cache=pm.PRC_CACHE_NEAR, precision=pm.PRC_PRECISION_FP32)),
-             ("radial_traced_bf16", dict(precision=pm.PRC_PRECISION_BF16, surrogate="traced"))]
-    if net is not None:
-        forms += [("learned_bf16", dict(precision=pm.PRC_PRECISION_BF16, surrogate=net,
-                                        target_scale=sg.TARGET_SCALE)),
-                  ("learned_judged_bf16", dict(precision=pm.PRC_PRECISION_BF16, surrogate=net,
-                                               target_scale=sg.TARGET_SCALE, fallback_nrmse=0.3))]
-    for name, kw in forms:
+    for name, kw in projector_forms(pm, sg, sg.load_trained()):
         t_setup = time.perf_counter()
         Q = pm.Projector(ISOTOPE, rho, spacing, rays=RAYS, support_rho=SUPPORT_RHO, **kw)
         Q.synchronize()
@@ -396,6 +392,62 @@ def compare_forms(args, rho, spacing, d_g, stream, l2_flush, value_fp32, correct
             out[name]["exact_fallback_share"] = round(Q.fallbacks / Q.n_active, 4)
         Q.close()
     return out
+
+
+def projector_forms(pm, sg, net):
+    """The projector forms compared with the headline fp32 field: (name, Projector keywords)."""
+    forms = [("bf16_field", dict(cache=pm.PRC_CACHE_FULL, precision=pm.PRC_PRECISION_BF16)),
+             ("traced", dict(cache=pm.PRC_CACHE_NEAR, precision=pm.PRC_PRECISION_FP32)),
+             ("radial_traced_bf16", dict(precision=pm.PRC_PRECISION_BF16, surrogate="traced"))]
+    if net is not None:
+        forms += [("learned_bf16", dict(precision=pm.PRC_PRECISION_BF16, surrogate=net,
+                                        target_scale=sg.TARGET_SCALE)),
+                  ("learned_judged_bf16", dict(precision=pm.PRC_PRECISION_BF16, surrogate=net,
+                                               target_scale=sg.TARGET_SCALE, fallback_nrmse=0.3))]
+    return forms
+
+
+def oracle_check(rho, spacing, g, args):
+    """Every projector form against the FP64 oracle (the CPU restatement of prc.cu with doubles
+    throughout) on a central 64x48x32 crop of the workload: NRMSE of the corrected image after
+    the benchmark's MAP-EM run, and the forward/adjoint identity residual
+    |<Ax, y> - <x, A^T y>| / |<Ax, y>| on seeded random volumes."""
+    import torch
+    import prc_mlem_b200 as pm
+    from prc_mlem_b200 import surrogate as sg
+    from oracle import oracle
+    nz, ny, nx = rho.shape
+    cz, cy, cx = nz // 2, ny // 2, nx // 2
+    sl = (slice(max(cz - 16, 0), cz + 16), slice(max(cy - 24, 0), cy + 24), slice(max(cx - 32, 0), cx + 32))
+    rc, gc = np.ascontiguousarray(rho[sl]), np.ascontiguousarray(g[sl], dtype=np.float32)
+    threads = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    O = oracle.Problem(ISOTOPE, rc, spacing, rays=RAYS, support_rho=SUPPORT_RHO, precision=64, threads=threads)
+    O.normalize()
+    ref = O.correct(gc, args.iterations, BETA, GAMMA, True)
+    t_oracle = time.perf_counter() - t0
+    rng = np.random.default_rng(3)
+    support = np.maximum(rc, 1e-3) >= SUPPORT_RHO
+    x = np.where(support, rng.random(rc.shape), 0.0).astype(np.float32)
+    y = rng.random(rc.shape).astype(np.float32)
+    forms = [("fp32_field", dict(cache=pm.PRC_CACHE_FULL, precision=pm.PRC_PRECISION_FP32))]
+    forms += projector_forms(pm, sg, sg.load_trained())
+    d_g = torch.from_numpy(gc).cuda()
+    out = {}
+    for name, kw in forms:
+        Q = pm.Projector(ISOTOPE, rc, spacing, rays=RAYS, support_rho=SUPPORT_RHO, **kw)
+        d_out = torch.empty_like(d_g)
+        Q.correct(d_g, d_out, args.iterations, BETA, GAMMA, True)
+        Q.synchronize()
+        ax, aty = Q.forward_host(x).astype(np.float64), Q.adjoint_host(y).astype(np.float64)
+        lhs = float(np.sum(ax * y))
+        rhs = float(np.sum(np.where(support, aty, 0.0) * x))
+        out[name] = {"nrmse_vs_fp64": nrmse(d_out.cpu().numpy(), ref),
+                     "identity_residual": abs(lhs - rhs) / abs(lhs)}
+        Q.close()
+    return {"crop": f"{rc.shape[2]}x{rc.shape[1]}x{rc.shape[0]} voxels at the volume centre "
+                    f"({int(support.sum())} tissue voxels)",
+            "oracle_seconds": round(t_oracle, 1), "oracle_threads": threads, "forms": out}
 
 
 # ------------------------------------------------------------------------------- CPU baseline
