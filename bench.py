@@ -287,6 +287,7 @@ def run_ours(args):
     stored_bytes = (far_t_entries if top == "forward" else far_entries) * elem
     traffic = ncu_traffic(f"{top}_{args.form}", stored_bytes) if mode == 2 else None
 
+    quality = image_quality(truth, g_host, corrected) if rank == 0 else None
     forms = None
     if not args.no_forms and rank == 0:
         forms = compare_forms(args, rho, spacing, d_g, stream, l2_flush, value, corrected, P)
@@ -341,6 +342,8 @@ def run_ours(args):
         "gpu_launches": args.steps * (3 + (7 if far_t_entries else 6) * args.iterations),
         "clocks": clock_info,
     }
+    if quality:
+        line["image_quality"] = quality
     if forms:
         line["forms"] = forms
     if cpu:
@@ -391,6 +394,23 @@ def compare_forms(args, rho, spacing, d_g, stream, l2_flush, value_fp32, correct
         if "surrogate" in kw:
             out[name]["exact_fallback_share"] = round(Q.fallbacks / Q.n_active, 4)
         Q.close()
+    return out
+
+
+def image_quality(truth, measured, corrected):
+    """What the correction gains, scored on the device against the known truth with the
+    reference's metrics (prc_mlem_b200.evaluate): the measured data and the corrected image,
+    both scaled by sum(truth) / sum(measured) into the truth's activity units."""
+    from prc_mlem_b200 import evaluate
+    ev = evaluate.Evaluator(truth)
+    scale = float(truth.sum(dtype=np.float64) / measured.sum(dtype=np.float64))
+    keys = ("nrmse", "ssim", "ssim_edge", "edge_nrmse", "rc_hot", "rc_min", "bg_cov", "ring", "halo")
+    out = {"scaling": "both images x sum(truth) / sum(measured)",
+           "hot_regions": ev.metric_settings["hot_region_count"]}
+    for name, img in (("measured", measured), ("corrected", corrected)):
+        m = ev(img.astype(np.float64) * scale)
+        out[name] = {k: (None if m[k] is None else round(m[k], 5)) for k in keys}
+    ev.close()
     return out
 
 

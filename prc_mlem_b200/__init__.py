@@ -102,6 +102,11 @@ _SIGNATURES = {
     "prc_nn_backward": (ctypes.c_int, [_P, _P, ctypes.c_int, ctypes.c_float, ctypes.POINTER(ctypes.c_double), _P]),
     "prc_nn_make_samples": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_float, _P,
                                            ctypes.c_uint64, ctypes.c_int, _P, _P, ctypes.c_float, _P]),
+    "prc_eval_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _P, _P, _P, ctypes.c_int, _P, _P,
+                                       _P, ctypes.c_double, ctypes.POINTER(ctypes.c_void_p)]),
+    "prc_eval_sums": (ctypes.c_int, [_P, _P, _P, _P]),
+    "prc_eval_sums_f64": (ctypes.c_int, [_P, _P, _P, _P]),
+    "prc_eval_destroy": (None, [_P]),
     "prc_last_error": (ctypes.c_char_p, []),
 }
 
