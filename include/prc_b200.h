@@ -209,6 +209,15 @@ void* prc_batch_stream(const prc_batch* b);
 int prc_batch_frame(prc_batch* b, int i, prc_handle** out);
 int prc_batch_warps(const prc_batch* b);
 
+/* Projection timing (no counterpart in the reference, whose main() prints only wall-clock
+ * totals): while timing is on, every forward and adjoint projection launch of the handle --
+ * those inside prc_em_iterate included -- is bracketed by CUDA events on its stream.
+ * prc_timing(h, 1) starts a new measurement, prc_timing(h, 0) stops recording; prc_timing_read
+ * waits for the recorded events and returns the summed device milliseconds and the number of
+ * launches of each kind since the start. */
+int prc_timing(prc_handle* h, int enable);
+int prc_timing_read(prc_handle* h, double* forward_ms, int64_t* n_forward, double* adjoint_ms, int64_t* n_adjoint);
+
 /* Waits for all work on the handle's stream; reports PRC_ERR_CUDA if a kernel gave up a
  * bounded wait since the last check. */
 int prc_synchronize(prc_handle* h);

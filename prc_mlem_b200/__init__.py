@@ -107,6 +107,9 @@ _SIGNATURES = {
     "prc_eval_sums": (ctypes.c_int, [_P, _P, _P, _P]),
     "prc_eval_sums_f64": (ctypes.c_int, [_P, _P, _P, _P]),
     "prc_eval_destroy": (None, [_P]),
+    "prc_timing": (ctypes.c_int, [_P, ctypes.c_int]),
+    "prc_timing_read": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int64),
+                                       ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int64)]),
     "prc_last_error": (ctypes.c_char_p, []),
 }
 
@@ -252,6 +255,17 @@ class Projector:
     @property
     def stream(self) -> int:
         return lib().prc_stream(self._h) or 0
+
+    def timing(self, enable: bool) -> None:
+        """Bracket every projection launch with CUDA events (True starts a new measurement)."""
+        _check(lib().prc_timing(self._h, int(bool(enable))))
+
+    def timing_read(self) -> dict:
+        """Summed device milliseconds and launch counts of the projections since timing(True)."""
+        fm, am, fn, an = ctypes.c_double(), ctypes.c_double(), ctypes.c_int64(), ctypes.c_int64()
+        _check(lib().prc_timing_read(self._h, ctypes.byref(fm), ctypes.byref(fn), ctypes.byref(am), ctypes.byref(an)))
+        return {"forward_ms": fm.value, "forward_launches": fn.value, "adjoint_ms": am.value,
+                "adjoint_launches": an.value}
 
     # device-memory operators -------------------------------------------------------------
     def forward(self, d_in, d_out, stream=None) -> None:

@@ -91,6 +91,10 @@ struct prc_handle {
     int64_t bytes = 0;
 
     std::vector<void*> allocations;
+    // projection timing (prc_timing): start/end event pairs of forward and adjoint launches
+    bool timing = false;
+    std::vector<cudaEvent_t> events[2];
+    size_t events_used[2] = {0, 0};
 
     template <class T>
     cudaError_t alloc(T** p, size_t count) {
@@ -159,6 +163,8 @@ void prc_destroy(prc_handle* h) {
     if (!h) return;
     if (h->stream) cudaStreamSynchronize(h->stream);
     for (void* p : h->allocations) cudaFree(p);
+    for (auto& pool : h->events)
+        for (cudaEvent_t e : pool) cudaEventDestroy(e);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
 }
@@ -613,6 +619,44 @@ int prc_device_bytes(const prc_handle* h, int64_t* b) {
 
 void* prc_stream(const prc_handle* h) { return h ? (void*)h->stream : nullptr; }
 
+// Records the next event of pool `kind` (0 forward, 1 adjoint) when timing is on; events come
+// in start / end pairs around each projection launch.
+static cudaError_t timing_mark(prc_handle* h, int kind, cudaStream_t s) {
+    if (!h->timing) return cudaSuccess;
+    std::vector<cudaEvent_t>& pool = h->events[kind];
+    if (h->events_used[kind] == pool.size()) {
+        cudaEvent_t e = nullptr;
+        const cudaError_t err = cudaEventCreate(&e);
+        if (err != cudaSuccess) return err;
+        pool.push_back(e);
+    }
+    return cudaEventRecord(pool[h->events_used[kind]++], s);
+}
+
+int prc_timing(prc_handle* h, int enable) {
+    if (!h) return fail(PRC_ERR_ARGUMENT, "Invalid argument");
+    if (enable) h->events_used[0] = h->events_used[1] = 0;
+    h->timing = enable != 0;
+    return PRC_OK;
+}
+
+int prc_timing_read(prc_handle* h, double* forward_ms, int64_t* n_forward, double* adjoint_ms, int64_t* n_adjoint) {
+    if (!h || !forward_ms || !n_forward || !adjoint_ms || !n_adjoint) return fail(PRC_ERR_ARGUMENT, "Invalid argument");
+    double* total[2] = {forward_ms, adjoint_ms};
+    int64_t* count[2] = {n_forward, n_adjoint};
+    for (int kind = 0; kind < 2; ++kind) {
+        *total[kind] = 0.0;
+        *count[kind] = (int64_t)(h->events_used[kind] / 2);
+        for (size_t i = 0; i + 1 < h->events_used[kind]; i += 2) {
+            PRC_CUDA(cudaEventSynchronize(h->events[kind][i + 1]));
+            float ms = 0.0f;
+            PRC_CUDA(cudaEventElapsedTime(&ms, h->events[kind][i], h->events[kind][i + 1]));
+            *total[kind] += ms;
+        }
+    }
+    return PRC_OK;
+}
+
 int prc_forward(prc_handle* h, const float* d_in, float* d_out, void* stream) {
     if (!h || !d_in || !d_out) return fail(PRC_ERR_ARGUMENT, "Invalid argument");
     const cudaStream_t s = h->pick(stream);
@@ -622,11 +666,12 @@ int prc_forward(prc_handle* h, const float* d_in, float* d_out, void* stream) {
     if (h->far_t.on()) {  // gather form: u = f / W, then out[t] = sum_k T_tk u[t - o_k]
         PRC_CUDA(forward_prep(h->params, h->W, d_in, h->u, d_out, s));
         a.in = h->u;
-        PRC_CUDA(project(Op::Forward, h->params, a, h->trace_near, s));
-        return PRC_OK;
+    } else {
+        PRC_CUDA(cudaMemsetAsync(d_out, 0, h->n * sizeof(float), s));
     }
-    PRC_CUDA(cudaMemsetAsync(d_out, 0, h->n * sizeof(float), s));
+    PRC_CUDA(timing_mark(h, 0, s));
     PRC_CUDA(project(Op::Forward, h->params, a, h->trace_near, s));
+    PRC_CUDA(timing_mark(h, 0, s));
     return PRC_OK;
 }
 
@@ -635,7 +680,10 @@ int prc_adjoint(prc_handle* h, const float* d_in, float* d_out, void* stream) {
     OpArgs a = h->op_args();
     a.in = d_in;
     a.out = d_out;
-    PRC_CUDA(project(Op::Adjoint, h->params, a, h->trace_near, h->pick(stream)));
+    const cudaStream_t s = h->pick(stream);
+    PRC_CUDA(timing_mark(h, 1, s));
+    PRC_CUDA(project(Op::Adjoint, h->params, a, h->trace_near, s));
+    PRC_CUDA(timing_mark(h, 1, s));
     return PRC_OK;
 }
 

@@ -152,3 +152,23 @@ def test_state_errors(fixture72):
         d = torch.from_numpy(x).cuda()
         with pytest.raises(pm.PrcError):
             P.correct(d, d, -1)
+
+
+def test_projection_timing_counts_the_launches_of_a_run(fixture72):
+    """prc_timing brackets every projection of prc_em_iterate with events: a 3-iteration run is
+    3 forward and 3 adjoint launches with positive device time; nothing is recorded when off."""
+    rho, x, y, shape, sp = fixture72
+    P = pm.Projector("68Ga", rho, sp, rays=32)
+    d_g = torch.from_numpy(np.ascontiguousarray(x, np.float32)).cuda()
+    d_out = torch.empty_like(d_g)
+    P.timing(True)
+    P.correct(d_g, d_out, 3, 0.03, 20.0, True)
+    t = P.timing_read()
+    assert t["forward_launches"] == 3 and t["adjoint_launches"] == 3
+    assert t["forward_ms"] > 0 and t["adjoint_ms"] > 0
+    P.timing(False)
+    P.correct(d_g, d_out, 2, 0.03, 20.0, True)
+    assert P.timing_read()["forward_launches"] == 3
+    P.timing(True)
+    assert P.timing_read()["forward_launches"] == 0
+    P.close()
