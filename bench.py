@@ -294,9 +294,12 @@ def run_ours(args):
     stored_bytes = (far_t_entries if top == "forward" else far_entries) * elem
     traffic = ncu_traffic(f"{top}_{args.form}", stored_bytes) if mode == 2 else None
 
-    quality = image_quality(truth, g_host, corrected) if rank == 0 else None
+    # the single-GPU line also carries the per-form comparison, the CPU baseline, the FP64-oracle
+    # check and the image quality; a multi-GPU run reports its timing only
+    single = world == 1
+    quality = image_quality(truth, g_host, corrected) if single else None
     forms = None
-    if not args.no_forms and rank == 0:
+    if not args.no_forms and single:
         forms = compare_forms(args, rho, spacing, d_g, stream, l2_flush, value, corrected, P)
 
     if world > 1:
@@ -305,8 +308,8 @@ def run_ours(args):
         if world > 1:
             torch.distributed.destroy_process_group()
         return
-    cpu = None if args.no_cpu_baseline else cpu_baseline(rho, spacing, g_host, sample_seconds=15.0)
-    check = None if args.no_oracle_check else oracle_check(rho, spacing, g_host, args)
+    cpu = None if args.no_cpu_baseline or not single else cpu_baseline(rho, spacing, g_host, sample_seconds=15.0)
+    check = None if args.no_oracle_check or not single else oracle_check(rho, spacing, g_host, args)
     nz, ny, nx = args.grid
     n_vox = nx * ny * nz
     line = {
