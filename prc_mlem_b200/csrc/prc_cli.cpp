@@ -14,6 +14,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 namespace {
@@ -159,27 +160,58 @@ std::string with_suffix(const std::string& path, const std::string& suffix) {
     return dot == std::string::npos || dot <= start ? path + suffix : path.substr(0, dot) + suffix + path.substr(dot);
 }
 
-void read_raw(const std::string& path, std::vector<float>* v) {  // prc.cu:339-347
+// Reads exactly v->size() floats; false when the file is missing, short or too long.
+bool read_raw_ok(const std::string& path, std::vector<float>* v) {  // prc.cu:339-347
     FILE* fp = fopen(path.c_str(), "rb");
-    if (!fp || fread(v->data(), sizeof(float), v->size(), fp) != v->size() || fgetc(fp) != EOF || ferror(fp)) {
-        fprintf(stderr, "Expected exactly %zu float32 values in %s\n", v->size(), path.c_str());
-        die();
-    }
-    fclose(fp);
+    const bool ok = fp && fread(v->data(), sizeof(float), v->size(), fp) == v->size() && fgetc(fp) == EOF && !ferror(fp);
+    if (fp) fclose(fp);
+    return ok;
 }
 
-void save_image(const std::string& path, const std::vector<float>& host) {  // prc.cu:349-360
+void read_failed(const std::string& path, size_t n) {
+    fprintf(stderr, "Expected exactly %zu float32 values in %s\n", n, path.c_str());
+    die();
+}
+
+// Writes an all-finite image; otherwise returns the reference's message and writes nothing.
+std::string save_image_ok(const std::string& path, const std::vector<float>& host) {  // prc.cu:349-360
     for (float value : host)
-        if (!std::isfinite(value)) {
-            fprintf(stderr, "Non-finite output: %s\n", path.c_str());
-            die();
-        }
+        if (!std::isfinite(value)) return "Non-finite output: " + path;
     FILE* fp = fopen(path.c_str(), "wb");
-    if (!fp || fwrite(host.data(), sizeof(float), host.size(), fp) != host.size() || fclose(fp) != 0) {
-        fprintf(stderr, "Cannot write %s\n", path.c_str());
+    if (!fp || fwrite(host.data(), sizeof(float), host.size(), fp) != host.size()) {
+        if (fp) fclose(fp);
+        return "Cannot write " + path;
+    }
+    if (fclose(fp) != 0) return "Cannot write " + path;
+    return "";
+}
+
+void save_image(const std::string& path, const std::vector<float>& host) {
+    const std::string err = save_image_ok(path, host);
+    if (!err.empty()) {
+        fprintf(stderr, "%s\n", err.c_str());
         die();
     }
 }
+
+// Checkpoints (--save-every) are written by a helper thread while the GPU runs the next
+// iterations; a write error is reported, with the reference's message, before anything else is
+// written.
+struct CheckpointWriter {
+    std::thread thread;
+    std::vector<float> image;
+    std::string error;
+    void finish() {
+        if (thread.joinable()) thread.join();
+        if (!error.empty()) {
+            fprintf(stderr, "%s\n", error.c_str());
+            die();
+        }
+    }
+    void start(const std::string& path) {
+        thread = std::thread([this, path] { error = save_image_ok(path, image); });
+    }
+};
 
 void check(int rc) {
     if (rc != PRC_OK) {
@@ -211,8 +243,12 @@ int main(int argc, char** argv) {
 
     const double t0 = now_s();
     std::vector<float> rho(n), img(n);
-    read_raw(o.density, &rho);
-    read_raw(o.input, &img);
+    bool img_ok = false;
+    std::thread reader([&] { img_ok = read_raw_ok(o.input, &img); });  // both files at once
+    const bool rho_ok = read_raw_ok(o.density, &rho);
+    reader.join();
+    if (!rho_ok) read_failed(o.density, n);  // the reference's order: density first
+    if (!img_ok) read_failed(o.input, n);
     size_t n_active = 0;
     double input_sum = 0.0, support_sum = 0.0;
     for (size_t i = 0; i < n; ++i) {  // prc.cu:598-613
@@ -281,6 +317,7 @@ int main(int argc, char** argv) {
     } else {
         check(prc_em_begin_host(h, img.data()));
         t = now_s();
+        CheckpointWriter writer;
         for (int it = 1; it <= o.iterations; ++it) {
             check(prc_em_iterate(h, 1, o.beta, o.gamma, o.accelerate, nullptr));
             if (it == 1 || it % 10 == 0 || it == o.iterations) {
@@ -290,10 +327,13 @@ int main(int argc, char** argv) {
             if (o.save_every > 0 && it % o.save_every == 0 && it < o.iterations) {
                 char tag[32];
                 snprintf(tag, sizeof(tag), "_it%03d", it);
-                check(prc_em_estimate_host(h, out.data()));
-                save_image(with_suffix(o.output, tag), out);
+                writer.finish();  // the previous checkpoint is on disk; its buffer is free
+                writer.image.resize(n);
+                check(prc_em_estimate_host(h, writer.image.data()));
+                writer.start(with_suffix(o.output, tag));
             }
         }
+        writer.finish();
         check(prc_em_estimate_host(h, out.data()));
     }
     const double t_iter = now_s() - t;

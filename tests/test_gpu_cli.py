@@ -85,3 +85,16 @@ def test_checkpoint_and_reprojection_names_in_dotted_directory(workdir, fixture7
     final = np.fromfile(dotted / "output", np.float32).reshape(shape)
     reproj = np.fromfile(dotted / "output_REPROJ", np.float32)
     assert abs(reproj.sum(dtype=np.float64) / final.sum(dtype=np.float64) - 1) < 3e-6
+
+
+def test_checkpoint_write_failure_stops_the_run(workdir):
+    """--save-every writes checkpoints from a helper thread while the GPU iterates; a failed
+    checkpoint write still ends the run with the reference's message and no final output."""
+    missing = workdir / "no_such_dir" / "output"
+    cmd = [str(CLI_PATH), "68Ga", "16", "14", "12", "1.1", "1.6", "2.3", "--input", str(workdir / "x.raw"),
+           "--density", str(workdir / "density.raw"), "--output", str(missing), "--rays", "32",
+           "--iterations", "3", "--save-every", "1"]
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=120)
+    assert r.returncode != 0
+    assert r.stderr.count("Cannot write") == 1 and "output_it001" in r.stderr
+    assert not missing.exists()
