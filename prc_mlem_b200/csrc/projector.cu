@@ -203,6 +203,14 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity
     return false;
 }
 
+// An 8-byte vector of the bf16 field, read once per projection: loaded without allocating in
+// L1, which keeps L1 for the volume being gathered.
+__device__ __forceinline__ uint2 ld_stream(const uint2* q) {
+    uint2 x;
+    asm("ld.global.nc.L1::no_allocate.v2.u32 {%0, %1}, [%2];" : "=r"(x.x), "=r"(x.y) : "l"(q));
+    return x;
+}
+
 __device__ __forceinline__ int near_offset(const ProjParams& p, int q) {
     const int dx = q % kNearSide - kNearR, dy = q / kNearSide % kNearSide - kNearR,
               dz = q / (kNearSide * kNearSide) - kNearR;
@@ -339,7 +347,7 @@ __device__ __forceinline__ void project_group(const ProjParams& p, const OpArgs&
             }
         }
     } else {
-        // Stored field, streamed by TMA.  Lane 0 keeps kStages bulk copies of kChunk bytes in
+        // Stored field.  fp32: streamed by TMA -- lane 0 keeps kStages bulk copies of kChunk bytes in
         // flight into this warp's shared-memory ring (cp.async.bulk, completion counted by an
         // mbarrier), so the weights arrive as contiguous DRAM bursts without holding
         // registers.  A chunk is consumed in batches of kBatch packs: the packs' template
@@ -359,73 +367,52 @@ __device__ __forceinline__ void project_group(const ProjParams& p, const OpArgs&
         const StreamLayout& lay = kGatherT ? p.tgt : p.src;
         const FarField& fld = kGatherT ? a.farT : a.far;
         const int* tmpl = kGatherT ? p.tmpl_neg : p.tmpl;
-        unsigned char* ring = dyn_smem + (size_t)warp * kStages * kChunk;
         const long long e0 = lay.group_base[group], e1 = lay.group_base[group + 1];
-        const char* src_bytes = (kBase == kFieldF32 ? reinterpret_cast<const char*>(fld.f32)
-                                                    : reinterpret_cast<const char*>(fld.b16)) + e0 * kElem;
         const int* desc = lay.desc + e0 / (kPack * kLanes);
-        const long long total = (e1 - e0) * kElem;
         const int n_packs = (int)((e1 - e0) / (kPack * kLanes));
-        const int n_chunks = (n_packs + kPacksPerChunk - 1) / kPacksPerChunk;
         // Gathered voxel: source + offset (adjoint) or target - offset (forward).  A 32-bit index
         // (one wide multiply-add per address); the sum wraps only on padding steps (w = 0),
         // whose loads are predicated off, since voxel indices stay below INT_MAX.
         auto gather_index = [&](int o) { return (int)((unsigned)s + (unsigned)o); };
-        auto issue = [&](int c) {  // lane 0 only
-            const int stage = c % kStages;
-            const unsigned bytes = (unsigned)min((long long)kChunk, total - (long long)c * kChunk);
-            mbar_expect_tx(&bars[stage], bytes);
-            bulk_copy_g2s(ring + stage * kChunk, src_bytes + (long long)c * kChunk, bytes, &bars[stage]);
-        };
-        if (lane == 0) {
-            for (int k = 0; k < kStages; ++k) mbar_init(&bars[k], 1);
-            fence_mbarrier_init();
-            for (int c = 0; c < n_chunks && c < kStages; ++c) issue(c);
-        }
-        __syncwarp();
-        static_assert(kPacksPerChunk % kBatch == 0, "batches stay inside a chunk");
-        auto desc_at = [&](int P) { return P < n_packs ? __ldg(desc + P) : 0; };
-        int4 tn[kBatch];
-        int dq[kBatch];
+        if constexpr (kBase == kFieldBF16) {
+            // bf16 form: each lane loads its own 8-byte vectors straight from HBM (a warp's loads
+            // of one pack coalesce into 256 contiguous bytes) one batch ahead of their use.  This
+            // form is bound by L1 wavefronts, not bytes, and skipping the shared-memory ring
+            // (its copies in and its reads out) measured 5 % faster than the TMA stream.
+            const uint2* vec = reinterpret_cast<const uint2*>(fld.b16) + e0 / kPack + lane;
+            auto load_vec = [&](int P) {
+                uint2 x = make_uint2(0u, 0u);
+                if (P < n_packs) x = ld_stream(vec + (size_t)P * kLanes);
+                return x;
+            };
+            auto desc_at = [&](int P) { return P < n_packs ? __ldg(desc + P) : 0; };
+            int4 tn[kBatch];
+            uint2 wn[kBatch];
+            int dq[kBatch];
 #pragma unroll
-        for (int k = 0; k < kBatch; ++k) tn[k] = __ldg(reinterpret_cast<const int4*>(tmpl + desc_at(k)));
+            for (int k = 0; k < kBatch; ++k) wn[k] = load_vec(k);
 #pragma unroll
-        for (int k = 0; k < kBatch; ++k) dq[k] = desc_at(kBatch + k);
-        bool ok = true;
-        for (int c = 0; c < n_chunks; ++c) {
-            const int packs = min(kPacksPerChunk, n_packs - c * kPacksPerChunk);
-            const int stage = c % kStages;
-            if (!mbar_wait_bounded(&bars[stage], (c / kStages) & 1)) {
-                ok = false;
-                break;
-            }
-            const unsigned char* chunk = ring + stage * kChunk;
-            for (int b = 0; b < packs; b += kBatch) {
-                const int P0 = c * kPacksPerChunk + b;
+            for (int k = 0; k < kBatch; ++k) tn[k] = __ldg(reinterpret_cast<const int4*>(tmpl + desc_at(k)));
+#pragma unroll
+            for (int k = 0; k < kBatch; ++k) dq[k] = desc_at(kBatch + k);
+            for (int P0 = 0; P0 < n_packs; P0 += kBatch) {
                 int o[kBatch * kPack];
                 float w[kBatch * kPack];
                 int4 tc[kBatch];
+                uint2 wc[kBatch];
 #pragma unroll
-                for (int k = 0; k < kBatch; ++k) tc[k] = tn[k];
+                for (int k = 0; k < kBatch; ++k) tc[k] = tn[k], wc[k] = wn[k];
 #pragma unroll
                 for (int k = 0; k < kBatch; ++k) tn[k] = __ldg(reinterpret_cast<const int4*>(tmpl + dq[k]));
+#pragma unroll
+                for (int k = 0; k < kBatch; ++k) wn[k] = load_vec(P0 + kBatch + k);
 #pragma unroll
                 for (int k = 0; k < kBatch; ++k) dq[k] = desc_at(P0 + 2 * kBatch + k);
 #pragma unroll
                 for (int k = 0; k < kBatch; ++k) {
-                    const bool here = b + k < packs;
-                    const int4 t = tc[k];
-                    o[k * kPack] = t.x, o[k * kPack + 1] = t.y, o[k * kPack + 2] = t.z, o[k * kPack + 3] = t.w;
-                    if constexpr (kBase == kFieldF32) {
-                        const float4 x = here ? reinterpret_cast<const float4*>(chunk + (b + k) * kPackBytes)[lane]
-                                              : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-                        w[k * kPack] = x.x, w[k * kPack + 1] = x.y, w[k * kPack + 2] = x.z, w[k * kPack + 3] = x.w;
-                    } else {
-                        const uint2 x = here ? reinterpret_cast<const uint2*>(chunk + (b + k) * kPackBytes)[lane]
-                                             : make_uint2(0u, 0u);
-                        w[k * kPack] = __uint_as_float(x.x << 16), w[k * kPack + 1] = __uint_as_float(x.x & 0xffff0000u);
-                        w[k * kPack + 2] = __uint_as_float(x.y << 16), w[k * kPack + 3] = __uint_as_float(x.y & 0xffff0000u);
-                    }
+                    o[k * kPack] = tc[k].x, o[k * kPack + 1] = tc[k].y, o[k * kPack + 2] = tc[k].z, o[k * kPack + 3] = tc[k].w;
+                    w[k * kPack] = __uint_as_float(wc[k].x << 16), w[k * kPack + 1] = __uint_as_float(wc[k].x & 0xffff0000u);
+                    w[k * kPack + 2] = __uint_as_float(wc[k].y << 16), w[k * kPack + 3] = __uint_as_float(wc[k].y & 0xffff0000u);
                 }
                 if constexpr (OP == Op::Adjoint || kGatherT) {
                     float v[kBatch * kPack];
@@ -439,23 +426,98 @@ __device__ __forceinline__ void project_group(const ProjParams& p, const OpArgs&
                         if (live && w[u] > 0.0f) deposit(s + o[u], w[u]);
                 }
             }
-            __syncwarp();
-            if (lane == 0 && c + kStages < n_chunks) {
-                fence_proxy_async();  // this stage's reads precede the copy that overwrites it
-                issue(c + kStages);
-            }
-        }
-        if (!ok) {
-            // A copy did not complete in time: report it, and give the copies still in flight
-            // a bounded chance to land before this warp's shared memory is released.
+        } else {
+            unsigned char* ring = dyn_smem + (size_t)warp * kStages * kChunk;
+            const char* src_bytes = (kBase == kFieldF32 ? reinterpret_cast<const char*>(fld.f32)
+                                                        : reinterpret_cast<const char*>(fld.b16)) + e0 * kElem;
+            const long long total = (e1 - e0) * kElem;
+            const int n_chunks = (n_packs + kPacksPerChunk - 1) / kPacksPerChunk;
+            auto issue = [&](int c) {  // lane 0 only
+                const int stage = c % kStages;
+                const unsigned bytes = (unsigned)min((long long)kChunk, total - (long long)c * kChunk);
+                mbar_expect_tx(&bars[stage], bytes);
+                bulk_copy_g2s(ring + stage * kChunk, src_bytes + (long long)c * kChunk, bytes, &bars[stage]);
+            };
             if (lane == 0) {
-                atomicOr(a.error, 1u);
-                for (int k = 0; k < kStages; ++k) {
-                    mbar_wait_bounded(&bars[k], 0);
-                    mbar_wait_bounded(&bars[k], 1);
+                for (int k = 0; k < kStages; ++k) mbar_init(&bars[k], 1);
+                fence_mbarrier_init();
+                for (int c = 0; c < n_chunks && c < kStages; ++c) issue(c);
+            }
+            __syncwarp();
+            static_assert(kPacksPerChunk % kBatch == 0, "batches stay inside a chunk");
+            auto desc_at = [&](int P) { return P < n_packs ? __ldg(desc + P) : 0; };
+            int4 tn[kBatch];
+            int dq[kBatch];
+    #pragma unroll
+            for (int k = 0; k < kBatch; ++k) tn[k] = __ldg(reinterpret_cast<const int4*>(tmpl + desc_at(k)));
+    #pragma unroll
+            for (int k = 0; k < kBatch; ++k) dq[k] = desc_at(kBatch + k);
+            bool ok = true;
+            for (int c = 0; c < n_chunks; ++c) {
+                const int packs = min(kPacksPerChunk, n_packs - c * kPacksPerChunk);
+                const int stage = c % kStages;
+                if (!mbar_wait_bounded(&bars[stage], (c / kStages) & 1)) {
+                    ok = false;
+                    break;
+                }
+                const unsigned char* chunk = ring + stage * kChunk;
+                for (int b = 0; b < packs; b += kBatch) {
+                    const int P0 = c * kPacksPerChunk + b;
+                    int o[kBatch * kPack];
+                    float w[kBatch * kPack];
+                    int4 tc[kBatch];
+    #pragma unroll
+                    for (int k = 0; k < kBatch; ++k) tc[k] = tn[k];
+    #pragma unroll
+                    for (int k = 0; k < kBatch; ++k) tn[k] = __ldg(reinterpret_cast<const int4*>(tmpl + dq[k]));
+    #pragma unroll
+                    for (int k = 0; k < kBatch; ++k) dq[k] = desc_at(P0 + 2 * kBatch + k);
+    #pragma unroll
+                    for (int k = 0; k < kBatch; ++k) {
+                        const bool here = b + k < packs;
+                        const int4 t = tc[k];
+                        o[k * kPack] = t.x, o[k * kPack + 1] = t.y, o[k * kPack + 2] = t.z, o[k * kPack + 3] = t.w;
+                        if constexpr (kBase == kFieldF32) {
+                            const float4 x = here ? reinterpret_cast<const float4*>(chunk + (b + k) * kPackBytes)[lane]
+                                                  : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                            w[k * kPack] = x.x, w[k * kPack + 1] = x.y, w[k * kPack + 2] = x.z, w[k * kPack + 3] = x.w;
+                        } else {
+                            const uint2 x = here ? reinterpret_cast<const uint2*>(chunk + (b + k) * kPackBytes)[lane]
+                                                 : make_uint2(0u, 0u);
+                            w[k * kPack] = __uint_as_float(x.x << 16), w[k * kPack + 1] = __uint_as_float(x.x & 0xffff0000u);
+                            w[k * kPack + 2] = __uint_as_float(x.y << 16), w[k * kPack + 3] = __uint_as_float(x.y & 0xffff0000u);
+                        }
+                    }
+                    if constexpr (OP == Op::Adjoint || kGatherT) {
+                        float v[kBatch * kPack];
+    #pragma unroll
+                        for (int u = 0; u < kBatch * kPack; ++u) v[u] = w[u] > 0.0f ? __ldg(a.in + gather_index(o[u])) : 0.0f;
+    #pragma unroll
+                        for (int u = 0; u < kBatch * kPack; ++u) acc = fmaf(w[u], v[u], acc);
+                    } else {
+    #pragma unroll
+                        for (int u = 0; u < kBatch * kPack; ++u)
+                            if (live && w[u] > 0.0f) deposit(s + o[u], w[u]);
+                    }
+                }
+                __syncwarp();
+                if (lane == 0 && c + kStages < n_chunks) {
+                    fence_proxy_async();  // this stage's reads precede the copy that overwrites it
+                    issue(c + kStages);
                 }
             }
-            __syncwarp();
+            if (!ok) {
+                // A copy did not complete in time: report it, and give the copies still in flight
+                // a bounded chance to land before this warp's shared memory is released.
+                if (lane == 0) {
+                    atomicOr(a.error, 1u);
+                    for (int k = 0; k < kStages; ++k) {
+                        mbar_wait_bounded(&bars[k], 0);
+                        mbar_wait_bounded(&bars[k], 1);
+                    }
+                }
+                __syncwarp();
+            }
         }
     }
 
@@ -767,7 +829,10 @@ cudaError_t launch(const ProjParams& p, const OpArgs& a, cudaStream_t s) {
     const int blocks = (groups + kWarps - 1) / kWarps;
     if (blocks == 0) return cudaSuccess;
     size_t smem = 0;
-    if (FAR_MODE != kMarch) smem = kFieldSmemBytes;  // the ring; the near block is in the field
+    // The ring (the near block is in the field).  The bf16 form reads HBM directly yet keeps the
+    // allocation: launched without it (and so with the largest L1 carveout) it measured 1.7-2x
+    // slower on the 128x128x159 torso.
+    if (FAR_MODE != kMarch) smem = kFieldSmemBytes;
     else if (NEAR_MODE == kTraceNear && OP != Op::Layout) smem = kNearSmemBytes;
     auto kernel = project_kernel<OP, EXACT, NEAR_MODE, FAR_MODE>;
     if (smem > 48 * 1024) {
