@@ -287,7 +287,10 @@ class Projector:
 
     def correct(self, d_g, d_out, iterations: int, beta: float = 0.2, gamma: float = 20.0,
                 accelerate: bool = True, stream=None) -> None:
-        """MAP-EM correction of d_g into d_out (prc.cu:659-711), fully on device."""
+        """MAP-EM correction of d_g into d_out (prc.cu:659-711), fully on device.
+
+        Enqueued on ``stream`` (default: the engine's own stream) and asynchronous to the host
+        and to torch's current stream: call ``synchronize()`` before reading d_out elsewhere."""
         _check(lib().prc_em_run(self._h, _ptr(d_g), _ptr(d_out), iterations, beta, gamma, int(accelerate), stream))
 
     def synchronize(self) -> None:
