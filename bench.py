@@ -59,8 +59,9 @@ def parse():
                     help="only run this many forward+adjoint pairs of the headline form (profiling)")
     ap.add_argument("--form", choices=("fp32", "bf16", "traced"), default="fp32",
                     help="projector form of the headline number (default: plain fp32 stored field)")
-    ap.add_argument("--workload", choices=("torso", "batch"), default="torso",
-                    help="batch: 32 dynamic-PET frames of mixed grids and isotopes, 10 iterations each")
+    ap.add_argument("--workload", choices=("torso", "batch", "surrogate"), default="torso",
+                    help="batch: 32 dynamic-PET frames of mixed grids and isotopes, 10 iterations each; "
+                         "surrogate: the learned surrogate's evaluation on the small phantom at 128x128x159")
     ap.add_argument("--frames", type=int, default=32)
     ap.add_argument("--surrogate", action="store_true", help="batch: learned surrogate where it applies")
     return ap.parse_args()
@@ -662,12 +663,86 @@ def run_batch(args):
     batch.close()
 
 
+def run_surrogate_eval(args):
+    """The learned surrogate's evaluation: the small phantom's geometry on the 128x128x159 grid,
+    data = the plain projector's blur of its activity, Poisson-sampled at 5e7 counts, 6-iteration
+    MAP-EM for each isotope the network was trained on.  Per form: EM iters/s, NRMSE of the
+    corrected image against the plain fp32 field (full volume) and against the FP64 oracle (a
+    central 64x48x32 crop), and the share of sources the tracer's judge sent back to exact
+    weights.  The crop comparison runs every form on the cropped volume and data, as the oracle
+    does, so both see the same problem."""
+    import torch
+    import prc_mlem_b200 as pm
+    from prc_mlem_b200 import phantoms, surrogate as sg
+    from oracle import oracle
+    world, rank, _ = dist_env()
+    if rank != 0:
+        return
+    torch.cuda.set_device(0)
+    rho, truth, spacing = phantoms.scaled_small_phantom(seed=1, shape=tuple(args.grid))
+    nz, ny, nx = rho.shape
+    sl = (slice(nz // 2 - 16, nz // 2 + 16), slice(ny // 2 - 24, ny // 2 + 24), slice(nx // 2 - 32, nx // 2 + 32))
+    net = sg.load_trained()
+    results = {}
+    for iso in sg.ISOTOPES:
+        forms = [("fp32_field", dict(cache=pm.PRC_CACHE_FULL)),
+                 ("bf16_field", dict(cache=pm.PRC_CACHE_FULL, precision=pm.PRC_PRECISION_BF16)),
+                 ("traced", dict(cache=pm.PRC_CACHE_NEAR)),
+                 ("radial_traced_bf16", dict(precision=pm.PRC_PRECISION_BF16, surrogate="traced"))]
+        if net is not None:
+            forms += [("learned_bf16", dict(precision=pm.PRC_PRECISION_BF16, surrogate=net,
+                                            target_scale=sg.TARGET_SCALE)),
+                      ("learned_judged_bf16", dict(precision=pm.PRC_PRECISION_BF16, surrogate=net,
+                                                   target_scale=sg.TARGET_SCALE, fallback_nrmse=0.3))]
+        out, plain = {}, None
+        g = None
+        for name, kw in forms:
+            Q = pm.Projector(iso, rho, spacing, rays=RAYS, support_rho=SUPPORT_RHO, **kw)
+            if g is None:  # the data: the plain projector's blur of the activity, Poisson-sampled
+                g = phantoms.poisson_counts(Q.forward_host(truth), COUNTS, seed=5)
+                d_g = torch.from_numpy(g).cuda()
+                d_out = torch.empty_like(d_g)
+            s = torch.cuda.ExternalStream(Q.stream)
+            Q.correct(d_g, d_out, args.iterations, BETA, GAMMA, True)
+            Q.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(s)
+            for _ in range(3):
+                Q.correct(d_g, d_out, args.iterations, BETA, GAMMA, True)
+            e1.record(s)
+            e1.synchronize()
+            img = d_out.cpu().numpy()
+            if plain is None:
+                plain = img
+            out[name] = {"iters_per_s": round(3 * args.iterations / (e0.elapsed_time(e1) / 1e3), 2),
+                         "nrmse_vs_fp32_field": nrmse(img, plain)}
+            if "surrogate" in kw:
+                out[name]["exact_fallback_share"] = round(Q.fallbacks / Q.n_active, 4)
+            Q.close()
+            with pm.Projector(iso, np.ascontiguousarray(rho[sl]), spacing, rays=RAYS, support_rho=SUPPORT_RHO,
+                              **kw) as C:
+                out[name]["crop_image"] = C.correct_host(np.ascontiguousarray(g[sl]), args.iterations, BETA, GAMMA,
+                                                         True)
+        O = oracle.Problem(iso, np.ascontiguousarray(rho[sl]), spacing, rays=RAYS, support_rho=SUPPORT_RHO,
+                           precision=64, threads=os.cpu_count() or 1)
+        ref = O.correct(np.ascontiguousarray(g[sl]), args.iterations, BETA, GAMMA, True)
+        for name in out:
+            out[name]["nrmse_vs_fp64_crop"] = nrmse(out[name].pop("crop_image"), ref)
+        results[iso] = out
+    print(json.dumps({"workload": f"surrogate evaluation: small phantom geometry on {nx}x{ny}x{nz} at "
+                                  f"{spacing[0]}x{spacing[1]}x{spacing[2]} mm, {args.iterations} MAP-EM iterations, "
+                                  f"beta {BETA}, gamma {GAMMA:g}, Poisson {COUNTS:g} counts",
+                      "network": "trained" if net is not None else "absent", "isotopes": results}))
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
     elif args.workload == "batch":
         run_batch(args)
+    elif args.workload == "surrogate":
+        run_surrogate_eval(args)
     else:
         run_ours(args)
 

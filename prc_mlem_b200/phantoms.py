@@ -6,6 +6,7 @@ measured and tested on:
 
 * :func:`solver_fixture`  -- the 16x14x12 anisotropic seed-72 fixture of the reference tests;
 * :func:`small_phantom`   -- 32x32x24 at 2 mm, water cylinder, lung, bone (18F workload);
+* :func:`scaled_small_phantom` -- the same geometry on another grid (surrogate evaluation);
 * :func:`torso_phantom`   -- 128x128x159 clinical torso (68Ga workload);
 * :func:`poisson_counts`  -- scales a blurred image to a total count and Poisson-samples it.
 
@@ -69,6 +70,35 @@ def small_phantom(seed: int = 1):
         zc, yc, xc = inside[rng.integers(len(inside))] + rng.uniform(-0.5, 0.5, 3)
         truth[_ellipsoid(shape, (xc, yc, zc), (r, r, r)) & body] += rng.uniform(2, 10)
     return rho.astype(np.float32), truth.astype(np.float32), (2.0, 2.0, 2.0)
+
+
+def scaled_small_phantom(seed: int = 1, shape=(159, 128, 128), spacing=(0.776, 0.776, 0.795)):
+    """(rho, truth, spacing): the small phantom's geometry stretched onto another grid.
+
+    Every position and radius of :func:`small_phantom` (given in voxels of its 32x32x24 grid) is
+    scaled by the grid ratio per axis (lesion radii by the mean ratio), with the same seeded
+    draws, so shape (24, 32, 32) with 2 mm voxels reproduces :func:`small_phantom` exactly.  At
+    128x128x159 it is the learned surrogate's evaluation phantom: one water cylinder, one lung
+    ellipsoid and one bone sphere, simpler than the torso.
+    """
+    nz, ny, nx = shape
+    sx, sy, sz = nx / 32.0, ny / 32.0, nz / 24.0
+    sr = (sx + sy + sz) / 3.0
+    z, y, x = np.indices(shape, dtype=np.float64)
+    cx, cy = (nx - 1) / 2, (ny - 1) / 2
+    body = ((x - cx) / (13 * sx)) ** 2 + ((y - cy) / (10 * sy)) ** 2 <= 1.0
+    rho = np.full(shape, AIR)
+    rho[body] = WATER
+    rho[_ellipsoid(shape, (10 * sx, 16 * sy, 12 * sz), (5 * sx, 6 * sy, 8 * sz)) & body] = 0.30
+    rho[_ellipsoid(shape, (22 * sx, 16 * sy, 12 * sz), (3 * sx, 3 * sy, 3 * sz)) & body] = 1.85
+    rng = np.random.default_rng(seed)
+    truth = body.astype(np.float64)
+    inside = np.argwhere(body)
+    for _ in range(6):
+        r = rng.uniform(2, 4) * sr
+        zc, yc, xc = inside[rng.integers(len(inside))] + rng.uniform(-0.5, 0.5, 3)
+        truth[_ellipsoid(shape, (xc, yc, zc), (r, r, r)) & body] += rng.uniform(2, 10)
+    return rho.astype(np.float32), truth.astype(np.float32), tuple(spacing)
 
 
 def torso_phantom(seed: int = 2, shape=(159, 128, 128)):
