@@ -50,7 +50,7 @@ struct ProjParams {
     const int* tmpl_neg;             // the same offsets negated (target-major gathers: source = t - o)
     int tmpl_len;                    // steps per row: covers every step a ray takes in the image
     int n_rows;                      // n_rays + 1
-    StreamLayout src;                // source-major field: group = 32 consecutive sources
+    StreamLayout src;                // source-major field: group = 32 consecutive sources (8x2x2 tiles)
     StreamLayout tgt;                // target-major field: group = 32 consecutive targets
     const int* vox2src;              // voxel -> source index, -1 off the support
 };

@@ -8,15 +8,15 @@
 //   adjoint:  (A^T y)_s = sum_t w_st * y_t / W_s     (gather)
 //
 // B200 mapping (the reference gives one warp to one source and strides its lanes over rays):
-// here a warp owns 32 consecutive tissue voxels (lanes) and all lanes trace the SAME ray k at
+// here a warp owns 32 consecutive sources (lanes) and all lanes trace the SAME ray k at
 // the same time.  Because ray k starts at the same sub-voxel offset with the same direction
 // in every source voxel and the grid is uniform, the face-crossing sequence (which axis, and
 // the path length dt of each segment) is identical in every lane: it is warp-uniform control
 // flow, computed once per ray with prc.cu's own float arithmetic, so the weights are the
 // reference's bit for bit.  Only the density along the path differs per lane, which decides
-// where each lane stops.  The 32 lanes are x-neighbours in one image row, so every density
-// read, gather and scatter of a step touches 32 consecutive voxels: coalesced 128-byte lines
-// from L2, where the 10 MB volumes stay resident.  The near block is either traced into a
+// where each lane stops.  Sources are ordered in 8x2x2 voxel tiles, so the 32 lanes are close
+// neighbours: every density read, gather and scatter of a step touches four 32-byte row
+// segments, from L1 / L2, where the 10 MB volumes stay resident.  The near block is either traced into a
 // per-warp shared-memory tile laid out [offset][lane] (conflict-free, no atomics: each lane
 // owns its column) or read from the group-interleaved cache.
 #include "engine.h"
