@@ -39,6 +39,8 @@ struct ProjParams {
     const int* active;       // linear voxel index of each source, increasing
     const RayStep* far;      // n_rays records
     const RayStep* near;     // kNearRays records
+    const short* near_order; // the near rays grouped by direction octant (increasing index in each)
+    const int* near_start;   // [9]: first entry of octant o in near_order (o = x+ | y+ << 1 | z+ << 2)
     const float* table;      // kRangeBins + 1 survival samples, or nullptr for analytic
     float table_scale;       // bins per mm
     int n_branch;            // analytic model (used when table == nullptr)
@@ -98,6 +100,10 @@ struct OpArgs {
     // Surrogate fields: groups whose flag is 1 keep exact traced weights (the Norm pass fills
     // only those), the others hold radial coefficients (surrogate_fill fills only those).
     const unsigned char* fallback_groups = nullptr;
+    // Norm: fp32 accumulator of the traced near block, [group][125 offsets][32 lanes].  When set,
+    // the near rays are traced one direction octant at a time into a 27-offset shared-memory tile
+    // (3.4 KB per warp instead of 16 KB, so four times the warps fit on an SM).
+    float* near_acc = nullptr;
 };
 
 // ---- radial surrogate support -----------------------------------------------------------------
@@ -194,6 +200,8 @@ cudaError_t forward_prep(const ProjParams& p, const float* W, const float* f, fl
 
 // projector.cu
 cudaError_t setup_rays(const Grid& g, int n_rays, RayStep* d_far, RayStep* d_near, cudaStream_t s);
+// Groups the near rays by direction octant (order[kNearRays], start[9]); after setup_rays.
+cudaError_t order_near_rays(const RayStep* d_near, short* d_order, int* d_start, cudaStream_t s);
 // trace_near: retrace the near block (no cache).  Forward / Adjoint / Count read the stored far
 // field when a.far is on, and march the far rays otherwise.
 cudaError_t project(Op op, const ProjParams& p, const OpArgs& a, bool trace_near, cudaStream_t s);

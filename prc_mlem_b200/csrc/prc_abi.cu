@@ -54,6 +54,8 @@ struct prc_handle {
     float* table = nullptr;
     RayStep* far = nullptr;
     RayStep* near_rays = nullptr;
+    short* near_order = nullptr;
+    int* near_start = nullptr;
     NearCache cache;
     FarField far_field;
     int* tmpl = nullptr;
@@ -172,6 +174,25 @@ void prc_destroy(prc_handle* h) {
 // The target-major copy of the stored field: per target group and template row, the longest
 // step any contributing source reaches, prefix sums, then a copy of every weight.  Optional:
 // without it (not enough memory) the forward projection scatters with atomics instead.
+// The normalisation pass, with its near blocks traced octant by octant into a temporary fp32
+// accumulator when one can be had (smaller shared-memory tiles, more warps per SM); otherwise
+// into the full per-warp tile.
+static int run_norm(prc_handle* h, OpArgs a) {
+    float* acc = nullptr;
+    if (cudaMalloc(&acc, (size_t)h->n_groups * kNear * kLanes * sizeof(float)) != cudaSuccess) {
+        cudaGetLastError();
+        acc = nullptr;
+    }
+    a.near_acc = acc;
+    const cudaError_t e = project(Op::Norm, h->params, a, true, h->stream);
+    if (acc) {
+        cudaStreamSynchronize(h->stream);
+        cudaFree(acc);
+    }
+    PRC_CUDA(e);
+    return PRC_OK;
+}
+
 static int build_target_major(prc_handle* h, const std::vector<int>& active, size_t elem) {
     ProjParams& p = h->params;
     const size_t rows = (size_t)h->n_groups * p.n_rows;
@@ -369,7 +390,7 @@ static int build_surrogate_field(prc_handle* h, prc_net* net, float target_scale
     p.src.desc = h->desc;
     OpArgs a = h->op_args();
     a.fallback_groups = d_group_fb;
-    PRC_CUDA(project(Op::Norm, p, a, true, h->stream));  // exact weights of the fallback groups
+    if (const int rc = run_norm(h, a); rc != PRC_OK) return rc;  // exact weights of the fallback groups
     PRC_CUDA(surrogate_fill(p, a, tab, coef, h->support, h->stream));
     PRC_CUDA(cudaStreamSynchronize(h->stream));
     h->far_entries = run;
@@ -422,6 +443,8 @@ static int create_impl(prc_handle* h, const float* density_host, prc_net* net, b
     PRC_CUDA(h->alloc(&h->W, h->n_active));
     PRC_CUDA(h->alloc(&h->far, h->opts.rays));
     PRC_CUDA(h->alloc(&h->near_rays, kNearRays));
+    PRC_CUDA(h->alloc(&h->near_order, kNearRays));
+    PRC_CUDA(h->alloc(&h->near_start, 9));
     PRC_CUDA(h->alloc(&h->counter, 1));
     PRC_CUDA(h->alloc(&h->error, 1));
     PRC_CUDA(cudaMemcpyAsync(h->rho, rho.data(), h->n * sizeof(float), cudaMemcpyHostToDevice, h->stream));
@@ -439,6 +462,8 @@ static int create_impl(prc_handle* h, const float* density_host, prc_net* net, b
     p.active = h->active;
     p.far = h->far;
     p.near = h->near_rays;
+    p.near_order = h->near_order;
+    p.near_start = h->near_start;
     p.n_branch = h->model.n;
     for (int b = 0; b < 3; ++b) p.br[b] = h->model.br[b];
     if (!h->opts.exact_range) {  // prc.cu:625-633
@@ -450,6 +475,7 @@ static int create_impl(prc_handle* h, const float* density_host, prc_net* net, b
         p.table_scale = h->model.table_scale();
     }
     PRC_CUDA(setup_rays(g, h->opts.rays, h->far, h->near_rays, h->stream));
+    PRC_CUDA(order_near_rays(h->near_rays, h->near_order, h->near_start, h->stream));
 
     const bool bf16 = h->opts.precision == PRC_PRECISION_BF16;
     const size_t elem = bf16 ? 2 : 4;
@@ -530,8 +556,7 @@ static int create_impl(prc_handle* h, const float* density_host, prc_net* net, b
             else cudaGetLastError();  // optional: fall back to retracing
         }
     }
-    OpArgs a = h->op_args();
-    PRC_CUDA(project(Op::Norm, p, a, true, h->stream));
+    if (const int rc = run_norm(h, h->op_args()); rc != PRC_OK) return rc;
     if (h->cache_mode == PRC_CACHE_SOURCE_MAJOR && h->opts.cache == PRC_CACHE_FULL) {
         const int rc = build_target_major(h, active, elem);
         if (rc != PRC_OK) return rc;

@@ -228,6 +228,47 @@ __device__ __forceinline__ void store_weight(const FarField& f, long long e, flo
     else f.b16[e] = __float2bfloat16_rn(w);
 }
 
+// Near block of one lane, traced one direction octant at a time.  A near ray whose direction
+// has signs (sx, sy, sz) only visits block offsets (sx a, sy b, sz c) with a, b, c in {0, 1, 2}
+// before it leaves the block, so the rays of one octant deposit into 27 offsets: a 27 x 32
+// shared-memory tile per warp, added to this lane's column of the fp32 accumulator acc
+// ([125 offsets] with stride 32) after each octant.  Rays keep increasing index within an octant.
+template <bool EXACT>
+__device__ __forceinline__ void trace_near_octants(const ProjParams& p, bool live, int s, int vx, int vy, int vz,
+                                                   int warp, int lane, unsigned char* dyn_smem, float* acc) {
+    float* tile = reinterpret_cast<float*>(dyn_smem) + warp * (27 * kLanes);
+    for (int q = 0; q < kNear; ++q) acc[q * kLanes] = 0.0f;
+    for (int o = 0; o < 8; ++o) {
+        const int sx = (o & 1) ? 1 : -1, sy = (o & 2) ? 1 : -1, sz = (o & 4) ? 1 : -1;
+        for (int j = 0; j < 27; ++j) tile[j * kLanes + lane] = 0.0f;
+        const int r0 = __ldg(p.near_start + o), r1 = __ldg(p.near_start + o + 1);
+        for (int i = r0; i < r1; ++i) {
+            const RayStep R = p.near[__ldg(p.near_order + i)];
+            march<true, EXACT>(p, R, live, s, vx, vy, vz, [&](int, float w, int q, int) {
+                const int a = abs(q % kNearSide - kNearR), b = abs(q / kNearSide % kNearSide - kNearR),
+                          c = abs(q / (kNearSide * kNearSide) - kNearR);
+                tile[((c * 3 + b) * 3 + a) * kLanes + lane] += w;
+            });
+        }
+        for (int j = 0; j < 27; ++j) {
+            const int dx = sx * (j % 3), dy = sy * (j / 3 % 3), dz = sz * (j / 9);
+            acc[(((dz + kNearR) * kNearSide + dy + kNearR) * kNearSide + dx + kNearR) * kLanes] += tile[j * kLanes + lane];
+        }
+    }
+}
+
+// Stable grouping of the near rays by direction octant (one thread; 2048 rays, setup only).
+__global__ void order_near_kernel(const RayStep* near, short* order, int* start) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    int count[8] = {};
+    for (int r = 0; r < kNearRays; ++r) ++count[(near[r].di > 0) | (near[r].dj > 0) << 1 | (near[r].dk > 0) << 2];
+    int pos[8];
+    start[0] = 0;
+    for (int o = 0; o < 8; ++o) start[o + 1] = start[o] + count[o], pos[o] = start[o];
+    for (int r = 0; r < kNearRays; ++r)
+        order[pos[(near[r].di > 0) | (near[r].dj > 0) << 1 | (near[r].dk > 0) << 2]++] = (short)r;
+}
+
 // One warp per group of 32 consecutive sources.  NEAR_MODE says where the 5x5x5 weights come
 // from when the far rays are marched; FAR_MODE selects marching or the stored field (which
 // then also holds the near block).  Norm always marches and writes W, and the near cache or
@@ -283,13 +324,21 @@ __device__ __forceinline__ void project_group(const ProjParams& p, const OpArgs&
         if constexpr (OP != Op::Layout) {
             float* sum = reinterpret_cast<float*>(dyn_smem) + warp * (kNear * kLanes);
             if constexpr (NEAR_MODE == kTraceNear) {
-                for (int q = 0; q < kNear; ++q) sum[q * kLanes + lane] = 0.0f;
-                for (int r = 0; r < kNearRays; ++r) {
-                    const RayStep R = p.near[r];
-                    march<true, EXACT>(p, R, live, s, vx, vy, vz,
-                                       [&](int, float w, int q, int) { sum[q * kLanes + lane] += w; });
+                if (OP == Op::Norm && a.near_acc) {
+                    trace_near_octants<EXACT>(p, live, s, vx, vy, vz, warp, lane, dyn_smem,
+                                              a.near_acc + (size_t)group * kNear * kLanes + lane);
+                } else {
+                    for (int q = 0; q < kNear; ++q) sum[q * kLanes + lane] = 0.0f;
+                    for (int r = 0; r < kNearRays; ++r) {
+                        const RayStep R = p.near[r];
+                        march<true, EXACT>(p, R, live, s, vx, vy, vz,
+                                           [&](int, float w, int q, int) { sum[q * kLanes + lane] += w; });
+                    }
                 }
             }
+            // traced near weights of this lane: the shared-memory tile or the octant accumulator
+            const bool octants = NEAR_MODE == kTraceNear && OP == Op::Norm && a.near_acc;
+            const float* near_sum = octants ? a.near_acc + (size_t)group * kNear * kLanes + lane : sum + lane;
             const size_t cache_base = (size_t)group * kNear * kLanes + lane;
             const float near_scale = (float)p.n_rays / kNearRays;
             for (int q = 0; q < kNear; ++q) {
@@ -299,7 +348,7 @@ __device__ __forceinline__ void project_group(const ProjParams& p, const OpArgs&
                 if constexpr (NEAR_MODE == kTraceNear) {
                     const bool in = (unsigned)(vx + dx) < (unsigned)nx && (unsigned)(vy + dy) < (unsigned)ny &&
                                     (unsigned)(vz + dz) < (unsigned)p.g.nz;
-                    w = in ? sum[q * kLanes + lane] * near_scale : 0.0f;
+                    w = in ? near_sum[q * kLanes] * near_scale : 0.0f;
                     if constexpr (OP == Op::Norm) {
                         if (near_round) w = __bfloat162float(__float2bfloat16_rn(w));
                         if (valid && a.near.b16) a.near.b16[cache_base + (size_t)q * kLanes] = __float2bfloat16_rn(w);
@@ -833,7 +882,8 @@ cudaError_t launch(const ProjParams& p, const OpArgs& a, cudaStream_t s) {
     // allocation: launched without it (and so with the largest L1 carveout) it measured 1.7-2x
     // slower on the 128x128x159 torso.
     if (FAR_MODE != kMarch) smem = kFieldSmemBytes;
-    else if (NEAR_MODE == kTraceNear && OP != Op::Layout) smem = kNearSmemBytes;
+    else if (NEAR_MODE == kTraceNear && OP != Op::Layout)
+        smem = OP == Op::Norm && a.near_acc ? size_t(kWarps) * 27 * kLanes * sizeof(float) : kNearSmemBytes;
     auto kernel = project_kernel<OP, EXACT, NEAR_MODE, FAR_MODE>;
     if (smem > 48 * 1024) {
         const cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -866,6 +916,11 @@ cudaError_t launch_op(const ProjParams& p, const OpArgs& a, bool trace_near, cud
 }
 
 }  // namespace
+
+cudaError_t order_near_rays(const RayStep* d_near, short* d_order, int* d_start, cudaStream_t s) {
+    order_near_kernel<<<1, 32, 0, s>>>(d_near, d_order, d_start);
+    return cudaGetLastError();
+}
 
 cudaError_t setup_rays(const Grid& g, int n_rays, RayStep* d_far, RayStep* d_near, cudaStream_t s) {
     const int n = n_rays > kNearRays ? n_rays : kNearRays;
