@@ -177,18 +177,24 @@ void prc_destroy(prc_handle* h) {
 // The normalisation pass, with its near blocks traced octant by octant into a temporary fp32
 // accumulator when one can be had (smaller shared-memory tiles, more warps per SM); otherwise
 // into the full per-warp tile.
-static int run_norm(prc_handle* h, OpArgs a) {
+static float* near_accumulator(prc_handle* h) {
     float* acc = nullptr;
     if (cudaMalloc(&acc, (size_t)h->n_groups * kNear * kLanes * sizeof(float)) != cudaSuccess) {
         cudaGetLastError();
-        acc = nullptr;
+        return nullptr;
     }
-    a.near_acc = acc;
+    return acc;
+}
+static void release_accumulator(prc_handle* h, float* acc) {
+    if (!acc) return;
+    cudaStreamSynchronize(h->stream);
+    cudaFree(acc);
+}
+
+static int run_norm(prc_handle* h, OpArgs a) {
+    a.near_acc = near_accumulator(h);
     const cudaError_t e = project(Op::Norm, h->params, a, true, h->stream);
-    if (acc) {
-        cudaStreamSynchronize(h->stream);
-        cudaFree(acc);
-    }
+    release_accumulator(h, a.near_acc);
     PRC_CUDA(e);
     return PRC_OK;
 }
@@ -391,7 +397,13 @@ static int build_surrogate_field(prc_handle* h, prc_net* net, float target_scale
     OpArgs a = h->op_args();
     a.fallback_groups = d_group_fb;
     if (const int rc = run_norm(h, a); rc != PRC_OK) return rc;  // exact weights of the fallback groups
-    PRC_CUDA(surrogate_fill(p, a, tab, coef, h->support, h->stream));
+    {
+        OpArgs fa = a;
+        fa.near_acc = near_accumulator(h);  // the surrogate groups' near blocks, octant by octant
+        const cudaError_t e = surrogate_fill(p, fa, tab, coef, h->support, h->stream);
+        release_accumulator(h, fa.near_acc);
+        PRC_CUDA(e);
+    }
     PRC_CUDA(cudaStreamSynchronize(h->stream));
     h->far_entries = run;
     h->cache_mode = PRC_CACHE_SOURCE_MAJOR;

@@ -810,18 +810,26 @@ __global__ void __launch_bounds__(kBlock) surrogate_fill_kernel(const ProjParams
     const FarField& f = a.far;
     const long long gbase = p.src.group_base[group];
     float acc = 0.0f;
-    float* sum = reinterpret_cast<float*>(dyn_smem) + warp * (kNear * kLanes);
-    for (int q = 0; q < kNear; ++q) sum[q * kLanes + lane] = 0.0f;
-    for (int r = 0; r < kNearRays; ++r)
-        march<true, EXACT>(p, p.near[r], valid, s, vx, vy, vz,
-                           [&](int, float w, int q, int) { sum[q * kLanes + lane] += w; });
+    const float* near_sum;
+    if (a.near_acc) {
+        float* acc_col = a.near_acc + (size_t)group * kNear * kLanes + lane;
+        trace_near_octants<EXACT>(p, valid, s, vx, vy, vz, warp, lane, dyn_smem, acc_col);
+        near_sum = acc_col;
+    } else {
+        float* sum = reinterpret_cast<float*>(dyn_smem) + warp * (kNear * kLanes);
+        for (int q = 0; q < kNear; ++q) sum[q * kLanes + lane] = 0.0f;
+        for (int r = 0; r < kNearRays; ++r)
+            march<true, EXACT>(p, p.near[r], valid, s, vx, vy, vz,
+                               [&](int, float w, int q, int) { sum[q * kLanes + lane] += w; });
+        near_sum = sum + lane;
+    }
     const float near_scale = (float)p.n_rays / kNearRays;
     for (int q = 0; q < kNear; ++q) {
         const int dx = q % kNearSide - kNearR, dy = q / kNearSide % kNearSide - kNearR,
                   dz = q / (kNearSide * kNearSide) - kNearR;
         const bool in = (unsigned)(vx + dx) < (unsigned)nx && (unsigned)(vy + dy) < (unsigned)ny &&
                         (unsigned)(vz + dz) < (unsigned)nz;
-        float w = in ? sum[q * kLanes + lane] * near_scale : 0.0f;
+        float w = in ? near_sum[q * kLanes] * near_scale : 0.0f;
         if (FAR_MODE == kFieldBF16) w = __bfloat162float(__float2bfloat16_rn(w));
         acc += w;
         if (valid) store_weight<FAR_MODE>(f, pack_slot(gbase, q, lane), w);
@@ -1037,10 +1045,11 @@ cudaError_t surrogate_fill(const ProjParams& p, const OpArgs& a, const RadialTab
     const int groups = (p.n_active + kLanes - 1) / kLanes;
     if (groups == 0) return cudaSuccess;
     const int blocks = (groups + kWarps - 1) / kWarps;
+    const size_t smem = a.near_acc ? size_t(kWarps) * 27 * kLanes * sizeof(float) : kNearSmemBytes;
     auto launch_fill = [&](auto kernel) {
-        cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kNearSmemBytes);
+        cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
-        kernel<<<blocks, kBlock, kNearSmemBytes, s>>>(p, a, t, coef, support);
+        kernel<<<blocks, kBlock, smem, s>>>(p, a, t, coef, support);
         return cudaGetLastError();
     };
     if (a.far.f32) return p.table ? launch_fill(surrogate_fill_kernel<false, kFieldF32>) : launch_fill(surrogate_fill_kernel<true, kFieldF32>);
