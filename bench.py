@@ -202,7 +202,7 @@ def run_ours(args):
     d_blur = torch.empty_like(d_truth)
     P.forward(d_truth, d_blur)
     P.synchronize()
-    g_host = phantoms.poisson_counts(d_blur.cpu().numpy(), COUNTS, seed=100 + rank)
+    g_host = phantoms.poisson_counts_device(d_blur, COUNTS, seed=100 + rank).cpu().numpy()  # on the GPU
     d_g = torch.from_numpy(g_host).cuda()
     d_out = torch.empty_like(d_g)
     flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device="cuda")
@@ -621,8 +621,9 @@ def run_batch(args):
         d_t = torch.from_numpy(truth).cuda()
         d_b = torch.empty_like(d_t)
         batch.forward(i, d_t, d_b)
-        gs.append(torch.from_numpy(phantoms.poisson_counts(d_b.cpu().numpy(), counts, seed=200 + i)).cuda())
+        gs.append(phantoms.poisson_counts_device(d_b, counts, seed=200 + i))
         outs.append(torch.empty_like(d_t))
+    torch.cuda.synchronize()  # the counts are drawn on torch's stream, the batch runs on its own
     stream = torch.cuda.ExternalStream(batch.stream)
     for _ in range(args.warmup):
         batch.correct(gs, outs, 10, BETA, GAMMA, True)
@@ -699,7 +700,8 @@ def run_surrogate_eval(args):
         for name, kw in forms:
             Q = pm.Projector(iso, rho, spacing, rays=RAYS, support_rho=SUPPORT_RHO, **kw)
             if g is None:  # the data: the plain projector's blur of the activity, Poisson-sampled
-                g = phantoms.poisson_counts(Q.forward_host(truth), COUNTS, seed=5)
+                g = phantoms.poisson_counts_device(torch.from_numpy(Q.forward_host(truth)).cuda(), COUNTS,
+                                                   seed=5).cpu().numpy()
                 d_g = torch.from_numpy(g).cuda()
                 d_out = torch.empty_like(d_g)
             s = torch.cuda.ExternalStream(Q.stream)

@@ -107,6 +107,7 @@ _SIGNATURES = {
     "prc_eval_sums": (ctypes.c_int, [_P, _P, _P, _P]),
     "prc_eval_sums_f64": (ctypes.c_int, [_P, _P, _P, _P]),
     "prc_eval_destroy": (None, [_P]),
+    "prc_poisson": (ctypes.c_int, [_P, ctypes.c_int64, ctypes.c_double, ctypes.c_uint64, _P, _P]),
     "prc_timing": (ctypes.c_int, [_P, ctypes.c_int]),
     "prc_timing_read": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int64),
                                        ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int64)]),

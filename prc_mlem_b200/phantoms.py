@@ -8,7 +8,8 @@ measured and tested on:
 * :func:`small_phantom`   -- 32x32x24 at 2 mm, water cylinder, lung, bone (18F workload);
 * :func:`scaled_small_phantom` -- the same geometry on another grid (surrogate evaluation);
 * :func:`torso_phantom`   -- 128x128x159 clinical torso (68Ga workload);
-* :func:`poisson_counts`  -- scales a blurred image to a total count and Poisson-samples it.
+* :func:`poisson_counts`  -- scales a blurred image to a total count and Poisson-samples it;
+* :func:`poisson_counts_device` -- the same on the GPU (``prc_poisson``).
 
 Blurring needs the projector, so callers do it (``Projector.forward_host``).
 """
@@ -147,6 +148,28 @@ def torso_phantom(seed: int = 2, shape=(159, 128, 128)):
         lesion = _ellipsoid(shape, (xc, yc, zc), (r, r, r)) & body
         truth[lesion] = contrast
     return rho.astype(np.float32), truth.astype(np.float32), (0.776, 0.776, 0.795)
+
+
+def poisson_counts_device(d_blurred, total_counts: float, seed: int = 0):
+    """Device form of :func:`poisson_counts`: a float32 CUDA tensor of counts drawn on the GPU
+    (``prc_poisson``: Philox4x32-10 keyed by ``seed``, inversion below a mean of 10, PTRS above)
+    after scaling ``d_blurred`` (a float32 CUDA tensor, negative values count as 0) to
+    ``total_counts``.  Counts differ from the host form's (another random stream) but follow
+    the same distribution.  The sampling is enqueued on torch's current stream."""
+    import ctypes
+    import torch
+    from . import PrcError, lib
+    d = d_blurred.contiguous()
+    if d.dtype != torch.float32 or not d.is_cuda:
+        raise ValueError("expected a float32 CUDA tensor")
+    total = float(torch.clamp(d, min=0).double().sum().item())
+    out = torch.empty_like(d)
+    scale = total_counts / total if total > 0 else 0.0
+    rc = lib().prc_poisson(d.data_ptr(), d.numel(), scale, int(seed), out.data_ptr(),
+                           torch.cuda.current_stream(d.device).cuda_stream)
+    if rc != 0:
+        raise PrcError(rc, lib().prc_last_error().decode())
+    return out
 
 
 def poisson_counts(blurred: np.ndarray, total_counts: float, seed: int = 0) -> np.ndarray:
