@@ -8,6 +8,7 @@
 #include "umma.cuh"
 
 #include <string>
+#include <type_traits>
 #include <vector>
 
 namespace {
@@ -93,6 +94,16 @@ struct ConvFwd {
         decode3(k / cin, 3, kz, ky, kx);
         return x[((((size_t)b * S + oz + kz) * S + oy + ky) * S + ox + kx) * cin + k % cin];
     }
+    // 8 channels of one tap are contiguous when cin is a multiple of 8 (the 32-channel layers)
+    __device__ bool vec_a() const { return cin % 8 == 0; }
+    __device__ uint4 a8(int m, int k) const {
+        const int So = S - 2, n3 = So * So * So, b = m / n3;
+        int oz, oy, ox, kz, ky, kx;
+        decode3(m % n3, So, oz, oy, ox);
+        decode3(k / cin, 3, kz, ky, kx);
+        return *reinterpret_cast<const uint4*>(x + ((((size_t)b * S + oz + kz) * S + oy + ky) * S + ox + kx) * cin +
+                                               k % cin);
+    }
     __device__ bf16 b(int n, int k) const { return w[(size_t)n * 27 * cin + k]; }
     __device__ void store(int m, int n, float v) const {
         out[(size_t)m * kC + n] = __float2bfloat16_rn(fmaxf(v + bias[n], 0.0f));
@@ -116,7 +127,18 @@ struct ConvDx {
         if (oz < 0 || oy < 0 || ox < 0 || oz >= So || oy >= So || ox >= So) return __float2bfloat16(0.0f);
         return dz[((((size_t)b * So + oz) * So + oy) * So + ox) * kC + k % kC];
     }
+    __device__ bool vec_a() const { return true; }
+    __device__ uint4 a8(int m, int k) const {
+        const int So = S - 2, n3 = S * S * S, b = m / n3;
+        int iz, iy, ix, kz, ky, kx;
+        decode3(m % n3, S, iz, iy, ix);
+        decode3(k / kC, 3, kz, ky, kx);
+        const int oz = iz - kz, oy = iy - ky, ox = ix - kx;
+        if (oz < 0 || oy < 0 || ox < 0 || oz >= So || oy >= So || ox >= So) return make_uint4(0u, 0u, 0u, 0u);
+        return *reinterpret_cast<const uint4*>(dz + ((((size_t)b * So + oz) * So + oy) * So + ox) * kC + k % kC);
+    }
     __device__ bf16 b(int n, int k) const { return w[((size_t)(k % kC) * 27 + k / kC) * kC + n]; }
+    static constexpr bool kRowsA = false, kRowsB = true;
     __device__ void store(int m, int n, float v) const {
         const size_t i = (size_t)m * kC + n;
         dz_prev[i] = __float2bfloat16_rn(__bfloat162float(x[i]) > 0.0f ? v : 0.0f);
@@ -147,6 +169,8 @@ struct HeadFwd {
     const float* bh;
     float* y;
     __device__ bf16 a(int m, int k) const { return a4[(size_t)m * kC + k]; }
+    __device__ bool vec_a() const { return true; }
+    __device__ uint4 a8(int m, int k) const { return *reinterpret_cast<const uint4*>(a4 + (size_t)m * kC + k); }
     __device__ bf16 b(int n, int k) const { return wh[(size_t)n * kC + k]; }
     __device__ void store(int m, int n, float v) const { y[(size_t)m * kOut + n] = v + bh[n]; }
 };
@@ -157,11 +181,12 @@ struct HeadDx {
     const bf16* a4;
     bf16* dz4;
     __device__ bf16 a(int m, int k) const { return dy[(size_t)m * kOut + k]; }
+    __device__ bool vec_a() const { return true; }
+    __device__ uint4 a8(int m, int k) const { return *reinterpret_cast<const uint4*>(dy + (size_t)m * kOut + k); }
     __device__ bf16 b(int n, int k) const { return wh[(size_t)k * kC + n]; }
-    __device__ void store(int m, int n, float v) const {
-        const size_t i = (size_t)m * kC + n;
-        dz4[i] = __float2bfloat16_rn(__bfloat162float(a4[i]) > 0.0f ? v : 0.0f);
-    }
+    static constexpr bool kRowsA = false, kRowsB = true;
+    // run split over K (SplitK); relu_grad_epilogue_kernel then writes
+    // dz4 = bf16(a4 > 0 ? sum : 0)
 };
 
 struct HeadDw {
@@ -173,6 +198,61 @@ struct HeadDw {
     __device__ void store(int m, int n, float v) const { atomicAdd(gwh + (size_t)m * kC + n, v); }
 };
 
+// Problems whose A operand has 16-byte rows in memory offer a8(m, k) (8 values at once) and
+// vec_a() (whether this instance may use it).
+template <class P, class = void>
+struct HasVecA : std::false_type {};
+template <class P>
+struct HasVecA<P, decltype((void)&P::a8)> : std::true_type {};
+// kRowsA / kRowsB (default false): the operand is contiguous along M / N, so its element loader
+// walks rows fastest.
+template <class P, class = void>
+struct RowsA : std::false_type {};
+template <class P>
+struct RowsA<P, std::enable_if_t<P::kRowsA>> : std::true_type {};
+template <class P, class = void>
+struct RowsB : std::false_type {};
+template <class P>
+struct RowsB<P, std::enable_if_t<P::kRowsB>> : std::true_type {};
+
+// (Measured: walking rows fastest helps the weight operand of the data gradients, whose rows are
+// contiguous channels, but slows the weight-gradient GEMMs down, whose operands are read from
+// several positions per row anyway; those keep the K-fastest order.)
+static_assert(!RowsA<ConvDx>::value && RowsB<ConvDx>::value && RowsB<HeadDx>::value && !RowsA<ConvDw>::value &&
+                  !RowsB<ConvDw>::value && !RowsA<ConvFwd>::value && !RowsB<ConvFwd>::value,
+              "loader order per operand");
+static_assert(HasVecA<ConvFwd>::value && HasVecA<ConvDx>::value && HasVecA<HeadFwd>::value && HasVecA<HeadDx>::value &&
+                  !HasVecA<ConvDw>::value && !HasVecA<HeadDw>::value,
+              "channels-last problems offer 16-byte A rows");
+
+// Few output rows (the 3^3 -> 1 convolution and the head's data gradient have one row per
+// sample) leave most SMs idle, so those GEMMs also split K: every slice adds into an fp32
+// buffer and a second pass applies the epilogue.  Same operands as the wrapped problem.
+template <class P>
+struct SplitK {
+    P p;
+    float* acc;  // [M][kC]
+    __device__ bf16 a(int m, int k) const { return p.a(m, k); }
+    __device__ bool vec_a() const { return p.vec_a(); }
+    __device__ uint4 a8(int m, int k) const { return p.a8(m, k); }
+    __device__ bf16 b(int n, int k) const { return p.b(n, k); }
+    __device__ void store(int m, int n, float v) const { atomicAdd(acc + (size_t)m * kC + n, v); }
+    static constexpr bool kRowsA = RowsA<P>::value, kRowsB = RowsB<P>::value;
+};
+
+static_assert(HasVecA<SplitK<ConvFwd>>::value && HasVecA<SplitK<HeadDx>>::value, "the split keeps the vector loader");
+
+// out = bf16(relu(acc + bias))
+__global__ void conv_epilogue_kernel(const float* acc, const float* bias, bf16* out, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        out[i] = __float2bfloat16_rn(fmaxf(acc[i] + bias[i % kC], 0.0f));
+}
+// dz = bf16(a > 0 ? acc : 0)
+__global__ void relu_grad_epilogue_kernel(const float* acc, const bf16* a, bf16* dz, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        dz[i] = __float2bfloat16_rn(__bfloat162float(a[i]) > 0.0f ? acc[i] : 0.0f);
+}
+
 template <int BN, class P>
 __global__ void __launch_bounds__(prc::umma::kThreads) problem_kernel(P prob, int M, int N, int K, int k_split,
                                                                       unsigned int* error) {
@@ -180,10 +260,20 @@ __global__ void __launch_bounds__(prc::umma::kThreads) problem_kernel(P prob, in
     __shared__ uint64_t bar;
     __shared__ uint32_t tmem_slot;
     const int k_lo = blockIdx.z * k_split;
-    const bool ok = prc::umma::gemm_tile<BN>(
-        M, N, K, blockIdx.x * prc::umma::kM, blockIdx.y * BN, k_lo, k_lo + k_split,
-        [&](int m, int k) { return prob.a(m, k); }, [&](int n, int k) { return prob.b(n, k); },
-        [&](int m, int n, float v) { prob.store(m, n, v); }, smem, &bar, &tmem_slot);
+    bool ok;
+    if constexpr (HasVecA<P>::value) {
+        ok = prc::umma::gemm_tile<BN, RowsA<P>::value, RowsB<P>::value>(
+            M, N, K, blockIdx.x * prc::umma::kM, blockIdx.y * BN, k_lo, k_lo + k_split,
+            [&](int m, int k) { return prob.a(m, k); }, prob.vec_a(), [&](int m, int k) { return prob.a8(m, k); },
+            [&](int n, int k) { return prob.b(n, k); }, [&](int m, int n, float v) { prob.store(m, n, v); }, smem, &bar,
+            &tmem_slot);
+    } else {
+        ok = prc::umma::gemm_tile<BN, RowsA<P>::value, RowsB<P>::value>(
+            M, N, K, blockIdx.x * prc::umma::kM, blockIdx.y * BN, k_lo, k_lo + k_split,
+            [&](int m, int k) { return prob.a(m, k); }, false, prc::umma::NoVecA{},
+            [&](int n, int k) { return prob.b(n, k); }, [&](int m, int n, float v) { prob.store(m, n, v); }, smem,
+            &bar, &tmem_slot);
+    }
     if (!ok && threadIdx.x == 0) atomicOr(error, 1u);
 }
 
@@ -275,6 +365,7 @@ struct prc_net {
     bf16* dy = nullptr;
     double* sse = nullptr;
     unsigned int* error = nullptr;
+    float* split_acc = nullptr;  // [max_batch][kC] fp32 partial sums of the split-K GEMMs
     int step = 0;
     std::vector<void*> allocs;
     cudaStream_t stream = nullptr;
@@ -340,6 +431,7 @@ int prc_nn_create(int max_batch, prc_net** out) {
     if (e == cudaSuccess) e = net_alloc(n, &n->y, B * kOut);
     if (e == cudaSuccess) e = net_alloc(n, &n->dy, B * kOut);
     if (e == cudaSuccess) e = net_alloc(n, &n->sse, 1);
+    if (e == cudaSuccess) e = net_alloc(n, &n->split_acc, B * kC);
     if (e == cudaSuccess) e = net_alloc(n, &n->error, 1);
     if (e != cudaSuccess) return fail_cleanup(nn_fail(e, "prc_nn_create"));
     *out = n;
@@ -403,7 +495,15 @@ int prc_nn_forward(prc_net* n, const void* d_x0, int batch, float* d_y, void* st
     for (int l = 0; l < 4; ++l) {
         const int S = kSide[l], So = S - 2, cin = l == 0 ? kIn : kC;
         ConvFwd p{n->act[l], n->wb[l], n->b[l], n->act[l + 1], S, cin};
-        NN_CUDA((run_problem<32>(p, batch * So * So * So, kC, 27 * cin, 1, n->error, s)), "prc_nn_forward");
+        const int rows = batch * So * So * So;
+        if (So == 1) {  // one row per sample: split K, then bias + ReLU
+            NN_CUDA(cudaMemsetAsync(n->split_acc, 0, (size_t)rows * kC * sizeof(float), s), "prc_nn_forward");
+            NN_CUDA((run_problem<32>(SplitK<ConvFwd>{p, n->split_acc}, rows, kC, 27 * cin, 14, n->error, s)),
+                    "prc_nn_forward");
+            conv_epilogue_kernel<<<64, 256, 0, s>>>(n->split_acc, n->b[l], n->act[l + 1], (size_t)rows * kC);
+        } else {
+            NN_CUDA((run_problem<32>(p, rows, kC, 27 * cin, 1, n->error, s)), "prc_nn_forward");
+        }
     }
     HeadFwd h{n->act[4], n->wb[4], n->b[4], d_y ? d_y : n->y};
     NN_CUDA((run_problem<256>(h, batch, kOut, kC, 1, n->error, s)), "prc_nn_forward");
@@ -426,7 +526,9 @@ int prc_nn_backward(prc_net* n, const float* d_target, int batch, float lr, doub
     NN_CUDA((run_problem<32>(hw, kOut, kC, batch, 8, n->error, s)), "prc_nn_backward");
     colsum_kernel<<<kOut, 256, 0, s>>>(n->dy, batch, kOut, n->gb[4]);
     HeadDx hx{n->dy, n->wb[4], n->act[4], n->dz[4]};
-    NN_CUDA((run_problem<32>(hx, batch, kC, kOut, 1, n->error, s)), "prc_nn_backward");
+    NN_CUDA(cudaMemsetAsync(n->split_acc, 0, (size_t)batch * kC * sizeof(float), s), "prc_nn_backward");
+    NN_CUDA((run_problem<32>(SplitK<HeadDx>{hx, n->split_acc}, batch, kC, kOut, 32, n->error, s)), "prc_nn_backward");
+    relu_grad_epilogue_kernel<<<64, 256, 0, s>>>(n->split_acc, n->act[4], n->dz[4], (size_t)batch * kC);
     // convolutions, last to first
     for (int l = 3; l >= 0; --l) {
         const int S = kSide[l], So = S - 2, cin = l == 0 ? kIn : kC;

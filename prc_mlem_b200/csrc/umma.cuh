@@ -69,13 +69,24 @@ __device__ __forceinline__ int tile_offset(int R, int row, int k) {
     return (((k >> 3) * (R >> 3) + (row >> 3)) * 8 + (row & 7)) * 16 + (k & 7) * 2;
 }
 
+// No vector loader for the A operand (the element loader fills the tile).
+struct NoVecA {
+    __device__ uint4 operator()(int, int) const { return make_uint4(0u, 0u, 0u, 0u); }
+};
+
 // C tile (128 x BN) at (m0, n0), summed over k in [k_lo, k_hi) (a split-K slice when the
 // caller splits; K bounds the problem).  LoadA(m, k) and LoadB(n, k) return the operand values
 // (bf16) for m < M, n < N, k < K; Store(m, n, v) receives the result for m < M, n < N.
+// With vec_a, LoadA8(m, k) returns the 8 A values k .. k + 7 (k a multiple of 8) as one 16-byte
+// vector -- exactly one row of a core matrix -- and the A tile is filled with 16-byte copies;
+// K and the slice bounds must then be multiples of 8.
 // Returns false (and stores nothing) if an MMA completion wait timed out.
-template <int BN, class LoadA, class LoadB, class Store>
-__device__ bool gemm_tile(int M, int N, int K, int m0, int n0, int k_lo, int k_hi, LoadA&& load_a, LoadB&& load_b,
-                          Store&& store, unsigned char* smem, uint64_t* bar, uint32_t* tmem_slot) {
+// ROWS_A / ROWS_B: the element loader walks rows fastest (consecutive threads read consecutive
+// m or n at one k), for operands stored contiguously along M or N rather than along K.
+template <int BN, bool ROWS_A = false, bool ROWS_B = false, class LoadA, class LoadA8, class LoadB, class Store>
+__device__ bool gemm_tile(int M, int N, int K, int m0, int n0, int k_lo, int k_hi, LoadA&& load_a, bool vec_a,
+                          LoadA8&& load_a8, LoadB&& load_b, Store&& store, unsigned char* smem, uint64_t* bar,
+                          uint32_t* tmem_slot) {
     static_assert(BN >= 32 && BN <= 256 && (BN & (BN - 1)) == 0, "BN: power of two in [32, 256]");
     __nv_bfloat16* sa = reinterpret_cast<__nv_bfloat16*>(smem);
     __nv_bfloat16* sb = reinterpret_cast<__nv_bfloat16*>(smem + kM * kKT * 2);
@@ -97,13 +108,22 @@ __device__ bool gemm_tile(int M, int N, int K, int m0, int n0, int k_lo, int k_h
     const int k_tiles = k_hi > k_lo ? (k_hi - k_lo + kKT - 1) / kKT : 0;
     for (int kt = 0; kt < k_tiles && ok; ++kt) {
         const int k0 = k_lo + kt * kKT;
-        for (int i = tid; i < kM * kKT; i += kThreads) {
-            const int r = i / kKT, k = i % kKT;
-            const __nv_bfloat16 v = (m0 + r < M && k0 + k < k_hi) ? load_a(m0 + r, k0 + k) : __float2bfloat16(0.0f);
-            *reinterpret_cast<__nv_bfloat16*>(reinterpret_cast<unsigned char*>(sa) + tile_offset(kM, r, k)) = v;
+        if (vec_a) {
+            // rows fastest: consecutive threads store consecutive 16-byte rows of a core matrix
+            for (int i = tid; i < kM * (kKT / 8); i += kThreads) {
+                const int r = i % kM, c = i / kM, k = k0 + c * 8;
+                const uint4 v = (m0 + r < M && k < k_hi) ? load_a8(m0 + r, k) : make_uint4(0u, 0u, 0u, 0u);
+                *reinterpret_cast<uint4*>(reinterpret_cast<unsigned char*>(sa) + tile_offset(kM, r, c * 8)) = v;
+            }
+        } else {
+            for (int i = tid; i < kM * kKT; i += kThreads) {
+                const int r = ROWS_A ? i % kM : i / kKT, k = ROWS_A ? i / kM : i % kKT;
+                const __nv_bfloat16 v = (m0 + r < M && k0 + k < k_hi) ? load_a(m0 + r, k0 + k) : __float2bfloat16(0.0f);
+                *reinterpret_cast<__nv_bfloat16*>(reinterpret_cast<unsigned char*>(sa) + tile_offset(kM, r, k)) = v;
+            }
         }
         for (int i = tid; i < BN * kKT; i += kThreads) {
-            const int r = i / kKT, k = i % kKT;
+            const int r = ROWS_B ? i % BN : i / kKT, k = ROWS_B ? i / BN : i % kKT;
             const __nv_bfloat16 v = (n0 + r < N && k0 + k < k_hi) ? load_b(n0 + r, k0 + k) : __float2bfloat16(0.0f);
             *reinterpret_cast<__nv_bfloat16*>(reinterpret_cast<unsigned char*>(sb) + tile_offset(BN, r, k)) = v;
         }
@@ -157,6 +177,14 @@ __device__ bool gemm_tile(int M, int N, int K, int m0, int n0, int k_lo, int k_h
     if (warp == 0)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BN) : "memory");
     return ok;
+}
+
+// The element-loader form.
+template <int BN, class LoadA, class LoadB, class Store>
+__device__ bool gemm_tile(int M, int N, int K, int m0, int n0, int k_lo, int k_hi, LoadA&& load_a, LoadB&& load_b,
+                          Store&& store, unsigned char* smem, uint64_t* bar, uint32_t* tmem_slot) {
+    return gemm_tile<BN, false, false>(M, N, K, m0, n0, k_lo, k_hi, load_a, false, NoVecA{}, load_b, store, smem, bar,
+                                       tmem_slot);
 }
 
 // Dynamic shared memory of a gemm_tile CTA.  Padded so that at most 512 / BN CTAs fit on an SM
