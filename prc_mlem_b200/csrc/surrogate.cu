@@ -663,6 +663,16 @@ struct ConvSame {
             return __float2bfloat16(0.0f);
         return x[(((size_t)zz * py + yy) * px + xx) * cin + k % cin];
     }
+    __device__ bool vec_a() const { return cin % 8 == 0; }
+    __device__ uint4 a8(int m, int k) const {
+        const int z = m / (py * px), y = (m / px) % py, x0 = m % px;
+        int kz, ky, kx;
+        decode3(k / cin, 3, kz, ky, kx);
+        const int zz = z + kz - 1, yy = y + ky - 1, xx = x0 + kx - 1;
+        if ((unsigned)zz >= (unsigned)pz || (unsigned)yy >= (unsigned)py || (unsigned)xx >= (unsigned)px)
+            return make_uint4(0u, 0u, 0u, 0u);
+        return *reinterpret_cast<const uint4*>(x + (((size_t)zz * py + yy) * px + xx) * cin + k % cin);
+    }
     __device__ bf16 b(int n, int k) const { return w[(size_t)n * 27 * cin + k]; }
     __device__ void store(int m, int n, float v) const {
         out[(size_t)m * kC + n] = __float2bfloat16_rn(fmaxf(v + bias[n], 0.0f));
@@ -682,6 +692,12 @@ struct HeadActive {
         const int s = active[m];
         const int x = s % nx + kHalo, y = (s / nx) % ny + kHalo, z = s / (nx * ny) + kHalo;
         return a4[(((size_t)z * py + y) * px + x) * kC + k];
+    }
+    __device__ bool vec_a() const { return true; }
+    __device__ uint4 a8(int m, int k) const {
+        const int s = active[m];
+        const int x = s % nx + kHalo, y = (s / nx) % ny + kHalo, z = s / (nx * ny) + kHalo;
+        return *reinterpret_cast<const uint4*>(a4 + (((size_t)z * py + y) * px + x) * kC + k);
     }
     __device__ bf16 b(int n, int k) const { return wh[(size_t)n * kC + k]; }
     __device__ void store(int m, int n, float v) const {
