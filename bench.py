@@ -141,6 +141,21 @@ def aggregate(total_ms: float, steps: int, iterations: int, world: int, device=N
     return total_ms, world * steps * iterations / (total_ms / 1e3)
 
 
+def algorithmic_bytes(n_vox: int, n_active: int, deposits: int, weight_bytes: int = 4) -> dict:
+    """Fixed byte accounting of the path (per projection and per MAP-EM iteration).
+
+    A projection moves 12 B per source (active index, W_s, f_s or out_s) and per deposit one
+    stored weight (4 B fp32, 2 B bf16) plus a 4 B target value.  An iteration adds the 74 B per
+    voxel of the elementwise chain (extrapolate 12, clear 4, ratio 13, RDP update 13, sum 4,
+    finish 16, two dots 12) to its two projections.  The compulsory figure is what an iteration
+    moves when every volume and per-source array is touched once and no deposit costs traffic.
+    """
+    projection = 12 * n_active + (weight_bytes + 4) * deposits
+    return {"projection": projection,
+            "iteration": 74 * n_vox + 2 * projection,
+            "compulsory": 74 * n_vox + 2 * 12 * n_active}
+
+
 def make_workload(grid):
     from prc_mlem_b200 import phantoms
     rho, truth, spacing = phantoms.torso_phantom(seed=2, shape=tuple(grid))
@@ -286,9 +301,18 @@ def run_ours(args):
                 ts.append(e0.elapsed_time(e1))
         launch_ms[name] = statistics.mean(ts)
     top = max(region_ms, key=region_ms.get)
-    alg_bytes = 12 * n_active + 8 * deposits  # 8 B per deposit (weight + target value), 12 B per source
+    nz, ny, nx = args.grid
+    n_vox = nx * ny * nz
+    acct = algorithmic_bytes(n_vox, n_active, deposits, weight_bytes=2 if args.form == "bf16" else 4)
+    alg_bytes = acct["projection"]
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / (region_ms[top] / 1e3) / 1e9
+    iter_s = total_ms / (args.steps * args.iterations) / 1e3
+    iteration = {"algorithmic_bytes": acct["iteration"],
+                 "achieved": round(acct["iteration"] / iter_s / 1e9, 1),
+                 "frac": round(acct["iteration"] / iter_s / 1e9 / peak, 4),
+                 "compulsory_bytes": acct["compulsory"],
+                 "compulsory_gbs": round(acct["compulsory"] / iter_s / 1e9, 1)}
     projection_share = (in_region["forward_ms"] + in_region["adjoint_ms"]) / sum(times)
     mode, far_entries, far_t_entries = P.cache_mode
     elem = 2 if args.form == "bf16" else 4
@@ -311,8 +335,6 @@ def run_ours(args):
         return
     cpu = None if args.no_cpu_baseline or not single else cpu_baseline(rho, spacing, g_host, sample_seconds=15.0)
     check = None if args.no_oracle_check or not single else oracle_check(rho, spacing, g_host, args)
-    nz, ny, nx = args.grid
-    n_vox = nx * ny * nz
     line = {
         "metric": METRIC,
         "value": round(value, 3),
@@ -350,7 +372,10 @@ def run_ours(args):
                      "launch_ms_alone": {k: round(v, 4) for k, v in launch_ms.items()},
                      "launches_timed": in_region["forward_launches"] + in_region["adjoint_launches"],
                      "projection_share_of_steps": round(projection_share, 4),
-                     "algorithmic_bytes": alg_bytes},
+                     "algorithmic_bytes": alg_bytes,
+                     # the whole MAP-EM iteration (both projections and the elementwise chain)
+                     # over the mean iteration time of the timed steps
+                     "iteration": iteration},
         # per step: 3 initialisation kernels, then per iteration extrapolate, forward (u = f / W
         # and the gather, or the scatter), ratio, adjoint, RDP update, finish
         "gpu_launches": args.steps * (3 + (7 if far_t_entries else 6) * args.iterations),

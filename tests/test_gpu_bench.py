@@ -34,6 +34,10 @@ def test_our_arm_line():
     assert r["bound"] == "hbm" and r["unit"] == "GB/s" and r["achieved"] > 0 and r["peak"] > 0
     assert abs(r["frac"] - r["achieved"] / r["peak"]) < 1e-3
     assert r["launches_timed"] == 2 * 3 * 6
+    it = r["iteration"]
+    assert it["algorithmic_bytes"] == 74 * 48 * 64 * 64 + 2 * r["algorithmic_bytes"]
+    assert 0 < it["compulsory_bytes"] < it["algorithmic_bytes"] and 0 < it["achieved"]
+    assert abs(it["frac"] - it["achieved"] / r["peak"]) < 1e-3
     c = d["cpu_baseline"]
     assert c["kind"] == "port" and c["cores"] >= 1 and c["value"] > 0 and c["sample"]
     assert d["gpu_launches"] > 0
