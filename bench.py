@@ -15,6 +15,8 @@ Arms:
              the host->device copy of the data and the device->host copy of the result inside.
   reference  the CPU restatement of the reference's algorithm (oracle/, rays re-marched every
              projection as prc.cu does), on all host cores, over a bounded sample of sources.
+Both arms' `cpu_baseline` also times the reference's own CPU computation, the FP64 water-kernel
+quadrature of its tests/reference.py (restated in oracle/kernel_oracle.py), single-threaded.
 
 Multi-GPU (torchrun): every rank corrects its own frame (replicas, no collective on the data
 path); value = iterations of all ranks / max-over-ranks time.
@@ -542,7 +544,25 @@ def cpu_baseline(rho, spacing, g, sample_seconds=15.0, seed=7):
     return {"value": round(1.0 / per_iter, 5), "unit": "EM iters/s", "cores": threads, "kind": "port",
             "sample": f"{len(sample)} of {n_active} sources ({100 * len(sample) / n_active:.2f}%): one forward "
                       f"and one adjoint projection ({dt:.1f} s), scaled to all sources, plus one full RDP "
-                      f"update ({t_update:.2f} s)"}
+                      f"update ({t_update:.2f} s)",
+            "reference_quadrature": reference_quadrature()}
+
+
+def reference_quadrature(repeats=3):
+    """The reference's own CPU computation (the FP64 homogeneous water-kernel quadrature of its
+    tests/reference.py, restated in oracle/kernel_oracle.py): the 68Ga kernel at 2 mm voxels,
+    half-width 6, 600 shells x 1000 directions, single-threaded NumPy; median of ``repeats``."""
+    sys.path.insert(0, str(ROOT))
+    from oracle import kernel_oracle
+    branches = kernel_oracle.table_branches(ISOTOPE)
+    times = []
+    for _ in range(repeats):
+        t0 = time.perf_counter()
+        k = kernel_oracle.water_kernel(branches, (2.0, 2.0, 2.0), 6)
+        times.append(time.perf_counter() - t0)
+    return {"seconds": round(statistics.median(times), 4), "cores": 1, "kind": "port",
+            "case": f"{ISOTOPE} water kernel, 2 mm voxels, half-width 6, 600 shells x 1000 directions "
+                    f"(mass inside the box {k.sum():.6f})"}
 
 
 def run_reference(args):

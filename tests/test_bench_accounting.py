@@ -37,3 +37,9 @@ def test_compulsory_figure_is_about_a_fifth_of_a_gigabyte():
 
 def test_empty_volume():
     assert bench.algorithmic_bytes(0, 0, 0) == {"projection": 0, "iteration": 0, "compulsory": 0}
+
+
+def test_reference_quadrature_leg_times_the_restated_cpu_path():
+    q = bench.reference_quadrature(repeats=1)
+    assert q["seconds"] > 0 and q["cores"] == 1 and q["kind"] == "port"
+    assert "68Ga" in q["case"] and "half-width 6" in q["case"]
