@@ -71,6 +71,16 @@ __device__ __forceinline__ void grid_reduce(double (&v)[NV], const Reduction& r,
 #define GRID_STRIDE(i, n) \
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < (n); i += (size_t)gridDim.x * blockDim.x)
 
+// The streaming passes move 16 bytes per access: element 4q + c of a volume is component c of
+// float4 q.  They take that path when every pointer they touch is 16-byte aligned (allocations
+// are; a caller's offset pointer may not be) and finish the last n % 4 elements one at a time.
+// Each element is computed by the same expression on both paths.
+#define TAIL_STRIDE(i, start, n)                                                                 \
+    for (size_t i = (start) + blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < (n);          \
+         i += (size_t)gridDim.x * blockDim.x)
+
+__device__ __forceinline__ bool aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
+
 // g = support ? max(g_in, 0) : 0 (prc.cu:604-612); f = g; support_sum, eps and the floor.
 __device__ __forceinline__ void begin_body(const float* __restrict__ g_in, const unsigned char* __restrict__ support,
                                            float* __restrict__ g, float* __restrict__ f, size_t n, int n_active,
@@ -116,17 +126,33 @@ __device__ __forceinline__ void init_scale_body(float* __restrict__ f, size_t n,
 __device__ __forceinline__ void extrapolate_body(const float* __restrict__ f, const float* __restrict__ prev,
                                                  float* __restrict__ y, size_t n, const EmScalars* sc) {
     const float lambda = sc->lambda;
-    GRID_STRIDE(i, n) {
-        const float fi = f[i];
-        y[i] = fmaxf(fi + lambda * (fi - prev[i]), 0.5f * fi);
+    auto predict = [lambda](float fi, float pi) { return fmaxf(fi + lambda * (fi - pi), 0.5f * fi); };
+    const size_t n4 = aligned16(f) && aligned16(prev) && aligned16(y) ? n / 4 : 0;
+    const float4* f4 = reinterpret_cast<const float4*>(f);
+    const float4* p4 = reinterpret_cast<const float4*>(prev);
+    float4* y4 = reinterpret_cast<float4*>(y);
+    GRID_STRIDE(q, n4) {
+        const float4 a = f4[q], b = p4[q];
+        y4[q] = make_float4(predict(a.x, b.x), predict(a.y, b.y), predict(a.z, b.z), predict(a.w, b.w));
     }
+    TAIL_STRIDE(i, 4 * n4, n) y[i] = predict(f[i], prev[i]);
 }
 
 // EM ratio g / max(A y, eps) on the support (prc.cu:270-274).
 __device__ __forceinline__ void ratio_body(const float* __restrict__ g, float* __restrict__ est,
                                            const unsigned char* __restrict__ support, size_t n, const EmScalars* sc) {
     const float eps = sc->eps;
-    GRID_STRIDE(i, n) est[i] = support[i] ? g[i] / fmaxf(est[i], eps) : 0.0f;
+    auto ratio = [eps](unsigned char s, float gi, float ei) { return s ? gi / fmaxf(ei, eps) : 0.0f; };
+    const size_t n4 = aligned16(g) && aligned16(est) && ((uintptr_t)support & 3u) == 0 ? n / 4 : 0;
+    const float4* g4 = reinterpret_cast<const float4*>(g);
+    const uchar4* s4 = reinterpret_cast<const uchar4*>(support);
+    float4* e4 = reinterpret_cast<float4*>(est);
+    GRID_STRIDE(q, n4) {
+        const uchar4 m = s4[q];
+        const float4 a = g4[q], e = e4[q];
+        e4[q] = make_float4(ratio(m.x, a.x, e.x), ratio(m.y, a.y, e.y), ratio(m.z, a.z, e.z), ratio(m.w, a.w, e.w));
+    }
+    TAIL_STRIDE(i, 4 * n4, n) est[i] = ratio(support[i], g[i], est[i]);
 }
 
 __device__ __forceinline__ bool in_grid(const Grid& g, int i, int j, int k) {
@@ -151,7 +177,17 @@ __device__ __forceinline__ void update_body(const float* __restrict__ f, const f
             if (beta == 0.0f) {
                 out = fmaxf(f_em, 0.0f);
             } else {
-                const int i = idx % g.nx, j = (idx / g.nx) % g.ny, k = idx / ((size_t)g.nx * g.ny);
+                int i, j, k;
+                if (n <= 0xffffffffull) {  // 32-bit division (the usual case)
+                    const unsigned u = (unsigned)idx, row = u / (unsigned)g.nx;
+                    i = (int)(u - row * (unsigned)g.nx);
+                    j = (int)(row % (unsigned)g.ny);
+                    k = (int)(row / (unsigned)g.ny);
+                } else {
+                    i = (int)(idx % g.nx);
+                    j = (int)((idx / g.nx) % g.ny);
+                    k = (int)(idx / ((size_t)g.nx * g.ny));
+                }
                 float grad = 0.0f, curv = 0.0f;
                 for (int dz = -1; dz <= 1; ++dz)
                     for (int dy = -1; dy <= 1; ++dy)
@@ -192,16 +228,37 @@ __device__ __forceinline__ void finish_body(float* __restrict__ next, float* __r
                                             Reduction r) {
     const float scale = use_scale ? sc->scale : 1.0f;
     double v[2] = {0.0, 0.0};
-    GRID_STRIDE(i, n) {
-        const float value = __fmul_rn(next[i], scale);
-        next[i] = value;
+    // one element: rescale, step h = next - y into residual, and the two products
+    auto step = [&](float& nx, float& res, float hp_f) {
+        nx = __fmul_rn(nx, scale);
         if (RESIDUAL) {
-            const float h = value - residual[i];
-            residual[i] = h;
-            const double hp = h_prev[i];
-            v[0] += (double)h * hp;
+            res = nx - res;
+            const double hp = hp_f;
+            v[0] += (double)res * hp;
             v[1] += hp * hp;
         }
+    };
+    const size_t n4 = aligned16(next) && (!RESIDUAL || (aligned16(residual) && aligned16(h_prev))) ? n / 4 : 0;
+    float4* x4 = reinterpret_cast<float4*>(next);
+    float4* r4 = reinterpret_cast<float4*>(residual);
+    const float4* h4 = reinterpret_cast<const float4*>(h_prev);
+    GRID_STRIDE(q, n4) {
+        float4 x = x4[q];
+        float4 res = RESIDUAL ? r4[q] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        const float4 hp = RESIDUAL ? h4[q] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        step(x.x, res.x, hp.x);
+        step(x.y, res.y, hp.y);
+        step(x.z, res.z, hp.z);
+        step(x.w, res.w, hp.w);
+        x4[q] = x;
+        if (RESIDUAL) r4[q] = res;
+    }
+    TAIL_STRIDE(i, 4 * n4, n) {
+        float x = next[i];
+        float res = RESIDUAL ? residual[i] : 0.0f;
+        step(x, res, RESIDUAL ? h_prev[i] : 0.0f);
+        next[i] = x;
+        if (RESIDUAL) residual[i] = res;
     }
     if (RESIDUAL)
         grid_reduce<2>(v, r, [&](const double* t) {
