@@ -42,6 +42,7 @@ sys.path.insert(0, str(ROOT))
 METRIC = "EM iters/sec at 128x128x159 68Ga, learned vs plain projector, NRMSE<=1% vs FP64"
 ISOTOPE, RAYS, BETA, GAMMA, ITERS, SUPPORT_RHO, COUNTS = "68Ga", 128, 0.03, 20.0, 6, 0.05, 5e7
 L2_BYTES = 126 * 2**20
+REFERENCE_ARM_SECONDS = 60.0  # projection time sampled by the whole reference arm (wall time about 2x)
 
 
 def parse():
@@ -512,10 +513,12 @@ def oracle_check(rho, spacing, g, args):
 
 
 # ------------------------------------------------------------------------------- CPU baseline
-def cpu_baseline(rho, spacing, g, sample_seconds=15.0, seed=7):
+def cpu_baseline(rho, spacing, g, sample_seconds=15.0, seed=7, extras=True):
     """The oracle's float restatement of prc.cu (near block cached, far rays re-marched each
     projection, as the reference does) on all host cores, over a random sample of sources.
-    iters/s = 1 / (forward + adjoint time scaled to all sources + one RDP update)."""
+    iters/s = 1 / (forward + adjoint time scaled to all sources + one RDP update).  With
+    ``extras`` the record also times the reference's own CPU quadrature and the FP64
+    restatement on the small configuration."""
     sys.path.insert(0, str(ROOT))
     from oracle import oracle
     threads = os.cpu_count() or 1
@@ -541,11 +544,42 @@ def cpu_baseline(rho, spacing, g, sample_seconds=15.0, seed=7):
     full.update(g, g, BETA, GAMMA, 1e-6)
     t_update = time.perf_counter() - t0
     per_iter = dt * n_active / len(sample) + t_update
-    return {"value": round(1.0 / per_iter, 5), "unit": "EM iters/s", "cores": threads, "kind": "port",
+    info = {"value": round(1.0 / per_iter, 5), "unit": "EM iters/s", "cores": threads, "kind": "port",
             "sample": f"{len(sample)} of {n_active} sources ({100 * len(sample) / n_active:.2f}%): one forward "
                       f"and one adjoint projection ({dt:.1f} s), scaled to all sources, plus one full RDP "
-                      f"update ({t_update:.2f} s)",
-            "reference_quadrature": reference_quadrature()}
+                      f"update ({t_update:.2f} s)"}
+    if extras:
+        info["reference_quadrature"] = reference_quadrature()
+        info["small_configuration_fp64"] = small_configuration_fp64(threads)
+    return info
+
+
+def small_configuration_fp64(threads: int) -> dict:
+    """The FP64 restatement of prc.cu run end to end on the small configuration the reference's
+    own CPU-runnable case uses: 32x32x24 at 2 mm, 18F, 32 rays; the truth blurred by the
+    projector and Poisson-sampled at 1e6 counts, then --mode forward, --mode adjoint and
+    --mode correct with beta 0, no acceleration, 4 iterations (each with its own setup)."""
+    sys.path.insert(0, str(ROOT))
+    from oracle import oracle
+    from prc_mlem_b200 import phantoms
+    rho, truth, spacing = phantoms.small_phantom(seed=1)
+    t0 = time.perf_counter()
+    P = oracle.Problem("18F", rho, spacing, rays=32, precision=64, threads=threads)
+    g = phantoms.poisson_counts(P.forward(truth.astype(np.float64)).astype(np.float32), 1e6, seed=1)
+    t_data = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    for mode in ("forward", "adjoint", "correct"):
+        Q = oracle.Problem("18F", rho, spacing, rays=32, precision=64, threads=threads)
+        x = Q.clamp_input(g).astype(np.float64)
+        if mode == "forward":
+            Q.forward(x)
+        elif mode == "adjoint":
+            Q.adjoint(x)
+        else:
+            Q.correct(g, 4, beta=0.0, accelerate=False)
+    return {"seconds": round(time.perf_counter() - t0, 4), "cores": threads, "kind": "port",
+            "case": "32x32x24 at 2 mm, 18F, rays 32, 1e6 counts: forward, adjoint and 4 RL iterations "
+                    f"(beta 0, no acceleration) in FP64, each with its own setup; data made in {t_data:.2f} s"}
 
 
 def reference_quadrature(repeats=3):
@@ -573,8 +607,12 @@ def run_reference(args):
     g = phantoms_poisson_without_gpu(truth)
     vals = []
     info = None
-    for i in range(args.warmup + args.steps):
-        c = cpu_baseline(rho, spacing, g, sample_seconds=8.0, seed=11 + i)
+    # every step is a bounded sample of 1-8 s of projection time, REFERENCE_ARM_SECONDS shared over
+    # all steps, so the arm ends in about two to three minutes whatever --steps is
+    n_runs = args.warmup + args.steps
+    per_step = max(1.0, min(8.0, REFERENCE_ARM_SECONDS / max(n_runs, 1)))
+    for i in range(n_runs):
+        c = cpu_baseline(rho, spacing, g, sample_seconds=per_step, seed=11 + i, extras=i == n_runs - 1)
         if i >= args.warmup:
             vals.append(c["value"])
             info = c

@@ -43,3 +43,17 @@ def test_reference_quadrature_leg_times_the_restated_cpu_path():
     q = bench.reference_quadrature(repeats=1)
     assert q["seconds"] > 0 and q["cores"] == 1 and q["kind"] == "port"
     assert "68Ga" in q["case"] and "half-width 6" in q["case"]
+
+
+def test_small_configuration_fp64_runs_the_three_modes():
+    r = bench.small_configuration_fp64(2)
+    assert r["seconds"] > 0 and r["cores"] == 2 and r["kind"] == "port"
+    assert "32x32x24" in r["case"] and "4 RL iterations" in r["case"]
+
+
+def test_reference_arm_samples_are_bounded():
+    """1-8 s of projection time per step, shared so that the default 63 runs stay short."""
+    for runs in (1, 5, 13, 63, 1000):
+        per = max(1.0, min(8.0, bench.REFERENCE_ARM_SECONDS / runs))
+        assert 1.0 <= per <= 8.0
+        assert runs * per <= max(bench.REFERENCE_ARM_SECONDS, runs * 1.0)

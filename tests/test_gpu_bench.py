@@ -41,6 +41,7 @@ def test_our_arm_line():
     c = d["cpu_baseline"]
     assert c["kind"] == "port" and c["cores"] >= 1 and c["value"] > 0 and c["sample"]
     assert c["reference_quadrature"]["seconds"] > 0 and c["reference_quadrature"]["cores"] == 1
+    assert c["small_configuration_fp64"]["seconds"] > 0
     assert d["gpu_launches"] > 0
     assert {"sm_mhz", "sm_max_mhz", "reasons"} <= set(d["clocks"])
     assert d["image_quality"]["corrected"]["nrmse"] < d["image_quality"]["measured"]["nrmse"]
