@@ -42,7 +42,7 @@ sys.path.insert(0, str(ROOT))
 METRIC = "EM iters/sec at 128x128x159 68Ga, learned vs plain projector, NRMSE<=1% vs FP64"
 ISOTOPE, RAYS, BETA, GAMMA, ITERS, SUPPORT_RHO, COUNTS = "68Ga", 128, 0.03, 20.0, 6, 0.05, 5e7
 L2_BYTES = 126 * 2**20
-REFERENCE_ARM_SECONDS = 60.0  # projection time sampled by the whole reference arm (wall time about 2x)
+REFERENCE_ARM_SECONDS = 150.0  # host seconds of projection the reference arm's timed steps share
 
 
 def parse():
@@ -65,6 +65,11 @@ def parse():
     ap.add_argument("--workload", choices=("torso", "batch", "surrogate"), default="torso",
                     help="batch: 32 dynamic-PET frames of mixed grids and isotopes, 10 iterations each; "
                          "surrogate: the learned surrogate's evaluation on the small phantom at 128x128x159")
+    ap.add_argument("--no-parity", action="store_true",
+                    help="skip the comparison with the reference executable and the time-to-image leg")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-frames sub-record")
+    ap.add_argument("--oracle-full", action="store_true",
+                    help="also run the FP64 oracle on the whole volume (minutes on the host cores)")
     ap.add_argument("--frames", type=int, default=32)
     ap.add_argument("--surrogate", action="store_true", help="batch: learned surrogate where it applies")
     return ap.parse_args()
@@ -159,6 +164,18 @@ def algorithmic_bytes(n_vox: int, n_active: int, deposits: int, weight_bytes: in
             "compulsory": 74 * n_vox + 2 * 12 * n_active}
 
 
+def workload_config(grid, iterations: int, world: int) -> dict:
+    """The `config` both arms print: the workload, identical in the reference arm's line."""
+    nz, ny, nx = grid
+    return {"workload": f"torso {nx}x{ny}x{nz} at 0.776x0.776x0.795 mm, {ISOTOPE}, rays {RAYS}, beta {BETA}, "
+                        f"gamma {GAMMA:g}, accel on, support rho {SUPPORT_RHO}, {iterations} MAP-EM iterations "
+                        "per step",
+            "iterations_per_step": iterations,
+            "l2": "flushed (256 MB write) before every timed GPU step; every step also streams a multi-GB "
+                  "coefficient field, far above the 126 MB L2",
+            "parallelism": f"replicas x{world}" if world > 1 else "single GPU"}
+
+
 def make_workload(grid):
     from prc_mlem_b200 import phantoms
     rho, truth, spacing = phantoms.torso_phantom(seed=2, shape=tuple(grid))
@@ -216,11 +233,8 @@ def run_ours(args):
     P.synchronize()
     setup_s = time.perf_counter() - t0
     stream = torch.cuda.ExternalStream(P.stream)
-    d_truth = torch.from_numpy(truth).cuda()
-    d_blur = torch.empty_like(d_truth)
-    P.forward(d_truth, d_blur)
-    P.synchronize()
-    g_host = phantoms.poisson_counts_device(d_blur, COUNTS, seed=100 + rank).cpu().numpy()  # on the GPU
+    # (profiling runs with --ops make their data with the engine: no second process under ncu)
+    g_host, data_how, data_sha = measured_data(rho, truth, spacing, P, use_reference=world == 1 and not args.ops)
     d_g = torch.from_numpy(g_host).cuda()
     d_out = torch.empty_like(d_g)
     flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device="cuda")
@@ -251,6 +265,7 @@ def run_ours(args):
     times = []
     barrier()
     P.timing(True)  # CUDA events around every projection launch of the timed steps
+    launches0 = P.launches
     for _ in range(args.steps):
         l2_flush()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -260,6 +275,7 @@ def run_ours(args):
         e1.synchronize()
         times.append(e0.elapsed_time(e1))
     barrier()
+    launches_timed = P.launches - launches0  # this handle's kernels inside the timed region
     P.timing(False)
     in_region = P.timing_read()
     clock_info = clocks.stop()
@@ -322,13 +338,21 @@ def run_ours(args):
     stored_bytes = (far_t_entries if top == "forward" else far_entries) * elem
     traffic = ncu_traffic(f"{top}_{args.form}", stored_bytes) if mode == 2 else None
 
-    # the single-GPU line also carries the per-form comparison, the CPU baseline, the FP64-oracle
-    # check and the image quality; a multi-GPU run reports its timing only
+    # the single-GPU line also carries the per-form comparison, the parity with the reference
+    # executable, the time to a corrected image, the CPU baseline, the FP64-oracle check, the
+    # batch sub-record and the image quality; a multi-GPU run reports its timing only
     single = world == 1
     quality = image_quality(truth, g_host, corrected) if single else None
-    forms = None
+    forms = images = None
     if not args.no_forms and single:
-        forms = compare_forms(args, rho, spacing, d_g, stream, l2_flush, value, corrected, P)
+        forms, images = compare_forms(args, rho, spacing, d_g, stream, l2_flush, value, corrected, P)
+    parity = tti = None
+    if single and not args.no_parity:
+        parity, ref_job = parity_vs_prc_cu(P, rho, spacing, g_host, corrected, images or {}, args.iterations)
+        tti = time_to_image(rho, spacing, g_host, args, ref_job)
+    batch = None
+    if single and not args.no_batch:
+        batch = batch_record(frames=8, iterations=10, steps=2, warmup=1)
 
     if world > 1:
         torch.distributed.barrier()
@@ -338,6 +362,11 @@ def run_ours(args):
         return
     cpu = None if args.no_cpu_baseline or not single else cpu_baseline(rho, spacing, g_host, sample_seconds=15.0)
     check = None if args.no_oracle_check or not single else oracle_check(rho, spacing, g_host, args)
+    if check and args.oracle_full:
+        check["full_volume"] = oracle_full_volume(rho, spacing, g_host, args, corrected, images or {})
+    dram_frac = None
+    if traffic:
+        dram_frac = round(traffic / (region_ms[top] / 1e3) / 1e9 / peak, 4)
     line = {
         "metric": METRIC,
         "value": round(value, 3),
@@ -349,29 +378,33 @@ def run_ours(args):
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f32",
-        "data": "synthetic (seeded torso phantom, projector-blurred, Poisson 5e7 counts)",
-        "config": {
-            "workload": f"torso {nx}x{ny}x{nz} at 0.776x0.776x0.795 mm, {ISOTOPE}, rays {RAYS}, beta {BETA}, "
-                        f"gamma {GAMMA:g}, accel on, {args.iterations} MAP-EM iterations per step",
-            "form": {"fp32": "plain projector, fp32 stored coefficient field (near block + far rays)",
+        "dtype": "f32" if args.form != "bf16" else "bf16 (stored weights; f32 accumulation, f64 sums)",
+        "data": data_how,
+        "data_sha256": data_sha,
+        "config": workload_config(args.grid, args.iterations, world),
+        "details": {
+            "form": {"fp32": "fp32 stored coefficient field (near block + far rays), the reference's numerics",
                      "bf16": "mixed precision: bf16 stored coefficient field, fp32 accumulation, fp64 sums",
-                     "traced": "plain projector, near cache + far rays re-marched every projection"}[args.form],
+                     "traced": "plain ray-traced projector: near cache + far rays re-marched every projection"}[
+                         args.form],
             "n_active": n_active,
             "deposits_per_projection": deposits,
             "field_entries": {"source_major": far_entries, "target_major": far_t_entries},
             "voxels_per_s": round(value * n_vox, 1),
-            "setup_s": round(setup_s, 4),
-            "l2": "flushed (256 MB write) before every timed step; the step also streams a "
-                  f"{P.device_bytes / 1e9:.1f} GB coefficient field, far above the 126 MB L2",
-            "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+            "device_gb": round(P.device_bytes / 1e9, 2),
+            "first_handle_setup_s": round(setup_s, 4),
         },
         "e2e": {"value": round(e2e_value, 3), "unit": "EM iters/s",
                 "h2d_bytes_per_step": int(g_host.nbytes), "d2h_bytes_per_step": int(g_host.nbytes)},
         "roofline": {"bound": "hbm", "kernel": f"project_kernel {top} ({args.form} form)",
                      "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
-                     "traffic": traffic, "launch_ms": {k: round(v, 4) for k, v in region_ms.items()},
+                     "traffic": traffic,
+                     # measured DRAM bytes of the launch over its in-region time: the HBM fraction
+                     # (the fixed accounting above charges 4 B per gathered target value, which
+                     # the kernel reads from L1/L2, so `frac` can exceed 1)
+                     "dram_frac": dram_frac,
+                     "launch_ms": {k: round(v, 4) for k, v in region_ms.items()},
                      "launch_ms_alone": {k: round(v, 4) for k, v in launch_ms.items()},
                      "launches_timed": in_region["forward_launches"] + in_region["adjoint_launches"],
                      "projection_share_of_steps": round(projection_share, 4),
@@ -379,19 +412,24 @@ def run_ours(args):
                      # the whole MAP-EM iteration (both projections and the elementwise chain)
                      # over the mean iteration time of the timed steps
                      "iteration": iteration},
-        # per step: 3 initialisation kernels, then per iteration extrapolate, forward (u = f / W
-        # and the gather, or the scatter), ratio, adjoint, RDP update, finish
-        "gpu_launches": args.steps * (3 + (7 if far_t_entries else 6) * args.iterations),
+        "gpu_launches": launches_timed,
         "clocks": clock_info,
     }
-    if quality:
-        line["image_quality"] = quality
+    if parity:
+        line["parity_vs_prc_cu"] = parity
+    if tti:
+        line["time_to_image"] = tti
     if forms:
         line["forms"] = forms
+        line["targets"] = targets(forms, check)
+    if quality:
+        line["image_quality"] = quality
     if cpu:
         line["cpu_baseline"] = cpu
     if check:
         line["fp64_oracle_check"] = check
+    if batch:
+        line["batch"] = batch
     print(json.dumps(line))
     if world > 1:
         torch.distributed.destroy_process_group()
@@ -404,11 +442,13 @@ def nrmse(a, b):
 
 
 def compare_forms(args, rho, spacing, d_g, stream, l2_flush, value_fp32, corrected_fp32, P_fp32):
-    """EM iters/s of the other projector forms on the same data, and their agreement."""
+    """EM iters/s of the other projector forms on the same data, and their agreement.  Returns
+    (per-form record, per-form corrected image)."""
     import torch
     import prc_mlem_b200 as pm
     from prc_mlem_b200 import surrogate as sg
     out = {"fp32_field": {"iters_per_s": round(value_fp32, 3)}}
+    images = {"fp32_field": corrected_fp32}
     for name, kw in projector_forms(pm, sg, sg.load_trained()):
         t_setup = time.perf_counter()
         Q = pm.Projector(ISOTOPE, rho, spacing, rays=RAYS, support_rho=SUPPORT_RHO, **kw)
@@ -431,11 +471,89 @@ def compare_forms(args, rho, spacing, d_g, stream, l2_flush, value_fp32, correct
             ts.append(e0.elapsed_time(e1))
         v = args.iterations * steps / (sum(ts) / 1e3)
         img = d_out.cpu().numpy()
+        images[name] = img
         out[name] = {"iters_per_s": round(v, 3), "nrmse_vs_fp32_field": nrmse(img, corrected_fp32),
                      "device_gb": round(Q.device_bytes / 1e9, 3), "setup_s": round(t_setup, 3)}
         if "surrogate" in kw:
             out[name]["exact_fallback_share"] = round(Q.fallbacks / Q.n_active, 4)
         Q.close()
+    return out, images
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def parity_vs_prc_cu(P, rho, spacing, g, corrected, images, iterations):
+    """The headline data run through the reference executable (prc.cu built for sm_100a, on the
+    same GPU, outside the timed region): relative L2 of one forward and one adjoint projection
+    of the measured data and of every form's corrected image against the reference's, on the
+    full volume.  Returns (record, the reference's whole-job times)."""
+    from oracle import ref_exe
+    if not ref_exe.available():
+        return {"unavailable": "oracle/_ref/prc was not built (needs the reference source)"}, None
+    nz, ny, nx = rho.shape
+    sp = spacing
+    opts = ("--rays", str(RAYS), "--support-rho", str(SUPPORT_RHO))
+    em = ref_exe.run("correct", ISOTOPE, g, rho, sp, *opts, "--iterations", str(iterations), "--beta", str(BETA),
+                     "--gamma", str(GAMMA))
+    fwd = ref_exe.run("forward", ISOTOPE, g, rho, sp, *opts)
+    adj = ref_exe.run("adjoint", ISOTOPE, g, rho, sp, *opts)
+    support = np.maximum(rho, np.float32(1e-3)) >= np.float32(SUPPORT_RHO)
+    g_in = np.where(support, g, 0.0).astype(np.float32)
+    out = {"what": f"relative L2 against prc.cu (sm_100a build) on the same {nx}x{ny}x{nz} data, full volume",
+           "forward_fp32_field": rel_l2(P.forward_host(g_in), fwd["out"]),
+           "adjoint_fp32_field": rel_l2(P.adjoint_host(g_in), adj["out"]),
+           "corrected": {name: rel_l2(img, em["out"]) for name, img in ({"fp32_field": corrected} | images).items()},
+           "tolerance_fp32": 1e-5}
+    job = {"setup_s": em["setup_s"], "iterations_s": em["iterations_s"], "total_s": em["total_s"],
+           "process_wall_s": round(em["wall_s"], 3)}
+    return out, job
+
+
+def time_to_image(rho, spacing, g, args, ref_job):
+    """Seconds from density and data in host memory to the corrected image in host memory, for
+    a fresh handle in a warm CUDA context (library loaded, context created): prc_create (host
+    clamp and source order, uploads, layout, normalisation, both field copies) plus
+    prc_em_run_host (upload, the MAP-EM iterations, download).  Beside it the reference
+    executable's whole job on the same data: its normalisation plus its iterations, by its own
+    clock, and its total (which also counts reading the files and creating its CUDA context)."""
+    import prc_mlem_b200 as pm
+    out = {}
+    for name, kw in (("fp32_field", dict(cache=pm.PRC_CACHE_FULL)),
+                     ("bf16_field", dict(cache=pm.PRC_CACHE_FULL, precision=pm.PRC_PRECISION_BF16))):
+        t0 = time.perf_counter()
+        Q = pm.Projector(ISOTOPE, rho, spacing, rays=RAYS, support_rho=SUPPORT_RHO, **kw)
+        t1 = time.perf_counter()
+        Q.correct_host(g, args.iterations, BETA, GAMMA, True)
+        t2 = time.perf_counter()
+        Q.close()
+        out[name] = {"seconds": round(t2 - t0, 4), "setup_s": round(t1 - t0, 4), "iterations_s": round(t2 - t1, 4)}
+    if ref_job and ref_job.get("setup_s") is not None:
+        ref_s = ref_job["setup_s"] + ref_job["iterations_s"]
+        out["prc_cu"] = dict(ref_job, seconds=round(ref_s, 3),
+                             note="setup + iterations from its 2-decimal clock (prc.cu:644, 719-720)")
+        out["speedup_fp32_field"] = round(ref_s / out["fp32_field"]["seconds"], 2)
+        out["speedup_bf16_field"] = round(ref_s / out["bf16_field"]["seconds"], 2)
+    return out
+
+
+def targets(forms, check):
+    """Every form's EM iterations/s as a multiple of the plain ray-traced projector (the
+    reference's algorithm: near block cached, far rays re-marched every projection) and of the
+    fp32 stored field, beside its FP64-oracle NRMSE.  "plain" always means the traced form."""
+    traced = forms.get("traced", {}).get("iters_per_s")
+    fp32 = forms["fp32_field"]["iters_per_s"]
+    fp64 = (check or {}).get("forms", {})
+    out = {"plain": "traced: the reference's algorithm on B200 (near cache, far rays re-marched)"}
+    for name, f in forms.items():
+        v = f["iters_per_s"]
+        out[name] = {"iters_per_s": v,
+                     "x_plain_traced": round(v / traced, 3) if traced else None,
+                     "x_fp32_field": round(v / fp32, 3),
+                     "nrmse_vs_fp64": fp64.get(name, {}).get("nrmse_vs_fp64")}
     return out
 
 
@@ -510,6 +628,21 @@ def oracle_check(rho, spacing, g, args):
     return {"crop": f"{rc.shape[2]}x{rc.shape[1]}x{rc.shape[0]} voxels at the volume centre "
                     f"({int(support.sum())} tissue voxels)",
             "oracle_seconds": round(t_oracle, 1), "oracle_threads": threads, "forms": out}
+
+
+def oracle_full_volume(rho, spacing, g, args, corrected, images):
+    """The FP64 oracle's corrected image of the whole volume (minutes on all host cores) and the
+    NRMSE of every form's full-volume corrected image against it."""
+    from oracle import oracle
+    threads = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    O = oracle.Problem(ISOTOPE, rho, spacing, rays=RAYS, support_rho=SUPPORT_RHO, precision=64, threads=threads)
+    O.normalize()
+    ref = O.correct(np.ascontiguousarray(g, np.float32), args.iterations, BETA, GAMMA, True)
+    dt = time.perf_counter() - t0
+    forms = {"fp32_field": corrected} | images
+    return {"oracle_seconds": round(dt, 1), "oracle_threads": threads,
+            "nrmse_vs_fp64": {name: nrmse(img, ref) for name, img in forms.items()}}
 
 
 # ------------------------------------------------------------------------------- CPU baseline
@@ -600,45 +733,97 @@ def reference_quadrature(repeats=3):
 
 
 def run_reference(args):
+    """The reference's algorithm on the host cores (the oracle's float restatement of prc.cu:
+    near block cached, far rays re-marched every projection), with the reference executable on
+    the same GPU beside it.  Every timed step is one forward and one adjoint projection over a
+    fixed random half of the sources (fewer only when many steps would exceed the arm's time
+    budget), scaled to all
+    sources, plus one full RDP update; the normalisation pass is timed once on that half and
+    reported, scaled to all sources, as the setup.  Warm-up steps run 4 % of the half."""
     world, rank, _ = dist_env()
     if rank != 0:
         return
+    sys.path.insert(0, str(ROOT))
+    from oracle import oracle
     rho, truth, spacing = make_workload(args.grid)
-    g = phantoms_poisson_without_gpu(truth)
-    vals = []
-    info = None
-    # every step is a bounded sample of 1-8 s of projection time, REFERENCE_ARM_SECONDS shared over
-    # all steps, so the arm ends in about two to three minutes whatever --steps is
-    n_runs = args.warmup + args.steps
-    per_step = max(1.0, min(8.0, REFERENCE_ARM_SECONDS / max(n_runs, 1)))
-    for i in range(n_runs):
-        c = cpu_baseline(rho, spacing, g, sample_seconds=per_step, seed=11 + i, extras=i == n_runs - 1)
-        if i >= args.warmup:
-            vals.append(c["value"])
-            info = c
+    g, data_how, data_sha = measured_data(rho, truth, spacing)
+    threads = os.cpu_count() or 1
+    full = oracle.Problem(ISOTOPE, rho, spacing, rays=RAYS, support_rho=SUPPORT_RHO, precision=32, threads=threads)
+    n_active = full.n_active
+    x = g.astype(np.float32)
+    t0 = time.perf_counter()
+    full.update(g, g, BETA, GAMMA, 1e-6)
+    t_update = time.perf_counter() - t0
+
+    # one fixed random half of the sources, normalised once (timed: the setup, scaled to all)
+    rng = np.random.default_rng(101)
+    half = np.sort(rng.choice(n_active, size=max(64, n_active // 2), replace=False))
+    base = oracle.Problem(ISOTOPE, rho, spacing, rays=RAYS, support_rho=SUPPORT_RHO, precision=32, threads=threads)
+    base.active = np.ascontiguousarray(full.active[half])
+    t0 = time.perf_counter()
+    base.normalize()
+    setup_s = (time.perf_counter() - t0) * n_active / len(half)
+
+    def step(frac, seed):
+        """One forward and one adjoint projection over `frac` of the normalised half."""
+        pick = np.arange(len(half))
+        if frac < 1.0:
+            pick = np.sort(np.random.default_rng(seed).choice(len(half), size=max(64, int(len(half) * frac)),
+                                                              replace=False))
+        sub = oracle.Problem(ISOTOPE, rho, spacing, rays=RAYS, support_rho=SUPPORT_RHO, precision=32,
+                             threads=threads)
+        sub.active = np.ascontiguousarray(base.active[pick])
+        sub.W, sub.near = np.ascontiguousarray(base.W[pick]), np.ascontiguousarray(base.near[pick])
+        t0 = time.perf_counter()
+        sub.forward(x)
+        sub.adjoint(x)
+        spent = time.perf_counter() - t0
+        return len(pick), spent * n_active / len(pick), spent
+
+    for i in range(args.warmup):
+        step(0.04, 11 + i)
+    budget = REFERENCE_ARM_SECONDS  # host seconds of projection the timed steps may take together
+    frac, vals, fracs = 1.0, [], []
+    for i in range(args.steps):
+        n_sample, pair_s, spent = step(frac, 1001 + i)
+        vals.append(1.0 / (pair_s + t_update))
+        fracs.append(n_sample / n_active)
+        budget -= spent
+        left = args.steps - i - 1
+        if left and budget < left * spent:  # keep the arm within a few minutes for any --steps
+            frac = max(0.1, frac * max(budget, 0.0) / (left * spent))
     value = statistics.mean(vals)
-    info["value"] = round(value, 5)
-    nz, ny, nx = args.grid
+    per_iter = 1.0 / value
+    info = {"value": round(value, 5), "unit": "EM iters/s", "cores": threads, "kind": "port",
+            "sample": f"per step one forward and one adjoint projection over a random {100 * min(fracs):.0f}-"
+                      f"{100 * max(fracs):.0f}% of the {n_active} sources, scaled to all sources, plus one full "
+                      f"RDP update ({t_update:.2f} s); {args.steps} steps",
+            "setup_s": round(setup_s, 2),
+            "time_to_image_s": round(setup_s + args.iterations * per_iter, 2),
+            "reference_quadrature": reference_quadrature(),
+            "small_configuration_fp64": small_configuration_fp64(threads)}
     line = {
         "metric": METRIC, "impl": "reference", "value": round(value, 5), "unit": "EM iters/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded torso phantom)",
-        "config": {"workload": f"torso {nx}x{ny}x{nz} at 0.776x0.776x0.795 mm, {ISOTOPE}, rays {RAYS}, "
-                               f"beta {BETA}, gamma {GAMMA:g}, accel on, {args.iterations} MAP-EM iterations"},
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": data_how,
+        "data_sha256": data_sha,
+        "config": workload_config(args.grid, args.iterations, world),
         "cpu_baseline": info,
         "e2e": {"value": round(value, 5), "unit": "EM iters/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "reference_gpu": reference_gpu(rho, g),
+        "reference_gpu": reference_gpu(rho, spacing, g, args.iterations),
     }
     print(json.dumps(line))
 
 
-def reference_gpu(rho, g, iterations=30):
-    """EM iterations/s of the reference executable itself (prc.cu compiled for sm_100a by
-    oracle/build_ref.sh) on the same workload, from its own `iterations X s` line."""
-    import re
-    import tempfile
-    exe = ROOT / "oracle" / "_ref" / "prc"
-    if not exe.is_file():
+def reference_gpu(rho, spacing, g, iterations: int, rate_iterations: int = 60):
+    """The reference executable itself (prc.cu compiled for sm_100a by oracle/build_ref.sh) on
+    the same workload: the whole job of `iterations` MAP-EM iterations (normalisation plus
+    iterations, by its own clock, and its total), and its iteration rate from a run of
+    `rate_iterations` (its clock prints 2 decimals, so a short run cannot give the rate)."""
+    sys.path.insert(0, str(ROOT))
+    from oracle import ref_exe
+    if not ref_exe.available():
         return {"unavailable": "oracle/_ref/prc was not built (needs the reference source)"}
     try:
         import torch
@@ -646,30 +831,55 @@ def reference_gpu(rho, g, iterations=30):
             return {"unavailable": "no CUDA device"}
     except Exception:
         return {"unavailable": "no CUDA device"}
-    nz, ny, nx = rho.shape
-    with tempfile.TemporaryDirectory() as d:
-        d = Path(d)
-        rho.astype(np.float32).tofile(d / "rho.raw")
-        g.astype(np.float32).tofile(d / "g.raw")
-        cmd = [str(exe), ISOTOPE, str(nx), str(ny), str(nz), "0.776", "0.776", "0.795", "--input", str(d / "g.raw"),
-               "--density", str(d / "rho.raw"), "--output", str(d / "out.raw"), "--rays", str(RAYS), "--beta",
-               str(BETA), "--gamma", str(GAMMA), "--support-rho", str(SUPPORT_RHO), "--iterations", str(iterations)]
-        r = subprocess.run(cmd, capture_output=True, text=True, timeout=900)
-    m = re.search(r"iterations ([0-9.]+) s", r.stdout)
-    n = re.search(r"normalisation .*: ([0-9.]+) s", r.stdout)
-    if r.returncode != 0 or not m:
-        return {"unavailable": f"reference executable failed: {r.stderr.strip()[:200]}"}
-    secs = float(m.group(1))
-    return {"value": round(iterations / secs, 3), "unit": "EM iters/s", "iterations": iterations,
-            "iteration_seconds": secs, "setup_seconds": float(n.group(1)) if n else None,
+    sp = spacing
+    opts = ("--rays", str(RAYS), "--beta", str(BETA), "--gamma", str(GAMMA), "--support-rho", str(SUPPORT_RHO))
+    try:
+        job = ref_exe.run("correct", ISOTOPE, g, rho, sp, *opts, "--iterations", str(iterations))
+        rate = ref_exe.run("correct", ISOTOPE, g, rho, sp, *opts, "--iterations", str(rate_iterations))
+    except (RuntimeError, OSError, subprocess.TimeoutExpired) as e:
+        return {"unavailable": f"reference executable failed: {str(e)[:200]}"}
+    return {"value": round(rate_iterations / rate["iterations_s"], 3), "unit": "EM iters/s",
+            "rate_iterations": rate_iterations, "rate_iteration_seconds": rate["iterations_s"],
+            "job": {"iterations": iterations, "setup_s": job["setup_s"], "iterations_s": job["iterations_s"],
+                    "seconds": round(job["setup_s"] + job["iterations_s"], 3), "total_s": job["total_s"]},
             "what": "prc.cu built for sm_100a, timed by its own 2-decimal clock"}
 
 
-def phantoms_poisson_without_gpu(truth):
-    """Measured data for the CPU arm: the truth Poisson-sampled at 5e7 counts (projection cost
-    does not depend on the activity values, only on the density)."""
+def measured_data(rho, truth, spacing, P=None, use_reference=True):
+    """The measured data both arms correct: the truth blurred by the plain projector with 128
+    rays -- the reference executable's own forward projection where it is built, else the
+    engine's fp32 field (`P`) -- and Poisson-sampled at 5e7 counts with seed 100 by the
+    counter-based device sampler (prc_poisson: every count depends only on its own mean, so the
+    last-bit noise of the reference's atomic forward changes no other voxel's count).
+    Multi-GPU replicas use the engine (the reference executable runs on one device only).
+    Returns (data, description, sha256 prefix of its bytes)."""
+    import hashlib
+    from oracle import ref_exe
     from prc_mlem_b200 import phantoms
-    return phantoms.poisson_counts(truth, COUNTS, seed=100)
+    blur, how = None, None
+    if use_reference and ref_exe.available():
+        try:
+            blur = ref_exe.run("forward", ISOTOPE, truth, rho, spacing, "--rays", str(RAYS),
+                               "--support-rho", str(SUPPORT_RHO))["out"]
+            how = "synthetic (seeded torso phantom, blurred by prc.cu's projector, Poisson 5e7 counts)"
+        except (RuntimeError, OSError, subprocess.TimeoutExpired):
+            blur = None
+    if blur is None and P is not None:
+        blur, how = P.forward_host(truth), "synthetic (seeded torso phantom, blurred by the fp32 field, Poisson 5e7)"
+    if blur is None:  # projection cost does not depend on the activity values, only on the density
+        blur, how = truth, "synthetic (seeded torso phantom, unblurred truth Poisson-sampled at 5e7 counts)"
+    try:
+        import torch
+        cuda = torch.cuda.is_available()
+    except ImportError:
+        cuda = False
+    if cuda:
+        g = phantoms.poisson_counts_device(torch.from_numpy(np.ascontiguousarray(blur, np.float32)).cuda(), COUNTS,
+                                           seed=100).cpu().numpy()
+    else:
+        g = phantoms.poisson_counts(blur, COUNTS, seed=100)
+        how += " (host sampler: no CUDA device)"
+    return g, how, hashlib.sha256(g.tobytes()).hexdigest()[:16]
 
 
 # ------------------------------------------------------------------------------- batched frames
@@ -677,24 +887,26 @@ BATCH_GRIDS = ((64, 64, 64), (80, 96, 96), (159, 128, 128), (200, 192, 192))
 BATCH_ISOTOPES = ("11C", "15O", "18F", "68Ga")
 
 
-def run_batch(args):
+def batch_record(frames: int, iterations: int, steps: int, warmup: int, surrogate: bool = False,
+                 clocks: bool = False) -> dict:
     """Dynamic-PET frames: grids drawn from {64^3, 96x96x80, 128x128x159, 192x192x200}, isotopes
     from {11C, 15O, 18F, 68Ga}, each the torso generator with its own seed and counts
-    log-uniform in [1e5, 5e7]; 10 MAP-EM iterations (beta 0.03, gamma 20, accelerated) of every
-    frame per step, all frames in one launch per phase inside one captured CUDA graph."""
+    log-uniform in [1e5, 5e7]; `iterations` MAP-EM iterations (beta 0.03, gamma 20,
+    accelerated) of every frame per step, all frames in one launch per phase inside one
+    captured CUDA graph.  Returns the record (frames/s and its context)."""
     import torch
     import prc_mlem_b200 as pm
     from prc_mlem_b200 import phantoms, surrogate as sg
     torch.cuda.set_device(0)
     rng = np.random.default_rng(5)
     specs = []
-    for i in range(args.frames):
+    for i in range(frames):
         shape = BATCH_GRIDS[rng.integers(len(BATCH_GRIDS))]
         iso = BATCH_ISOTOPES[rng.integers(len(BATCH_ISOTOPES))]
         counts = float(np.exp(rng.uniform(np.log(1e5), np.log(5e7))))
         rho, truth, sp = phantoms.torso_phantom(seed=100 + i, shape=shape)
         specs.append((iso, rho, sp, truth, counts))
-    net = sg.load_trained() if args.surrogate else None
+    net = sg.load_trained() if surrogate else None
     t0 = time.perf_counter()
     batch = pm.Batch([(iso, rho, sp) for iso, rho, sp, _, _ in specs], precision=pm.PRC_PRECISION_BF16,
                      surrogate=net, target_scale=sg.TARGET_SCALE, fallback_nrmse=0.3 if net else 0.0)
@@ -708,43 +920,54 @@ def run_batch(args):
         outs.append(torch.empty_like(d_t))
     torch.cuda.synchronize()  # the counts are drawn on torch's stream, the batch runs on its own
     stream = torch.cuda.ExternalStream(batch.stream)
-    for _ in range(args.warmup):
-        batch.correct(gs, outs, 10, BETA, GAMMA, True)
+    for _ in range(warmup):
+        batch.correct(gs, outs, iterations, BETA, GAMMA, True)
     batch.synchronize()
-    clocks = ClockSampler(0)
-    clocks.start()
+    sampler = ClockSampler(0) if clocks else None
+    if sampler:
+        sampler.start()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    for _ in range(args.steps):
-        batch.correct(gs, outs, 10, BETA, GAMMA, True)
+    for _ in range(steps):
+        batch.correct(gs, outs, iterations, BETA, GAMMA, True)
     e1.record(stream)
     e1.synchronize()
     batch.synchronize()
-    clock_info = clocks.stop()
+    clock_info = sampler.stop() if sampler else None
     ms = e0.elapsed_time(e1)
-    frames_per_s = args.frames * args.steps / (ms / 1e3)
+    frames_per_s = frames * steps / (ms / 1e3)
     # per-frame NRMSE against the plain method (fp32 weights, reference numerics), first 4 frames
     nrmse_list = []
-    for i in range(min(4, args.frames)):
+    for i in range(min(4, frames)):
         iso, rho, sp, truth, counts = specs[i]
         with pm.Projector(iso, rho, sp, cache=pm.PRC_CACHE_NEAR) as P:
             d = torch.empty_like(gs[i])
-            P.correct(gs[i], d, 10, BETA, GAMMA, True)
+            P.correct(gs[i], d, iterations, BETA, GAMMA, True)
             P.synchronize()
             nrmse_list.append(nrmse(outs[i].cpu().numpy(), d.cpu().numpy()))
-    modes = collections.Counter(batch.cache_mode(i)[0] for i in range(args.frames))
-    print(json.dumps({
-        "metric": "batched dynamic-PET frames per second (10 MAP-EM iterations each)",
-        "value": round(frames_per_s, 3), "unit": "frames/s", "n_gpus": 1, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True,
-        "em_iters_per_s": round(frames_per_s * 10, 2), "dtype": "f32 (bf16 stored weights)",
-        "config": {"workload": f"{args.frames} frames, grids {BATCH_GRIDS}, isotopes {BATCH_ISOTOPES}, "
-                               "torso phantoms, counts log-uniform 1e5-5e7, beta 0.03, gamma 20, accel",
-                   "frames": [f"{iso} {rho.shape[2]}x{rho.shape[1]}x{rho.shape[0]}" for iso, rho, *_ in specs],
-                   "projector_forms": {str(k): v for k, v in modes.items()},
-                   "surrogate": bool(net), "autotuned_warps_per_block": batch.warps, "setup_s": round(setup_s, 2)},
-        "nrmse_vs_plain_first_frames": nrmse_list, "clocks": clock_info}))
+    modes = collections.Counter(batch.cache_mode(i)[0] for i in range(frames))
+    rec = {"value": round(frames_per_s, 3), "unit": "frames/s", "steps": steps, "warmup": warmup,
+           "ms_per_step": round(ms / steps, 3), "em_iters_per_s": round(frames_per_s * iterations, 2),
+           "dtype": "f32 (bf16 stored weights)",
+           "config": {"workload": f"{frames} frames, grids {BATCH_GRIDS}, isotopes {BATCH_ISOTOPES}, torso "
+                                  f"phantoms, counts log-uniform 1e5-5e7, {iterations} MAP-EM iterations, beta 0.03, "
+                                  "gamma 20, accel",
+                      "frames": [f"{iso} {rho.shape[2]}x{rho.shape[1]}x{rho.shape[0]}" for iso, rho, *_ in specs],
+                      "projector_forms": {str(k): v for k, v in modes.items()},
+                      "surrogate": bool(net), "autotuned": {"warps_per_block": batch.warps},
+                      "setup_s": round(setup_s, 2)},
+           "nrmse_vs_plain_first_frames": nrmse_list}
+    if clock_info:
+        rec["clocks"] = clock_info
     batch.close()
+    return rec
+
+
+def run_batch(args):
+    rec = batch_record(args.frames, 10, args.steps, args.warmup, surrogate=args.surrogate, clocks=True)
+    rec = {"metric": "batched dynamic-PET frames per second (10 MAP-EM iterations each)", "n_gpus": 1,
+           "higher_is_better": True} | rec
+    print(json.dumps(rec))
 
 
 def run_surrogate_eval(args):

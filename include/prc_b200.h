@@ -177,8 +177,12 @@ int prc_count_deposits(prc_handle* h, int64_t* deposits);
  * synchronisation, operators inside another framework's allocator).  Its scratch is a
  * file-scope device array of about 512 KiB that every GPU loading the library holds until
  * exit; n is limited to 2^28 elements (PRC_ERR_LIMIT beyond).  The first call on each device
- * looks up that array's device address, so it should come before any stream capture.  All
- * calls share the array: calls that overlap on the GPU (other streams, other threads) race. */
+ * looks up that array's device address, and under CUDA's lazy module loading (the default)
+ * that lookup is what loads the array onto the device: make one warm-up call per device at
+ * start-up, before reserving the rest of device memory and before any stream capture (or run
+ * with CUDA_MODULE_LOADING=EAGER); later calls allocate nothing.  A failed lookup is retried by
+ * the next call.  All calls share the array: calls that overlap on the GPU (other streams,
+ * other threads) race. */
 int prc_sum_static(const float* d_x, int64_t n, double* d_sum, void* stream);
 
 /* ---- batched frames (dynamic PET) ---------------------------------------------------------
@@ -217,6 +221,11 @@ int prc_batch_warps(const prc_batch* b);
  * launches of each kind since the start. */
 int prc_timing(prc_handle* h, int enable);
 int prc_timing_read(prc_handle* h, double* forward_ms, int64_t* n_forward, double* adjoint_ms, int64_t* n_adjoint);
+
+/* Number of kernels the handle's entry points have enqueued since it was created (projections,
+ * MAP-EM image updates and reductions; copies and memsets are not counted).  No counterpart in
+ * the reference. */
+int prc_launch_count(const prc_handle* h, int64_t* n);
 
 /* Waits for all work on the handle's stream; reports PRC_ERR_CUDA if a kernel gave up a
  * bounded wait since the last check. */

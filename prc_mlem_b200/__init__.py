@@ -79,6 +79,7 @@ _SIGNATURES = {
     "prc_sum": (ctypes.c_int, [_P, _P, ctypes.POINTER(ctypes.c_double), _P]),
     "prc_count_deposits": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int64)]),
     "prc_synchronize": (ctypes.c_int, [_P]),
+    "prc_launch_count": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int64)]),
     "prc_wait_selftest": (ctypes.c_int, [_P, ctypes.c_int]),
     "prc_sum_static": (ctypes.c_int, [_P, ctypes.c_int64, _P, _P]),
     "prc_create_surrogate": (ctypes.c_int, [ctypes.POINTER(Geometry), ctypes.c_char_p, ctypes.POINTER(Options), _P,
@@ -300,6 +301,13 @@ class Projector:
     def sum(self, d_x) -> float:
         v = ctypes.c_double()
         _check(lib().prc_sum(self._h, _ptr(d_x), ctypes.byref(v), None))
+        return v.value
+
+    @property
+    def launches(self) -> int:
+        """Kernels this handle has enqueued since it was created (prc_launch_count)."""
+        v = ctypes.c_int64()
+        _check(lib().prc_launch_count(self._h, ctypes.byref(v)))
         return v.value
 
     def count_deposits(self) -> int:

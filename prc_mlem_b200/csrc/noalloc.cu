@@ -10,11 +10,19 @@
 // scratch (block partials and a completion counter) in a file-scope __device__ array that is
 // part of the library image: every GPU that loads the library holds it (kStaticBlocks * 8 + 256
 // bytes, about 512 KiB) until the process exits.
+//
+// When the array is committed: under CUDA's lazy module loading (the default since CUDA 12.2)
+// the module holding it is loaded on a device by the first address lookup, i.e. by the first
+// prc_sum_static call made with that device current; with CUDA_MODULE_LOADING=EAGER it is
+// loaded with the library.  A caller that must not allocate after start-up therefore makes one
+// warm-up call per device at start-up (before reserving its memory and before any stream
+// capture); every later call allocates nothing.
 #include "../../include/prc_b200.h"
 #include "engine.h"
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <mutex>
 #include <string>
 
@@ -30,11 +38,30 @@ constexpr int kMaxDevices = 64;
 // [0, 256): the completion counter (first 4 bytes); [256, 256 + 8 * kStaticBlocks): partials.
 static __device__ __align__(256) unsigned char g_sum_scratch[256 + sizeof(double) * kStaticBlocks];
 
-// Per-device address of g_sum_scratch, looked up once per device (the name is only a host
-// stand-in for the device symbol; a kernel must be given the device address).
-void* g_scratch_ptr[kMaxDevices] = {};
-cudaError_t g_scratch_err[kMaxDevices] = {};
-std::once_flag g_scratch_once[kMaxDevices];
+// Per-device address of g_sum_scratch (the name is only a host stand-in for the device symbol;
+// a kernel must be given the device address).  Only a successful lookup is kept, so a lookup
+// that failed for a passing reason (for example inside a stream capture) is retried by the
+// next call.
+std::atomic<void*> g_scratch_ptr[kMaxDevices] = {};
+std::mutex g_scratch_mutex;
+
+cudaError_t scratch_address(int dev, unsigned char** out) {
+    void* p = g_scratch_ptr[dev].load(std::memory_order_acquire);
+    if (!p) {
+        std::lock_guard<std::mutex> lock(g_scratch_mutex);
+        p = g_scratch_ptr[dev].load(std::memory_order_relaxed);
+        if (!p) {
+            const cudaError_t e = cudaGetSymbolAddress(&p, g_sum_scratch);  // with `dev` current
+            if (e != cudaSuccess) {
+                cudaGetLastError();  // a failed lookup leaves no error behind for the caller
+                return e;
+            }
+            g_scratch_ptr[dev].store(p, std::memory_order_release);
+        }
+    }
+    *out = static_cast<unsigned char*>(p);
+    return cudaSuccess;
+}
 
 __global__ void __launch_bounds__(kStaticThreads) static_sum_kernel(const float* __restrict__ x, long long n,
                                                                     unsigned char* scratch, double* out) {
@@ -91,15 +118,10 @@ extern "C" int prc_sum_static(const float* d_x, int64_t n, double* d_sum, void* 
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e == cudaSuccess && (dev < 0 || dev >= kMaxDevices)) e = cudaErrorInvalidDevice;
-    if (e == cudaSuccess) {
-        // Once per device, with that device current: the device address of the scratch array.
-        std::call_once(g_scratch_once[dev], [dev] {
-            g_scratch_err[dev] = cudaGetSymbolAddress(&g_scratch_ptr[dev], g_sum_scratch);
-        });
-        e = g_scratch_err[dev];
-    }
+    // The device address of the scratch array, looked up once per device with it current.
+    unsigned char* scratch = nullptr;
+    if (e == cudaSuccess) e = scratch_address(dev, &scratch);
     const cudaStream_t s = static_cast<cudaStream_t>(stream);
-    unsigned char* scratch = static_cast<unsigned char*>(g_scratch_ptr[dev < kMaxDevices ? dev : 0]);
     // The array keeps the previous call's contents: the counter must start at zero.
     if (e == cudaSuccess) e = cudaMemsetAsync(scratch, 0, sizeof(unsigned int), s);
     if (e == cudaSuccess) {

@@ -91,6 +91,7 @@ struct prc_handle {
     Reduction red{};
     bool em_started = false;
     int64_t bytes = 0;
+    int64_t launches = 0;  // kernels this handle's entry points have enqueued (prc_launch_count)
 
     std::vector<void*> allocations;
     // projection timing (prc_timing): start/end event pairs of forward and adjoint launches
@@ -702,12 +703,14 @@ int prc_forward(prc_handle* h, const float* d_in, float* d_out, void* stream) {
     a.out = d_out;
     if (h->far_t.on()) {  // gather form: u = f / W, then out[t] = sum_k T_tk u[t - o_k]
         PRC_CUDA(forward_prep(h->params, h->W, d_in, h->u, d_out, s));
+        ++h->launches;
         a.in = h->u;
     } else {
         PRC_CUDA(cudaMemsetAsync(d_out, 0, h->n * sizeof(float), s));
     }
     PRC_CUDA(timing_mark(h, 0, s));
     PRC_CUDA(project(Op::Forward, h->params, a, h->trace_near, s));
+    ++h->launches;
     PRC_CUDA(timing_mark(h, 0, s));
     return PRC_OK;
 }
@@ -720,6 +723,7 @@ int prc_adjoint(prc_handle* h, const float* d_in, float* d_out, void* stream) {
     const cudaStream_t s = h->pick(stream);
     PRC_CUDA(timing_mark(h, 1, s));
     PRC_CUDA(project(Op::Adjoint, h->params, a, h->trace_near, s));
+    ++h->launches;
     PRC_CUDA(timing_mark(h, 1, s));
     return PRC_OK;
 }
@@ -744,6 +748,7 @@ static int em_begin_impl(prc_handle* h, const float* d_g, bool initialize, cudaS
     PRC_CUDA(cudaMemsetAsync(h->y, 0, h->n * sizeof(float), s));
     PRC_CUDA(cudaMemsetAsync(h->h_prev, 0, h->n * sizeof(float), s));
     PRC_CUDA(em_begin(h->em_volumes(), d_g, h->g_em, h->f, h->n_active, initialize, s));
+    h->launches += initialize ? 3 : 1;
     h->em_started = true;
     return PRC_OK;
 }
@@ -764,16 +769,21 @@ int prc_em_iterate(prc_handle* h, int n_iter, float beta, float gamma, int accel
         const float* start = h->f;
         if (accelerate) {
             PRC_CUDA(em_extrapolate(v, h->f, h->prev, h->y, s));
+            ++h->launches;
             start = h->y;
         }
         int rc = prc_forward(h, start, h->est, s);
         if (rc != PRC_OK) return rc;
         PRC_CUDA(em_ratio(v, h->g_em, h->est, s));
+        ++h->launches;
         rc = prc_adjoint(h, h->est, h->prev, s);  // prediction has consumed prev
         if (rc != PRC_OK) return rc;
         PRC_CUDA(em_update(v, h->g, start, h->prev, h->est, beta, gamma, s));
-        if (beta > 0.0f || accelerate)
+        ++h->launches;
+        if (beta > 0.0f || accelerate) {
             PRC_CUDA(em_finish(v, h->est, accelerate ? h->y : nullptr, h->h_prev, beta > 0.0f, s));
+            ++h->launches;
+        }
         if (accelerate) {
             std::swap(h->y, h->h_prev);
             std::swap(h->prev, h->f);
@@ -871,6 +881,7 @@ int prc_sum(prc_handle* h, const float* d_x, double* sum, void* stream) {
     if (rc != PRC_OK) return rc;
     const cudaStream_t s = h->pick(stream);
     PRC_CUDA(em_sum(h->em_volumes(), d_x, s));
+    ++h->launches;
     PRC_CUDA(cudaMemcpyAsync(sum, &h->scalars->sum, sizeof(double), cudaMemcpyDeviceToHost, s));
     PRC_CUDA(cudaStreamSynchronize(s));
     return PRC_OK;
@@ -893,6 +904,12 @@ int prc_wait_selftest(prc_handle* h, int rounds) {
     if (!h || rounds < 1 || rounds > (1 << 20)) return fail(PRC_ERR_ARGUMENT, "Invalid argument");
     PRC_CUDA(wait_selftest(rounds, h->error, h->stream));
     return prc_synchronize(h);
+}
+
+int prc_launch_count(const prc_handle* h, int64_t* n) {
+    if (!h || !n) return fail(PRC_ERR_ARGUMENT, "Invalid argument");
+    *n = h->launches;
+    return PRC_OK;
 }
 
 int prc_synchronize(prc_handle* h) {

@@ -15,6 +15,8 @@
 #include <cstring>
 #include <string>
 #include <thread>
+#include <type_traits>
+#include <utility>
 #include <vector>
 
 namespace {
@@ -26,17 +28,19 @@ double now_s() {
     return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
 
-struct Options {  // prc.cu:452-459
+// Everything the command line can set.  Defaults are the reference's (prc.cu:452-459); the
+// last two fields are this engine's additions (--cache, --bf16-weights).
+struct Settings {
     std::string isotope, mode = "correct", input = "ACTIVITY.raw", density = "DENSITY.raw", output;
-    int nx = 0, ny = 0, nz = 0;
-    float dx = 0, dy = 0, dz = 0;
+    int dims[3] = {0, 0, 0};       // NX NY NZ
+    float voxel[3] = {0, 0, 0};    // DX DY DZ [mm]
     int rays = 128, iterations = 20, save_every = 0;
     float beta = 0.2f, gamma = 20.0f, support_rho = 0.05f, air_cap_mm = 50.0f;
-    bool reproject = false, cache_near = true, exact_range = false, accelerate = true, bf16 = false;
+    bool reproject = false, trace_near_every_pass = false, exact_range = false, plain = false, bf16 = false;
     int cache = PRC_CACHE_FULL;
 };
 
-void print_usage(const char* prog, FILE* stream = stderr) {  // prc.cu:461-484
+void print_usage(const char* prog, FILE* stream = stderr) {  // the usage text of prc.cu:461-484
     fprintf(stream,
             "Usage: %s ISOTOPE NX NY NZ DX DY DZ [options]\n"
             "  --mode correct|forward|adjoint   (default correct)\n"
@@ -65,99 +69,133 @@ void print_usage(const char* prog, FILE* stream = stderr) {  // prc.cu:461-484
 
 [[noreturn]] void die() { exit(EXIT_FAILURE); }
 
-int parse_int(const char* text, const char* name) {  // prc.cu:486-495
+// A whole-string decimal number.  The messages are the reference's, which its tests match.
+template <class T>
+T number(const char* text, const char* label) {
     char* end = nullptr;
     errno = 0;
-    const long value = strtol(text, &end, 10);
-    if (errno || end == text || *end || value < INT_MIN || value > INT_MAX) {
-        fprintf(stderr, "Invalid integer for %s: %s\n", name, text);
-        die();
+    bool ok;
+    T value;
+    if constexpr (std::is_same_v<T, int>) {
+        const long long v = strtoll(text, &end, 10);
+        ok = v >= INT_MIN && v <= INT_MAX;
+        value = (int)v;
+    } else {
+        value = strtof(text, &end);
+        ok = std::isfinite(value);
     }
-    return (int)value;
-}
-
-float parse_float(const char* text, const char* name) {  // prc.cu:497-506
-    char* end = nullptr;
-    errno = 0;
-    const float value = strtof(text, &end);
-    if (errno || end == text || *end || !std::isfinite(value)) {
-        fprintf(stderr, "Invalid finite number for %s: %s\n", name, text);
+    if (errno != 0 || end == text || *end != '\0' || !ok) {
+        fprintf(stderr, std::is_same_v<T, int> ? "Invalid integer for %s: %s\n" : "Invalid finite number for %s: %s\n",
+                label, text);
         die();
     }
     return value;
 }
 
-Options parse(int argc, char** argv) {  // prc.cu:508-555
-    Options o;
-    if (argc < 8) {
+// The option table: a name, whether it takes a value, and what it does with it.
+using Apply = void (*)(Settings&, const char* value, const char* name);
+struct Spec {
+    const char* name;
+    bool takes_value;
+    Apply apply;
+};
+const Spec kSpecs[] = {
+    {"--mode", true, [](Settings& s, const char* v, const char*) { s.mode = v; }},
+    {"--input", true, [](Settings& s, const char* v, const char*) { s.input = v; }},
+    {"--density", true, [](Settings& s, const char* v, const char*) { s.density = v; }},
+    {"--output", true, [](Settings& s, const char* v, const char*) { s.output = v; }},
+    {"--rays", true, [](Settings& s, const char* v, const char* n) { s.rays = number<int>(v, n); }},
+    {"--iterations", true, [](Settings& s, const char* v, const char* n) { s.iterations = number<int>(v, n); }},
+    {"--beta", true, [](Settings& s, const char* v, const char* n) { s.beta = number<float>(v, n); }},
+    {"--gamma", true, [](Settings& s, const char* v, const char* n) { s.gamma = number<float>(v, n); }},
+    {"--support-rho", true, [](Settings& s, const char* v, const char* n) { s.support_rho = number<float>(v, n); }},
+    {"--air-cap-mm", true, [](Settings& s, const char* v, const char* n) { s.air_cap_mm = number<float>(v, n); }},
+    {"--save-every", true, [](Settings& s, const char* v, const char* n) { s.save_every = number<int>(v, n); }},
+    {"--reproject", false, [](Settings& s, const char*, const char*) { s.reproject = true; }},
+    {"--no-cache-near", false, [](Settings& s, const char*, const char*) { s.trace_near_every_pass = true; }},
+    {"--exact-range", false, [](Settings& s, const char*, const char*) { s.exact_range = true; }},
+    {"--no-accel", false, [](Settings& s, const char*, const char*) { s.plain = true; }},
+    {"--bf16-weights", false, [](Settings& s, const char*, const char*) { s.bf16 = true; }},
+    {"--cache", true,
+     [](Settings& s, const char* v, const char*) {
+         static const std::pair<const char*, int> modes[] = {{"none", PRC_CACHE_NONE},
+                                                             {"near", PRC_CACHE_NEAR},
+                                                             {"full", PRC_CACHE_FULL},
+                                                             {"source", PRC_CACHE_SOURCE_MAJOR}};
+         s.cache = -1;  // an unknown mode fails the parameter check below
+         for (const auto& m : modes)
+             if (!strcmp(v, m.first)) s.cache = m.second;
+     }},
+};
+
+// Default output file of each mode (prc.cu:553-554).
+const char* default_output(const std::string& mode) {
+    return mode == "forward" ? "ACTIVITY_FWD.raw" : mode == "adjoint" ? "ACTIVITY_ADJ.raw" : "ACTIVITY_PRC_V2.raw";
+}
+
+Settings parse(int argc, char** argv) {
+    Settings s;
+    if (argc < 8) {  // the seven positional arguments are required
         print_usage(argv[0]);
         die();
     }
-    o.isotope = argv[1];
-    o.nx = parse_int(argv[2], "NX"), o.ny = parse_int(argv[3], "NY"), o.nz = parse_int(argv[4], "NZ");
-    o.dx = parse_float(argv[5], "DX"), o.dy = parse_float(argv[6], "DY"), o.dz = parse_float(argv[7], "DZ");
+    s.isotope = argv[1];
+    static const char* const dim_names[3] = {"NX", "NY", "NZ"}, *const voxel_names[3] = {"DX", "DY", "DZ"};
+    for (int a = 0; a < 3; ++a) s.dims[a] = number<int>(argv[2 + a], dim_names[a]);
+    for (int a = 0; a < 3; ++a) s.voxel[a] = number<float>(argv[5 + a], voxel_names[a]);
     for (int i = 8; i < argc; ++i) {
-        const std::string key = argv[i];
-        auto value = [&]() -> const char* {
-            if (i + 1 >= argc) {
-                fprintf(stderr, "Missing value for %s\n", key.c_str());
-                die();
-            }
-            return argv[++i];
-        };
-        if (key == "--mode") o.mode = value();
-        else if (key == "--input") o.input = value();
-        else if (key == "--density") o.density = value();
-        else if (key == "--output") o.output = value();
-        else if (key == "--rays") o.rays = parse_int(value(), key.c_str());
-        else if (key == "--iterations") o.iterations = parse_int(value(), key.c_str());
-        else if (key == "--beta") o.beta = parse_float(value(), key.c_str());
-        else if (key == "--gamma") o.gamma = parse_float(value(), key.c_str());
-        else if (key == "--support-rho") o.support_rho = parse_float(value(), key.c_str());
-        else if (key == "--air-cap-mm") o.air_cap_mm = parse_float(value(), key.c_str());
-        else if (key == "--save-every") o.save_every = parse_int(value(), key.c_str());
-        else if (key == "--reproject") o.reproject = true;
-        else if (key == "--no-cache-near") o.cache_near = false;
-        else if (key == "--cache") {
-            const std::string m = value();
-            o.cache = m == "none"     ? PRC_CACHE_NONE
-                      : m == "near"   ? PRC_CACHE_NEAR
-                      : m == "full"   ? PRC_CACHE_FULL
-                      : m == "source" ? PRC_CACHE_SOURCE_MAJOR
-                                      : -1;
-        }
-        else if (key == "--exact-range") o.exact_range = true;
-        else if (key == "--no-accel") o.accelerate = false;
-        else if (key == "--bf16-weights") o.bf16 = true;
-        else {
-            fprintf(stderr, "Unknown option %s\n", key.c_str());
+        const char* key = argv[i];
+        const Spec* spec = nullptr;
+        for (const Spec& candidate : kSpecs)
+            if (!strcmp(key, candidate.name)) spec = &candidate;
+        if (!spec) {
+            fprintf(stderr, "Unknown option %s\n", key);
             print_usage(argv[0]);
             die();
         }
+        const char* value = nullptr;
+        if (spec->takes_value) {
+            if (i + 1 == argc) {
+                fprintf(stderr, "Missing value for %s\n", key);
+                die();
+            }
+            value = argv[++i];
+        }
+        spec->apply(s, value, key);
     }
-    if (o.nx <= 0 || o.ny <= 0 || o.nz <= 0 || o.dx <= 0 || o.dy <= 0 || o.dz <= 0 || o.rays < 2 || (o.rays & 1) ||
-        o.rays > INT_MAX - 31 || o.iterations < 0 || o.iterations == INT_MAX || o.beta < 0 || o.gamma < 0 ||
-        o.support_rho < 0 || o.air_cap_mm <= 0 || o.save_every < 0 || o.cache < 0 ||
-        (o.mode != "correct" && o.mode != "forward" && o.mode != "adjoint")) {
+    // Every parameter in its range (the reference's conditions, prc.cu:540-546), then the
+    // 32-bit voxel index limit on the exact 64-bit product (prc.cu:547-551).
+    const bool in_range[] = {
+        s.dims[0] > 0 && s.dims[1] > 0 && s.dims[2] > 0,
+        s.voxel[0] > 0 && s.voxel[1] > 0 && s.voxel[2] > 0,
+        s.rays >= 2 && s.rays % 2 == 0 && s.rays <= INT_MAX - 31,
+        s.iterations >= 0 && s.iterations < INT_MAX,
+        s.beta >= 0 && s.gamma >= 0 && s.support_rho >= 0 && s.air_cap_mm > 0,
+        s.save_every >= 0 && s.cache >= 0,
+        s.mode == "correct" || s.mode == "forward" || s.mode == "adjoint",
+    };
+    if (!std::all_of(std::begin(in_range), std::end(in_range), [](bool b) { return b; })) {
         fprintf(stderr, "Invalid geometry or solver parameters\n");
         die();
     }
-    if (o.nx > INT_MAX / o.ny || o.nx * o.ny > INT_MAX / o.nz) {
+    if ((long long)s.dims[0] * s.dims[1] * s.dims[2] > INT_MAX) {
         fprintf(stderr, "Volume exceeds the INT_MAX voxel index limit\n");
         die();
     }
-    if (o.output.empty())
-        o.output = o.mode == "correct" ? "ACTIVITY_PRC_V2.raw" : o.mode == "forward" ? "ACTIVITY_FWD.raw" : "ACTIVITY_ADJ.raw";
-    return o;
+    if (s.output.empty()) s.output = default_output(s.mode);
+    return s;
 }
 
-// "_it003" / "_REPROJ" go before the extension of the file name, never into a dotted
-// directory (prc.cu:557-562).
-std::string with_suffix(const std::string& path, const std::string& suffix) {
-    const size_t dot = path.rfind('.');
-    const size_t slash = path.find_last_of("/\\");
-    const size_t start = slash == std::string::npos ? 0 : slash + 1;
-    return dot == std::string::npos || dot <= start ? path + suffix : path.substr(0, dot) + suffix + path.substr(dot);
+// Checkpoint and reprojection names: the tag goes before the extension of the file name
+// ("out.raw" -> "out_it003.raw"), or at the end when the file name has none or starts with its
+// only dot; a dot in a directory name is never an extension (prc.cu:557-562).
+std::string with_suffix(const std::string& path, const std::string& tag) {
+    const size_t sep = path.find_last_of("/\\");
+    const size_t name = sep == std::string::npos ? 0 : sep + 1;
+    const size_t ext = path.find_last_of('.');
+    if (ext == std::string::npos || ext <= name) return path + tag;
+    std::string out = path;
+    return out.insert(ext, tag);
 }
 
 // Reads exactly v->size() floats; false when the file is missing, short or too long.
@@ -233,13 +271,14 @@ int main(int argc, char** argv) {
         print_usage(argv[0], stdout);
         return EXIT_SUCCESS;
     }
-    const Options o = parse(argc, argv);
+    const Settings o = parse(argc, argv);
     float cutoff = 0.0f;
     if (prc_isotope_cutoff(o.isotope.c_str(), &cutoff) != PRC_OK) {
         print_usage(argv[0]);
         return EXIT_FAILURE;
     }
-    const size_t n = (size_t)o.nx * o.ny * o.nz;
+    const int nx = o.dims[0], ny = o.dims[1], nz = o.dims[2];
+    const size_t n = (size_t)nx * ny * nz;
 
     const double t0 = now_s();
     std::vector<float> rho(n), img(n);
@@ -267,7 +306,7 @@ int main(int argc, char** argv) {
         }
     }
     printf("isotope %s, grid %dx%dx%d, voxel %.3fx%.3fx%.3f mm, cutoff %.3f mm (water), air cap %.1f mm\n",
-           o.isotope.c_str(), o.nx, o.ny, o.nz, o.dx, o.dy, o.dz, cutoff, o.air_cap_mm);
+           o.isotope.c_str(), nx, ny, nz, o.voxel[0], o.voxel[1], o.voxel[2], cutoff, o.air_cap_mm);
     printf("tissue voxels %zu (%.1f%%), input counts in tissue %.6g of %.6g (%.2f%%)\n", n_active,
            100.0 * n_active / n, support_sum, input_sum, input_sum > 0 ? 100.0 * support_sum / input_sum : 0.0);
     if (support_sum == 0.0) {
@@ -276,14 +315,14 @@ int main(int argc, char** argv) {
     }
 
     // First CUDA contact.
-    prc_geometry geo{o.nx, o.ny, o.nz, o.dx, o.dy, o.dz};
+    prc_geometry geo{nx, ny, nz, o.voxel[0], o.voxel[1], o.voxel[2]};
     prc_options opts;
     prc_default_options(&opts);
     opts.rays = o.rays;
     opts.support_rho = o.support_rho;
     opts.air_cap_mm = o.air_cap_mm;
     opts.exact_range = o.exact_range;
-    opts.cache = o.cache_near ? o.cache : PRC_CACHE_NONE;
+    opts.cache = o.trace_near_every_pass ? PRC_CACHE_NONE : o.cache;
     opts.precision = o.bf16 ? PRC_PRECISION_BF16 : PRC_PRECISION_FP32;
     double t = now_s();
     prc_handle* h = nullptr;
@@ -313,13 +352,13 @@ int main(int argc, char** argv) {
     printf("MAP-EM: %d iterations, beta %.4g, gamma %.3g\n", o.iterations, o.beta, o.gamma);
     t = now_s();
     if (o.iterations == 0) {
-        check(prc_em_run_host(h, img.data(), out.data(), 0, o.beta, o.gamma, o.accelerate));
+        check(prc_em_run_host(h, img.data(), out.data(), 0, o.beta, o.gamma, !o.plain));
     } else {
         check(prc_em_begin_host(h, img.data()));
         t = now_s();
         CheckpointWriter writer;
         for (int it = 1; it <= o.iterations; ++it) {
-            check(prc_em_iterate(h, 1, o.beta, o.gamma, o.accelerate, nullptr));
+            check(prc_em_iterate(h, 1, o.beta, o.gamma, !o.plain, nullptr));
             if (it == 1 || it % 10 == 0 || it == o.iterations) {
                 check(prc_synchronize(h));
                 printf("iteration %d/%d: %.2f s\n", it, o.iterations, now_s() - t);

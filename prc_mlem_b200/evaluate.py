@@ -22,6 +22,7 @@ from __future__ import annotations
 import argparse
 import ctypes
 import json
+import math
 from pathlib import Path
 
 import numpy as np
@@ -37,99 +38,118 @@ SSIM_WINDOW = 11
 
 
 def load(path, shape):
-    """A headerless float32 volume of the given (NZ, NY, NX) shape (tools/evaluate.py:23-33)."""
-    if len(shape) != 3 or any(s <= 0 for s in shape):
+    """A headerless little-endian float32 volume of shape (NZ, NY, NX); the file must hold
+    exactly that many values (the loader contract of tools/evaluate.py:23-33)."""
+    dims = tuple(int(d) for d in shape)
+    if len(dims) != 3 or min(dims) <= 0:
         raise ValueError("shape must contain three positive dimensions (NZ NY NX)")
-    expected_bytes = int(np.prod(shape)) * np.dtype(np.float32).itemsize
-    actual_bytes = Path(path).stat().st_size
-    if actual_bytes != expected_bytes:
-        raise ValueError(f"{path}: expected {expected_bytes} bytes, got {actual_bytes}")
-    values = np.fromfile(path, dtype=np.float32)
-    if values.size != int(np.prod(shape)):
-        raise ValueError(f"{path}: expected {int(np.prod(shape))} float32 values, got {values.size}")
-    return values.reshape(shape)
+    want = 4 * math.prod(dims)
+    raw = Path(path).read_bytes()
+    if len(raw) != want:
+        raise ValueError(f"{path}: expected {want} bytes, got {len(raw)}")
+    return np.frombuffer(raw, dtype="<f4").reshape(dims).astype(np.float32)
 
 
 def _ratio_sqrt(num, den):
     return float(np.sqrt(num / den)) if den > 0 else None
 
 
+def _finite_volume_like(a, shape, what):
+    """`a` as an array of `shape` with only finite values, else ValueError."""
+    a = np.asarray(a)
+    if a.shape != shape or not np.isfinite(a).all():
+        raise ValueError(f"{what} must be finite and have the truth shape")
+    return a
+
+
+def _bounding_box(mask):
+    """Slices of the smallest box holding every set voxel of a non-empty 3D mask."""
+    box = []
+    for axis in range(3):
+        hit = np.flatnonzero(mask.any(axis=tuple(a for a in range(3) if a != axis)))
+        box.append(slice(int(hit[0]), int(hit[-1]) + 1))
+    return tuple(box)
+
+
+def _class_volume(truth, body, hot, bg):
+    """The per-voxel class byte of the scorer's regions, built in one pass over the masks of
+    tools/evaluate.py:93-103 (their definitions are the metrics' meaning):
+      body        tissue (the mask, or truth > 0);
+      hot         the high-uptake regions;
+      background  background-level tissue (|t - bg| < 1e-6 bg) eroded 4 times by a 3x3x3 cube;
+      edge        voxels whose 5x5x5 neighbourhood of the truth is not constant;
+      halo        background tissue 2-3 voxels outside a hot region and 4 voxels inside the skin;
+      roi         the bounding box of the body dilated 4 times (PSNR and SSIM are taken there).
+    Returns (classes uint8, 5x5x5 minimum, 5x5x5 maximum, roi slices)."""
+    level = (np.abs(truth.astype(np.float64) - bg) < 1e-6 * bg) & body
+    lo = ndi.minimum_filter(truth, size=5, mode="nearest").astype(np.float64)
+    hi = ndi.maximum_filter(truth, size=5, mode="nearest").astype(np.float64)
+    near_hot = ndi.binary_dilation(hot)  # 1 step; the halo's outer limit grows it 2 steps more
+    shell = ndi.binary_dilation(near_hot, iterations=2) & ~near_hot
+    classes = np.zeros(truth.shape, np.uint8)
+    for bit, region in ((CLASS_BODY, body), (CLASS_HOT, hot),
+                        (CLASS_BACKGROUND, ndi.binary_erosion(level, structure=np.ones((3, 3, 3)), iterations=4)),
+                        (CLASS_EDGE, hi > lo),
+                        (CLASS_HALO, shell & level & ndi.binary_erosion(body, iterations=4))):
+        classes[region] |= bit
+    roi = _bounding_box(ndi.binary_dilation(body, iterations=4))
+    classes[roi] |= CLASS_ROI
+    return classes, lo, hi, roi
+
+
 class Evaluator:
-    """Scores reconstructions against one truth (tools/evaluate.py:47-154)."""
+    """Scores reconstructions against one truth (the Evaluator of tools/evaluate.py:47-154:
+    same arguments, same checks and messages, same metric dictionary)."""
 
     def __init__(self, truth, mask=None, data_range=None, background=None, hot_mask=None):
         truth = np.asarray(truth)
-        if truth.ndim != 3 or not np.all(np.isfinite(truth)) or np.any(truth < 0):
+        if truth.ndim != 3 or not np.isfinite(truth).all() or (truth < 0).any():
             raise ValueError("truth must be a finite, nonnegative 3D activity volume")
-        if not np.any(truth > 0):
+        if not (truth > 0).any():
             raise ValueError("truth must contain positive activity")
-        t = truth.astype(np.float64)
-        if mask is None:
-            body = truth > 0
-        else:
-            mask = np.asarray(mask)
-            if mask.shape != truth.shape or not np.all(np.isfinite(mask)):
-                raise ValueError("mask must be finite and have the truth shape")
-            body = mask > 0
-            if not np.any(body):
+        shape = truth.shape
+        body = truth > 0
+        if mask is not None:
+            body = _finite_volume_like(mask, shape, "mask") > 0
+            if not body.any():
                 raise ValueError("mask must contain tissue voxels")
-        self.body = body
-        self.data_range = float(truth.max() if data_range is None else data_range)
-        if not np.isfinite(self.data_range) or self.data_range <= 0:
+        rng = float(truth.max()) if data_range is None else float(data_range)
+        if not (np.isfinite(rng) and rng > 0):
             raise ValueError("data_range must be finite and positive")
-        if background is None:
+        if background is None:  # the most frequent positive tissue value (the smallest on a tie)
             values, counts = np.unique(truth[body & (truth > 0)], return_counts=True)
-            if not values.size:
+            if values.size == 0:
                 raise ValueError("mask must include positive truth activity, or supply background")
-            background = values[np.argmax(counts)]
-        self.bg = float(background)
-        if not np.isfinite(self.bg) or self.bg <= 0:
+            background = values[counts == counts.max()][0]
+        bg = float(background)
+        if not (np.isfinite(bg) and bg > 0):
             raise ValueError("background must be finite and positive")
         if hot_mask is None:
-            hot = (truth > 1.5 * self.bg) & body
+            hot = (truth > 1.5 * bg) & body
             hot_definition = "truth > 1.5 * background (high-uptake regions; not necessarily lesions)"
         else:
-            hot_mask = np.asarray(hot_mask)
-            if hot_mask.shape != truth.shape or not np.all(np.isfinite(hot_mask)):
-                raise ValueError("hot_mask must be finite and have the truth shape")
-            hot = hot_mask > 0
-            if np.any(hot & (~body | (truth <= 0))):
+            hot = _finite_volume_like(hot_mask, shape, "hot_mask") > 0
+            if (hot & ~(body & (truth > 0))).any():
                 raise ValueError("hot_mask must lie inside tissue with positive truth activity")
             hot_definition = "explicit hot mask; connected positive components define lesions"
-        self.hot = hot
-        self.hot_labels, self.n_hot = ndi.label(hot)
+        labels, n_hot = ndi.label(hot)
+        self.body, self.hot, self.hot_labels, self.n_hot = body, hot, labels, n_hot
+        self.data_range, self.bg, self.shape = rng, bg, shape
         self.metric_settings = {
-            "data_range": self.data_range, "background": self.bg,
-            "tissue_mask": "explicit mask" if mask is not None else "truth > 0",
-            "hot_regions": hot_definition, "hot_region_count": int(self.n_hot),
-            "hot_region_voxels": int(hot.sum()),
+            "data_range": rng, "background": bg,
+            "tissue_mask": "truth > 0" if mask is None else "explicit mask",
+            "hot_regions": hot_definition, "hot_region_count": int(n_hot),
+            "hot_region_voxels": int(np.count_nonzero(hot)),
             "ssim_window": "3D Gaussian sigma 1.5, 11 voxels",
         }
-        self.roi = ndi.find_objects(ndi.binary_dilation(body, iterations=4), max_label=1)[0]
-        is_background = (np.abs(t - self.bg) < 1e-6 * self.bg) & body
-        bg_interior = ndi.binary_erosion(is_background, structure=np.ones((3, 3, 3)), iterations=4)
-        lo = ndi.minimum_filter(truth, size=5, mode="nearest").astype(np.float64)
-        hi = ndi.maximum_filter(truth, size=5, mode="nearest").astype(np.float64)
-        edge_band = hi > lo
-        hot_shell = ndi.binary_dilation(hot, iterations=3) & ~ndi.binary_dilation(hot, iterations=1)
-        skin_core = ndi.binary_erosion(body, iterations=4)
-        halo_shell = hot_shell & skin_core & is_background
-        self.t, self.lo, self.hi = t, lo, hi
-        self.bg_interior, self.edge_band, self.halo_shell = bg_interior, edge_band, halo_shell
-        classes = (body * CLASS_BODY | hot * CLASS_HOT | bg_interior * CLASS_BACKGROUND | edge_band * CLASS_EDGE
-                   | halo_shell * CLASS_HALO).astype(np.uint8)
-        classes[self.roi] |= CLASS_ROI
-        self.shape = truth.shape
-        self._box = tuple(s.stop - s.start for s in self.roi)
-        roi = np.array([self.roi[0].start, self.roi[0].stop, self.roi[1].start, self.roi[1].stop,
-                        self.roi[2].start, self.roi[2].stop], dtype=np.int32)
-        labels = np.ascontiguousarray(self.hot_labels, dtype=np.int32)
-        t = np.ascontiguousarray(t)
+        classes, lo, hi, self.roi = _class_volume(truth, body, hot, bg)
+        self._box = tuple(r.stop - r.start for r in self.roi)
+        corners = np.array([[r.start, r.stop] for r in self.roi], dtype=np.int32).ravel()
+        t = np.ascontiguousarray(truth, dtype=np.float64)
+        lab = np.ascontiguousarray(labels, dtype=np.int32)
         handle = ctypes.c_void_p()
-        nz, ny, nx = truth.shape
-        rc = lib().prc_eval_create(nz, ny, nx, t.ctypes.data, classes.ctypes.data,
-                                   labels.ctypes.data if self.n_hot else None, int(self.n_hot),
-                                   lo.ctypes.data, hi.ctypes.data, roi.ctypes.data, self.data_range,
+        rc = lib().prc_eval_create(*shape, t.ctypes.data, classes.ctypes.data, lab.ctypes.data if n_hot else None,
+                                   int(n_hot), lo.ctypes.data, hi.ctypes.data, corners.ctypes.data, rng,
                                    ctypes.byref(handle))
         if rc != 0:
             raise PrcError(rc, lib().prc_last_error().decode())
@@ -216,40 +236,45 @@ COLUMNS = ["nrmse", "ssim", "ssim_tissue", "ssim_edge", "edge_nrmse", "rc_hot", 
 
 
 def format_table(rows):
-    """Markdown table of the COLUMNS of each (name, metrics) row (tools/evaluate.py:160-171)."""
-    head = "| image | " + " | ".join(COLUMNS) + " |"
-    sep = "|---|" + "---:|" * len(COLUMNS)
-    lines = [head, sep]
-    for name, m in rows:
-        cells = ["—" if m.get(c) is None else f"{m.get(c):.4f}" for c in COLUMNS]
-        lines.append(f"| {name} | " + " | ".join(cells) + " |")
-    return "\n".join(lines)
+    """Markdown table: one row per (name, metrics), the COLUMNS to 4 decimals, a dash where a
+    score is unavailable (the table of tools/evaluate.py:160-171)."""
+    def cell(v):
+        return "—" if v is None else f"{v:.4f}"
+    table = [f"| image | {' | '.join(COLUMNS)} |", "|---|" + "---:|" * len(COLUMNS)]
+    table += [f"| {name} | {' | '.join(cell(m.get(c)) for c in COLUMNS)} |" for name, m in rows]
+    return "\n".join(table)
+
+
+# the command line of tools/evaluate.py:174-197: flag, options
+_FLAGS = (("--truth", dict(required=True)),
+          ("--shape", dict(type=int, nargs=3, required=True, metavar=("NZ", "NY", "NX"))),
+          ("--json", dict(help="write metrics to this JSON file")),
+          ("--mask", dict(help="float32 tissue mask (positive = tissue), including cold regions")),
+          ("--hot-mask", dict(help="float32 true hot-lesion mask (positive = lesion); recommended for smooth uptake")),
+          ("--data-range", dict(type=float, help="fixed reference intensity range for SSIM/PSNR")),
+          ("--background", dict(type=float, help="known background level for phantom metrics")),
+          ("images", dict(nargs="+", help="name=path.raw")))
 
 
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
-    ap.add_argument("--truth", required=True)
-    ap.add_argument("--shape", type=int, nargs=3, required=True, metavar=("NZ", "NY", "NX"))
-    ap.add_argument("--json", help="write metrics to this JSON file")
-    ap.add_argument("--mask", help="float32 tissue mask (positive = tissue), including cold regions")
-    ap.add_argument("--hot-mask", help="float32 true hot-lesion mask (positive = lesion); recommended for smooth uptake")
-    ap.add_argument("--data-range", type=float, help="fixed reference intensity range for SSIM/PSNR")
-    ap.add_argument("--background", type=float, help="known background level for phantom metrics")
-    ap.add_argument("images", nargs="+", help="name=path.raw")
-    args = ap.parse_args(argv)
-    ev = Evaluator(load(args.truth, args.shape),
-                   mask=load(args.mask, args.shape) if args.mask else None,
-                   data_range=args.data_range, background=args.background,
-                   hot_mask=load(args.hot_mask, args.shape) if args.hot_mask else None)
-    rows = []
-    for item in args.images:
-        name, path = item.rsplit("=", 1)
-        rows.append((name, ev(load(path, args.shape))))
-    print(format_table(rows))
+    for flag, kw in _FLAGS:
+        ap.add_argument(flag, **kw)
+    a = ap.parse_args(argv)
+
+    def optional(path):
+        return None if not path else load(path, a.shape)
+
+    ev = Evaluator(load(a.truth, a.shape), mask=optional(a.mask), data_range=a.data_range,
+                   background=a.background, hot_mask=optional(a.hot_mask))
+    scored = {}
+    for item in a.images:
+        name, _, path = item.rpartition("=")
+        scored[name] = ev(load(path, a.shape))
+    print(format_table(scored.items()))
     print("Hot-region definition: " + ev.metric_settings["hot_regions"])
-    if args.json:
-        with open(args.json, "w") as fh:
-            json.dump({name: m for name, m in rows}, fh, indent=2, allow_nan=False)
+    if a.json:
+        Path(a.json).write_text(json.dumps(scored, indent=2, allow_nan=False))
 
 
 if __name__ == "__main__":

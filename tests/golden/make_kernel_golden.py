@@ -1,8 +1,9 @@
 """Generates tests/golden/water_kernel.npz and range_model.npz from the reference's own
 FP64 range-model quadrature, tests/reference.py of jlherraiz/PRC_MLEM.
 
-Run in a checkout where the reference is readable:
-    python tests/golden/make_kernel_golden.py /root/reference
+Run where the reference checkout is readable, giving its directory as the argument or in
+PRC_REFERENCE_DIR:
+    python tests/golden/make_kernel_golden.py path/to/PRC_MLEM
 It imports the reference module (read-only), evaluates
   * reference.kernel(68Ga, voxel, half) for 4 mm and 2 mm voxels -- the homogeneous water
     kernel the reference's GPU test compares against (tests/test_solver.py:216-243);
@@ -10,6 +11,7 @@ It imports the reference module (read-only), evaluates
     (tests/test_rdp.py:18-24);
 and writes the arrays.  The fixtures travel with the repository; the reference does not.
 """
+import os
 import sys
 from pathlib import Path
 
@@ -43,4 +45,7 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    ref_dir = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("PRC_REFERENCE_DIR")
+    if not ref_dir:
+        raise SystemExit("give the reference checkout as the argument or in PRC_REFERENCE_DIR")
+    main(ref_dir)

@@ -1,12 +1,14 @@
 """Golden metric values from the reference's own scorer, tools/evaluate.py.
 
-Run in a checkout that holds the reference:  python tests/golden/make_metrics_golden.py
+Run with the reference checkout as the argument or in PRC_REFERENCE_DIR:
+    python tests/golden/make_metrics_golden.py path/to/PRC_MLEM
 It imports the reference's Evaluator with scikit-image replaced by a stand-in SSIM (the
 oracle's restatement; scikit-image is not installed here), runs every case of
 metrics_cases.py and writes tests/golden/metrics_golden.json.  The non-SSIM metrics pin the
 oracle to the reference's code; the SSIM entries only record the stand-in.
 """
 import json
+import os
 import sys
 import types
 from pathlib import Path
@@ -33,7 +35,10 @@ def main():
     metrics.structural_similarity = structural_similarity
     skimage.metrics = metrics
     sys.modules["skimage"], sys.modules["skimage.metrics"] = skimage, metrics
-    sys.path.insert(0, "/root/reference/tools")
+    ref_dir = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("PRC_REFERENCE_DIR")
+    if not ref_dir:
+        raise SystemExit("give the reference checkout as the argument or in PRC_REFERENCE_DIR")
+    sys.path.insert(0, str(Path(ref_dir) / "tools"))
     import evaluate as ref  # the reference's tools/evaluate.py
     golden = {}
     for name, truth, kw, candidates in metrics_cases.cases():

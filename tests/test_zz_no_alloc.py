@@ -1,10 +1,12 @@
 """prc_sum_static: the FP64 volume sum for callers that cannot allocate device memory where
 they need it (services that reserve all GPU memory at start-up, hot paths that must not pay
 cudaMalloc's synchronisation, operators inside another framework's allocator).  It keeps its
-scratch in a static device array, so this test checks, through the C ABI, that two calls in a
-row agree with the handle-based prc_sum on the same data, that the size limit is enforced, and
-that an empty input gives zero.  This file is collected last, so a run that stops at the first
-failure has already run every other test."""
+scratch in a static device array, so this test checks, through the C ABI, that the calls after
+the first one on a device leave free device memory unchanged (the first may load the array's
+module under CUDA's lazy loading), that two calls in a row agree with the handle-based prc_sum
+on the same data, that the size limit is enforced, and that an empty input gives zero.  This
+file is collected last, so a run that stops at the first failure has already run every other
+test."""
 import ctypes
 
 import numpy as np
@@ -23,6 +25,29 @@ def static_sum(d_x, n=None):
     assert rc == pm.PRC_OK, pm.lib().prc_last_error().decode()
     torch.cuda.synchronize()
     return float(out.item())
+
+
+def test_calls_after_the_first_allocate_no_device_memory(record_property):
+    x = torch.rand(1 << 20, dtype=torch.float32, device="cuda")
+    out = torch.zeros(4, dtype=torch.float64, device="cuda")  # every buffer exists before measuring
+    expect = x.double().sum().item()
+    torch.cuda.synchronize()
+
+    def call():
+        rc = pm.lib().prc_sum_static(x.data_ptr(), x.numel(), out.data_ptr(), None)
+        assert rc == pm.PRC_OK, pm.lib().prc_last_error().decode()
+        torch.cuda.synchronize()
+
+    free0, _ = torch.cuda.mem_get_info()
+    call()  # warm-up: under lazy module loading this is what loads the static array
+    free1, _ = torch.cuda.mem_get_info()
+    record_property("first_call_device_bytes", free0 - free1)
+    assert free0 - free1 <= 16 << 20  # at most the module image, never a volume-sized buffer
+    for _ in range(8):
+        call()
+    free2, _ = torch.cuda.mem_get_info()
+    assert free2 == free1, f"later calls changed free device memory by {free1 - free2} bytes"
+    assert abs(out[0].item() - expect) <= 1e-9 * expect
 
 
 def test_two_calls_in_a_row_match_prc_sum():
