@@ -350,6 +350,7 @@ def run_ours(args):
     if single and not args.no_parity:
         parity, ref_job = parity_vs_prc_cu(P, rho, spacing, g_host, corrected, images or {}, args.iterations)
         tti = time_to_image(rho, spacing, g_host, args, ref_job)
+        tti["command_line"] = cli_vs_prc_cu(rho, spacing, g_host, args.iterations)
     batch = None
     if single and not args.no_batch:
         batch = batch_record(frames=8, iterations=10, steps=2, warmup=1)
@@ -511,6 +512,48 @@ def parity_vs_prc_cu(P, rho, spacing, g, corrected, images, iterations):
     job = {"setup_s": em["setup_s"], "iterations_s": em["iterations_s"], "total_s": em["total_s"],
            "process_wall_s": round(em["wall_s"], 3)}
     return out, job
+
+
+def cli_vs_prc_cu(rho, spacing, g, iterations):
+    """The drop-in command line end to end on the headline data: this engine's `prc` executable
+    and the reference executable with the same arguments (--mode correct, 128 rays, beta 0.03,
+    gamma 20, support density 0.05, acceleration on), each a fresh process that reads the raw
+    files, creates its CUDA context, builds the projector, iterates and writes the image.
+    Reports each process's wall time and the total it prints (prc.cu:719-720), and the relative
+    L2 distance of the two output images."""
+    import tempfile
+    from oracle import ref_exe
+    import prc_mlem_b200 as pm
+    if not (ref_exe.available() and pm.CLI_PATH.is_file()):
+        return {"unavailable": "the reference executable or the prc command line was not built"}
+    nz, ny, nx = rho.shape
+    out = {}
+    with tempfile.TemporaryDirectory(prefix="prc_cli_bench_") as d:
+        d = Path(d)
+        np.ascontiguousarray(rho, np.float32).tofile(d / "rho.raw")
+        np.ascontiguousarray(g, np.float32).tofile(d / "g.raw")
+        images = {}
+        for name, exe in (("prc_cli", pm.CLI_PATH), ("prc_cu", ref_exe.EXE)):
+            cmd = [str(exe), ISOTOPE, str(nx), str(ny), str(nz), *(repr(float(s)) for s in spacing), "--input",
+                   str(d / "g.raw"), "--density", str(d / "rho.raw"), "--output", str(d / f"{name}.raw"), "--rays",
+                   str(RAYS), "--iterations", str(iterations), "--beta", str(BETA), "--gamma", str(GAMMA),
+                   "--support-rho", str(SUPPORT_RHO)]
+            walls = []
+            for _ in range(2):  # the second run sees warm file caches
+                t0 = time.perf_counter()
+                r = subprocess.run(cmd, capture_output=True, text=True, timeout=900)
+                walls.append(time.perf_counter() - t0)
+                if r.returncode != 0:
+                    return {"unavailable": f"{name} failed: {r.stderr.strip()[:200]}"}
+            import re
+            total = re.search(r"total ([0-9.]+) s", r.stdout)
+            norm = re.search(r"normalisation [^:]*: ([0-9.]+) s", r.stdout)
+            out[name] = {"process_wall_s": round(min(walls), 3), "printed_total_s": float(total.group(1)) if total else None,
+                         "printed_setup_s": float(norm.group(1)) if norm else None}
+            images[name] = np.fromfile(d / f"{name}.raw", np.float32)
+        out["speedup_process_wall"] = round(out["prc_cu"]["process_wall_s"] / out["prc_cli"]["process_wall_s"], 2)
+        out["output_rel_l2"] = rel_l2(images["prc_cli"], images["prc_cu"])
+    return out
 
 
 def time_to_image(rho, spacing, g, args, ref_job):

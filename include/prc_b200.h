@@ -55,6 +55,21 @@ enum {
                                   the forward projection scatters with atomics */
 };
 
+/* Source tiles of the stored coefficient field: a warp owns 32 tissue voxels taken in tiles
+ * of this shape (x fastest inside a tile, tiles in x, y, z order), so every gather of one step
+ * touches the rows of one tile shifted by the step's offset.  PRC_TILE_AUTO lets the engine
+ * choose (an autotuner that times the candidate shapes on the handle's own field, remembered
+ * per grid, isotope and form for the rest of the process).  The shape changes no result:
+ * every source keeps its own weights and summation order. */
+enum {
+    PRC_TILE_AUTO = 0,
+    PRC_TILE_8x2x2 = 1,
+    PRC_TILE_16x2x1 = 2,
+    PRC_TILE_32x1x1 = 3,
+    PRC_TILE_4x4x2 = 4,
+    PRC_TILE_16x1x2 = 5
+};
+
 /* Volume geometry: positional arguments NX NY NZ DX DY DZ of prc.cu:515-516. */
 typedef struct prc_geometry {
     int nx, ny, nz;
@@ -62,7 +77,7 @@ typedef struct prc_geometry {
 } prc_geometry;
 
 /* Projector options: --rays, --support-rho, --air-cap-mm, --exact-range, --no-cache-near of
- * prc.cu:452-459, plus the cache mode and the stored-weight precision. */
+ * prc.cu:452-459, plus the cache mode, the stored-weight precision and the source tile. */
 typedef struct prc_options {
     int rays;          /* even far-field rays per source, >= 2 (default 128) */
     float support_rho; /* voxels with density >= support_rho hold activity (default 0.05) */
@@ -70,6 +85,7 @@ typedef struct prc_options {
     int exact_range;   /* 1: analytic survival instead of the 4097-entry table */
     int cache;         /* PRC_CACHE_* (default PRC_CACHE_FULL) */
     int precision;     /* PRC_PRECISION_* */
+    int tile;          /* PRC_TILE_* source tile of the stored field (default PRC_TILE_AUTO) */
 } prc_options;
 
 typedef struct prc_handle prc_handle;
@@ -222,6 +238,9 @@ int prc_batch_warps(const prc_batch* b);
 int prc_timing(prc_handle* h, int enable);
 int prc_timing_read(prc_handle* h, double* forward_ms, int64_t* n_forward, double* adjoint_ms, int64_t* n_adjoint);
 
+/* The source tile (PRC_TILE_*) the handle's stored field uses, after any automatic choice. */
+int prc_tile(const prc_handle* h, int* tile);
+
 /* Number of kernels the handle's entry points have enqueued since it was created (projections,
  * MAP-EM image updates and reductions; copies and memsets are not counted).  No counterpart in
  * the reference. */
@@ -236,6 +255,12 @@ int prc_synchronize(prc_handle* h);
  * gives up, raises the handle's error flag and returns, so this returns PRC_ERR_CUDA with the
  * bounded-wait message while the CUDA context stays usable. */
 int prc_wait_selftest(prc_handle* h, int rounds);
+
+/* Page-locked host memory for image buffers (cudaMallocHost / cudaFreeHost): the host-memory
+ * entry points copy from and to it at full PCIe / C2C speed.  No counterpart in the reference,
+ * whose host buffers are pageable std::vectors (prc.cu:592, 646). */
+int prc_host_alloc(size_t bytes, void** ptr);
+void prc_host_free(void* ptr);
 
 /* Message of the most recent failure on this thread ("" if none). */
 const char* prc_last_error(void);

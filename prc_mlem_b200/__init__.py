@@ -17,7 +17,9 @@ from pathlib import Path
 import numpy as np
 
 PKG_DIR = Path(__file__).resolve().parent
-LIB_PATH = PKG_DIR / "lib" / "libprc_b200.so"
+# PRC_B200_LIB selects another build of the library (for example one compiled with other
+# tuning constants); the default is the in-tree build.
+LIB_PATH = Path(os.environ.get("PRC_B200_LIB") or PKG_DIR / "lib" / "libprc_b200.so")
 CLI_PATH = PKG_DIR / "bin" / "prc"
 HEADER_PATH = PKG_DIR.parent / "include" / "prc_b200.h"
 
@@ -28,6 +30,9 @@ PRC_CACHE_NONE = 0
 PRC_CACHE_NEAR = 1
 PRC_CACHE_FULL = 2
 PRC_CACHE_SOURCE_MAJOR = 3
+PRC_TILE_AUTO, PRC_TILE_8x2x2, PRC_TILE_16x2x1, PRC_TILE_32x1x1, PRC_TILE_4x4x2, PRC_TILE_16x1x2 = range(6)
+TILE_SHAPES = {PRC_TILE_8x2x2: (8, 2, 2), PRC_TILE_16x2x1: (16, 2, 1), PRC_TILE_32x1x1: (32, 1, 1),
+               PRC_TILE_4x4x2: (4, 4, 2), PRC_TILE_16x1x2: (16, 1, 2)}
 ISOTOPES = ("11C", "13N", "15O", "18F", "64Cu", "68Ga", "82Rb", "124I")
 
 
@@ -46,7 +51,8 @@ class Geometry(ctypes.Structure):
 
 class Options(ctypes.Structure):
     _fields_ = [("rays", ctypes.c_int), ("support_rho", ctypes.c_float), ("air_cap_mm", ctypes.c_float),
-                ("exact_range", ctypes.c_int), ("cache", ctypes.c_int), ("precision", ctypes.c_int)]
+                ("exact_range", ctypes.c_int), ("cache", ctypes.c_int), ("precision", ctypes.c_int),
+                ("tile", ctypes.c_int)]
 
 
 _P = ctypes.c_void_p
@@ -80,6 +86,7 @@ _SIGNATURES = {
     "prc_count_deposits": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int64)]),
     "prc_synchronize": (ctypes.c_int, [_P]),
     "prc_launch_count": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int64)]),
+    "prc_tile": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int)]),
     "prc_wait_selftest": (ctypes.c_int, [_P, ctypes.c_int]),
     "prc_sum_static": (ctypes.c_int, [_P, ctypes.c_int64, _P, _P]),
     "prc_create_surrogate": (ctypes.c_int, [ctypes.POINTER(Geometry), ctypes.c_char_p, ctypes.POINTER(Options), _P,
@@ -113,6 +120,8 @@ _SIGNATURES = {
     "prc_timing_read": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int64),
                                        ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int64)]),
     "prc_last_error": (ctypes.c_char_p, []),
+    "prc_host_alloc": (ctypes.c_int, [ctypes.c_size_t, ctypes.POINTER(_P)]),
+    "prc_host_free": (None, [_P]),
 }
 
 class Frame(ctypes.Structure):
@@ -179,7 +188,7 @@ class Projector:
     def __init__(self, isotope: str, density: np.ndarray, spacing, rays: int = 128, support_rho: float = 0.05,
                  air_cap_mm: float = 50.0, exact_range: bool = False, cache: int = PRC_CACHE_FULL,
                  precision: int = PRC_PRECISION_FP32, surrogate=None, target_scale: float = 1.0,
-                 fallback_nrmse: float = 0.0):
+                 fallback_nrmse: float = 0.0, tile: int = PRC_TILE_AUTO):
         """surrogate: None for the plain projector; a trained network (prc_mlem_b200.surrogate.Network)
         or the string "traced" for the radial coefficient field (prc_create_surrogate)."""
         density = _host(density)
@@ -193,6 +202,7 @@ class Projector:
         opts = default_options()
         opts.rays, opts.support_rho, opts.air_cap_mm = rays, support_rho, air_cap_mm
         opts.exact_range, opts.cache, opts.precision = int(exact_range), int(cache), int(precision)
+        opts.tile = int(tile)
         h = _P()
         self.fallbacks = 0
         if surrogate is None:
@@ -301,6 +311,13 @@ class Projector:
     def sum(self, d_x) -> float:
         v = ctypes.c_double()
         _check(lib().prc_sum(self._h, _ptr(d_x), ctypes.byref(v), None))
+        return v.value
+
+    @property
+    def tile(self) -> int:
+        """The source tile (PRC_TILE_*) of the stored field."""
+        v = ctypes.c_int()
+        _check(lib().prc_tile(self._h, ctypes.byref(v)))
         return v.value
 
     @property

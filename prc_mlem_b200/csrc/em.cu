@@ -220,6 +220,75 @@ __device__ __forceinline__ void update_body(const float* __restrict__ f, const f
         });
 }
 
+// Distance weight of neighbour offset (dx, dy, dz): min(dx, dy, dz) / |offset| with the
+// reciprocal square root of prc.cu:293-296; computed once per run for the 26 offsets.
+__global__ void geometry_weights_kernel(Grid g, float* geo_w) {
+    const int q = threadIdx.x;
+    if (q >= 27) return;
+    const int dx = q % 3 - 1, dy = q / 3 % 3 - 1, dz = q / 9 - 1;
+    const float mx = dx * g.sx, my = dy * g.sy, mz = dz * g.sz;
+    geo_w[q] = (dx | dy | dz) ? fminf(g.sx, fminf(g.sy, g.sz)) * rsqrtf(mx * mx + my * my + mz * mz) : 0.0f;
+}
+
+// The RDP update of update_body, one thread per tissue voxel: threads walk the tissue list, so
+// no lane idles on air, and the distance weights are read from geo_w (uniform across the warp)
+// instead of being recomputed per neighbour.  An interior voxel (one voxel away from every
+// face) reads its 26 neighbours at fixed linear offsets with no bounds tests; only voxels on
+// the volume's faces test each neighbour.  Per neighbour the arithmetic is update_body's, in the
+// same order, so the result is the same for every voxel.
+template <bool SUM>
+__global__ void __launch_bounds__(kEmThreads) update_active_kernel(
+    const float* __restrict__ f, const float* __restrict__ back, const unsigned char* __restrict__ support,
+    float* __restrict__ next, const int* __restrict__ active, int n_active, Grid g, const float* __restrict__ geo_w,
+    float beta, float gamma, EmScalars* sc, Reduction r) {
+    __shared__ float w_sh[27];
+    if (threadIdx.x < 27) w_sh[threadIdx.x] = geo_w[threadIdx.x];
+    __syncthreads();
+    const float eps = sc->eps;
+    const int nx = g.nx, ny = g.ny, nz = g.nz, nxy = nx * ny;
+    double v[1] = {0.0};
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < n_active; a += gridDim.x * blockDim.x) {
+        const int idx = __ldg(active + a);
+        const float fj = __ldg(f + idx), f_em = fj * __ldg(back + idx);
+        float out;
+        if (beta == 0.0f) {
+            out = fmaxf(f_em, 0.0f);
+        } else {
+            const unsigned row = (unsigned)idx / (unsigned)nx;
+            const int i = idx - (int)row * nx, j = (int)(row % (unsigned)ny), k = (int)(row / (unsigned)ny);
+            const bool interior = i > 0 && i < nx - 1 && j > 0 && j < ny - 1 && k > 0 && k < nz - 1;
+            float grad = 0.0f, curv = 0.0f;
+#pragma unroll
+            for (int q = 0; q < 27; ++q) {
+                const int dx = q % 3 - 1, dy = q / 3 % 3 - 1, dz = q / 9 - 1;
+                if (q == 13) continue;  // the voxel itself
+                if (!interior && !(i + dx >= 0 && i + dx < nx && j + dy >= 0 && j + dy < ny && k + dz >= 0 &&
+                                   k + dz < nz))
+                    continue;
+                const int nb = idx + dz * nxy + dy * nx + dx;
+                if (!__ldg(support + nb)) continue;
+                const float w = w_sh[q];
+                const float fk = __ldg(f + nb), d = fj - fk, ad = fabsf(d);
+                const float D = fj + fk + gamma * ad + eps, invD = 1.0f / D;
+                grad += w * d * (fj + 3.0f * fk + gamma * ad + 2.0f * eps) * invD * invD;
+                const float half_quad = (2.0f * (fj + fk + eps) + gamma * ad) * invD * invD;
+                const float hess = 2.0f * (2.0f * fk + eps) * (2.0f * fk + eps) * invD * invD * invD;
+                curv += 2.0f * w * fmaxf(half_quad, hess);
+            }
+            const float a2 = beta * curv, B = 1.0f + beta * (grad - curv * fj);
+            const float root = sqrtf(B * B + 4.0f * a2 * f_em);
+            out = B >= 0.0f ? (f_em > 0.0f ? 2.0f * f_em / (B + root) : 0.0f) : (root - B) / (2.0f * a2);
+        }
+        next[idx] = out;
+        if (SUM) v[0] += out;
+    }
+    if (SUM)
+        grid_reduce<1>(v, r, [&](const double* t) {
+            sc->sum = t[0];
+            sc->scale = t[0] > 0.0 ? (float)(sc->support_sum / t[0]) : 1.0f;
+        });
+}
+
 // Count rescale and, when accelerating, the step h = next - y and the two FP64 inner products
 // that give lambda = clamp(<h, h_prev> / <h_prev, h_prev>, 0, 1) (prc.cu:325-332, 693-696).
 template <bool RESIDUAL>
@@ -361,6 +430,24 @@ cudaError_t em_update(const EmVolumes& v, const Grid& grid, const float* start, 
     else
         update_kernel<false><<<kReduceBlocks, kEmThreads, 0, s>>>(start, back, v.support, next, grid, beta, gamma,
                                                                   v.scalars, v.red);
+    return cudaGetLastError();
+}
+
+cudaError_t em_geometry_weights(const Grid& grid, float* geo_w, cudaStream_t s) {
+    geometry_weights_kernel<<<1, 32, 0, s>>>(grid, geo_w);
+    return cudaGetLastError();
+}
+
+cudaError_t em_update_active(const EmVolumes& v, const Grid& grid, const int* active, int n_active,
+                             const float* geo_w, const float* start, const float* back, float* next, float beta,
+                             float gamma, cudaStream_t s) {
+    if (beta > 0.0f)
+        update_active_kernel<true><<<kReduceBlocks, kEmThreads, 0, s>>>(start, back, v.support, next, active, n_active,
+                                                                        grid, geo_w, beta, gamma, v.scalars, v.red);
+    else
+        update_active_kernel<false><<<kReduceBlocks, kEmThreads, 0, s>>>(start, back, v.support, next, active,
+                                                                         n_active, grid, geo_w, beta, gamma,
+                                                                         v.scalars, v.red);
     return cudaGetLastError();
 }
 

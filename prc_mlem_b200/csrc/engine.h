@@ -22,11 +22,17 @@ struct RayStep {
     int pad;
 };
 
-// Layout of a stored field stream (see FarField).
+// Layout of a stored field stream (see FarField).  The stream is built with every lane vector
+// in place (pack P of the stream holds 32 vectors); compaction then drops the vectors that hold
+// only zeros: pack P keeps the lanes of mask[P], stored in lane order from the group's running
+// vector offset (vec_base[G] + the stored vectors of the group's earlier packs).
 struct StreamLayout {
     const unsigned short* len = nullptr;    // [n_groups][n_rows]: stored steps of row k in group G
     const long long* group_base = nullptr;  // [n_groups + 1]: element offset of group G's stream
+                                            // before compaction (pack P = offset / 128)
     const int* desc = nullptr;              // per pack: template element offset of its first step
+    const unsigned* mask = nullptr;         // per pack: lanes whose 4-step vector is stored
+    const long long* vec_base = nullptr;    // [n_groups + 1]: first stored vector of group G
 };
 
 // Everything a projector kernel needs to know about one volume.
@@ -104,6 +110,14 @@ struct OpArgs {
     // the near rays are traced one direction octant at a time into a 27-offset shared-memory tile
     // (3.4 KB per warp instead of 16 KB, so four times the warps fit on an SM).
     float* near_acc = nullptr;
+    // Forward gather form inside MAP-EM: when set, the epilogue writes the EM ratio
+    // ratio_g[t] / max((A f)_t, *ratio_eps) of every tissue voxel instead of (A f)_t (prc.cu:270-274).
+    const float* ratio_g = nullptr;
+    const float* ratio_eps = nullptr;
+    // bf16 volumes (mixed-precision form inside MAP-EM): the gathered input and the forward's
+    // ratio output; only with the bf16 field (the gather of in16 replaces that of in).
+    const __nv_bfloat16* in16 = nullptr;
+    __nv_bfloat16* out16 = nullptr;
 };
 
 // ---- radial surrogate support -----------------------------------------------------------------
@@ -197,6 +211,14 @@ cudaError_t transpose_fill(const ProjParams& p, const FarField& far, const FarFi
 // u = f / W on the support (0 where that is not positive, as prc.cu:244-248 skips the source)
 // and out = 0 off the support: the input of the gather form of the forward projection.
 cudaError_t forward_prep(const ProjParams& p, const float* W, const float* f, float* u, float* out, cudaStream_t s);
+// The same preparation fused with the Biggs-Andrews prediction (prc.cu:318-321): every voxel's
+// y = max(f + lambda (f - prev), f / 2) with lambda = *lambda, then u = y / W on the support.
+cudaError_t forward_prep_extrapolate(const ProjParams& p, const float* W, const float* f, const float* prev,
+                                     const float* lambda, float* y, float* u, float* out, cudaStream_t s);
+// The same with u stored in bf16 (u16) and no `out` (the ratio goes to its own bf16 volume);
+// lambda == nullptr: no prediction, y is not written and u = f / W.
+cudaError_t forward_prep_half(const ProjParams& p, const float* W, const float* f, const float* prev,
+                              const float* lambda, float* y, __nv_bfloat16* u16, cudaStream_t s);
 
 // projector.cu
 cudaError_t setup_rays(const Grid& g, int n_rays, RayStep* d_far, RayStep* d_near, cudaStream_t s);
@@ -209,6 +231,17 @@ cudaError_t project(Op op, const ProjParams& p, const OpArgs& a, bool trace_near
 cudaError_t build_template(const ProjParams& p, int* tmpl, int* tmpl_neg, cudaStream_t s);
 // Fills the pack descriptors (one int per 128 stored entries) of a stream layout.
 cudaError_t build_descriptors(const ProjParams& p, const StreamLayout& l, int* desc, cudaStream_t s);
+// Compaction of a filled stream (l.group_base as built): mask[P] = lanes of pack P whose vector
+// holds a nonzero weight, group_vecs[G] = the group's stored vectors.
+cudaError_t field_masks(const ProjParams& p, const StreamLayout& l, const FarField& f, unsigned* mask,
+                        long long* group_vecs, cudaStream_t s);
+// Copies every stored vector of `from` (built layout) to its compacted place in `to`
+// (l.mask and l.vec_base set).
+cudaError_t field_compact(const ProjParams& p, const StreamLayout& l, const FarField& from, const FarField& to,
+                          cudaStream_t s);
+// Masks of an uncompacted stream (every lane stored) and vec_base[G] = group_base[G] / 4.
+cudaError_t field_identity_layout(const ProjParams& p, const StreamLayout& l, unsigned* mask, long long* vec_base,
+                                  cudaStream_t s);
 // Stored steps of the near-block row (125 offsets padded to whole packs).
 int near_row_steps();
 
@@ -247,6 +280,16 @@ cudaError_t em_extrapolate(const EmVolumes& v, const float* f, const float* prev
 cudaError_t em_ratio(const EmVolumes& v, const float* g, float* est, cudaStream_t s);
 cudaError_t em_update(const EmVolumes& v, const Grid& grid, const float* start, const float* back, float* next,
                       float beta, float gamma, cudaStream_t s);
+// The RDP update over the tissue voxels only (active[0..n_active), any order): the 26
+// neighbour distance weights come precomputed from geo_w (em_geometry_weights), and voxels off
+// the support are not written -- `next` must already be 0 there (it is: it holds the EM ratio,
+// which is 0 off the support).  Same arithmetic per voxel as em_update.
+cudaError_t em_update_active(const EmVolumes& v, const Grid& grid, const int* active, int n_active,
+                             const float* geo_w, const float* start, const float* back, float* next, float beta,
+                             float gamma, cudaStream_t s);
+// geo_w[27] = min(dx, dy, dz) / |offset| for every 3x3x3 neighbour offset (0 at the centre),
+// with the expression of prc.cu:293-296.
+cudaError_t em_geometry_weights(const Grid& grid, float* geo_w, cudaStream_t s);
 cudaError_t em_finish(const EmVolumes& v, float* next, float* residual, const float* h_prev, bool use_scale,
                       cudaStream_t s);
 cudaError_t em_sum(const EmVolumes& v, const float* x, cudaStream_t s);

@@ -7,8 +7,11 @@
 #include <algorithm>
 #include <climits>
 #include <cmath>
+#include <cstddef>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
 #include <utility>
 #include <vector>
@@ -64,11 +67,15 @@ struct prc_handle {
     long long* group_base = nullptr;
     long long* group_total = nullptr;
     int* desc = nullptr;
+    unsigned* mask = nullptr;        // compaction: per pack kept lanes, per group first vector
+    long long* vec_base = nullptr;
     // target-major copy of the field (forward projection as a gather)
     FarField far_t;
     unsigned short* len_t = nullptr;
     long long* group_base_t = nullptr;
     int* desc_t = nullptr;
+    unsigned* mask_t = nullptr;
+    long long* vec_base_t = nullptr;
     int* vox2src = nullptr;
     float* u = nullptr;  // f / W volume for the gather form of the forward projection
     int64_t far_t_entries = 0;
@@ -85,6 +92,10 @@ struct prc_handle {
 
     // MAP-EM state
     float* g_em = nullptr;
+    float* geo_w = nullptr;  // the RDP's 27 neighbour distance weights
+    // mixed-precision form: the gathered volumes of MAP-EM in bf16 (u = y / W, the EM ratio)
+    __nv_bfloat16* u16 = nullptr;
+    __nv_bfloat16* ratio16 = nullptr;
     float* vol[5] = {};  // f, prev, y, h_prev, est (rotated by pointer swaps)
     float *f = nullptr, *prev = nullptr, *y = nullptr, *h_prev = nullptr, *est = nullptr;
     EmScalars* scalars = nullptr;
@@ -92,8 +103,10 @@ struct prc_handle {
     bool em_started = false;
     int64_t bytes = 0;
     int64_t launches = 0;  // kernels this handle's entry points have enqueued (prc_launch_count)
+    int tile = PRC_TILE_AUTO;  // source tile in effect (PRC_TILE_*)
 
     std::vector<void*> allocations;
+    std::vector<size_t> allocation_bytes;
     // projection timing (prc_timing): start/end event pairs of forward and adjoint launches
     bool timing = false;
     std::vector<cudaEvent_t> events[2];
@@ -105,9 +118,22 @@ struct prc_handle {
         const cudaError_t e = cudaMalloc(&v, count * sizeof(T) > 0 ? count * sizeof(T) : 1);
         if (e != cudaSuccess) return e;
         allocations.push_back(v);
+        allocation_bytes.push_back(count * sizeof(T));
         bytes += (int64_t)(count * sizeof(T));
         *p = static_cast<T*>(v);
         return cudaMemsetAsync(v, 0, count * sizeof(T), stream);
+    }
+
+    // Frees one allocation of the handle early (after the stream has finished with it).
+    void release(void* v) {
+        for (size_t i = 0; i < allocations.size(); ++i)
+            if (allocations[i] == v) {
+                cudaFree(v);
+                bytes -= (int64_t)allocation_bytes[i];
+                allocations.erase(allocations.begin() + (long)i);
+                allocation_bytes.erase(allocation_bytes.begin() + (long)i);
+                return;
+            }
     }
 
     cudaStream_t pick(void* s) const { return s ? static_cast<cudaStream_t>(s) : stream; }
@@ -124,6 +150,15 @@ struct prc_handle {
         return a;
     }
 };
+
+// The tile of handles that are not tuned (see choose_tile).
+static constexpr int kDefaultTile = PRC_TILE_32x1x1;
+
+// (x, y, z) extent of a PRC_TILE_* source tile; every shape holds 32 voxels.
+static const int* tile_dims(int tile) {
+    static const int dims[][3] = {{8, 2, 2}, {8, 2, 2}, {16, 2, 1}, {32, 1, 1}, {4, 4, 2}, {16, 1, 2}};
+    return dims[tile >= 0 && tile <= PRC_TILE_16x1x2 ? tile : 0];
+}
 
 // Reads and clears the device error flag; a raised flag means a kernel gave up a bounded wait.
 static int check_device_error(prc_handle* h) {
@@ -147,6 +182,7 @@ void prc_default_options(prc_options* o) {
     o->exact_range = 0;
     o->cache = PRC_CACHE_FULL;
     o->precision = PRC_PRECISION_FP32;
+    o->tile = PRC_TILE_AUTO;
 }
 
 int prc_isotope_count(void) { return kNumIsotopes; }
@@ -161,6 +197,22 @@ int prc_isotope_cutoff(const char* isotope, float* cutoff_mm) {
 }
 
 const char* prc_last_error(void) { return g_last_error.c_str(); }
+
+int prc_host_alloc(size_t bytes, void** ptr) {
+    if (!ptr) return fail(PRC_ERR_ARGUMENT, "Invalid argument");
+    *ptr = nullptr;
+    const cudaError_t e = cudaMallocHost(ptr, bytes > 0 ? bytes : 1);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        *ptr = nullptr;
+        return fail(PRC_ERR_MEMORY, std::string("cudaMallocHost failed: ") + cudaGetErrorString(e));
+    }
+    return PRC_OK;
+}
+
+void prc_host_free(void* ptr) {
+    if (ptr) cudaFreeHost(ptr);
+}
 
 void prc_destroy(prc_handle* h) {
     if (!h) return;
@@ -267,6 +319,65 @@ static int build_target_major(prc_handle* h, const std::vector<int>& active, siz
     PRC_CUDA(cudaStreamSynchronize(h->stream));
     h->far_t_entries = run;
     return PRC_OK;
+}
+
+// Compaction of one stored stream (source-major, or the target-major copy): the lanes of every
+// pack whose 4-step vector holds a nonzero weight, a new allocation holding only those vectors,
+// and the built stream released.  When the new allocation cannot be had the built stream stays
+// and every lane of every pack counts as kept (the same consumer reads both).
+static int compact_stream(prc_handle* h, bool target) {
+    ProjParams& p = h->params;
+    StreamLayout& l = target ? p.tgt : p.src;
+    FarField& field = target ? h->far_t : h->far_field;
+    unsigned*& mask = target ? h->mask_t : h->mask;
+    long long*& vec_base = target ? h->vec_base_t : h->vec_base;
+    int64_t& entries = target ? h->far_t_entries : h->far_entries;
+    if (!field.on() || mask) return PRC_OK;
+    const size_t packs = (size_t)entries / (4 * kLanes);
+    PRC_CUDA(h->alloc(&mask, packs));
+    PRC_CUDA(h->alloc(&vec_base, (size_t)h->n_groups + 1));
+    l.mask = mask;
+    long long* d_kept = nullptr;
+    PRC_CUDA(cudaMalloc(&d_kept, (size_t)h->n_groups * sizeof(long long)));
+    struct Free {
+        long long* p;
+        ~Free() { cudaFree(p); }
+    } free_kept{d_kept};
+    PRC_CUDA(field_masks(p, l, field, mask, d_kept, h->stream));
+    std::vector<long long> base((size_t)h->n_groups + 1);
+    PRC_CUDA(cudaMemcpyAsync(base.data(), d_kept, (size_t)h->n_groups * sizeof(long long), cudaMemcpyDeviceToHost,
+                             h->stream));
+    PRC_CUDA(cudaStreamSynchronize(h->stream));
+    long long run = 0;
+    for (int g = 0; g < h->n_groups; ++g) {
+        const long long k = base[g];
+        base[g] = run;
+        run += k;
+    }
+    base[h->n_groups] = run;
+    FarField compact;
+    cudaError_t e = field.f32 ? h->alloc(&compact.f32, (size_t)run * 4) : h->alloc(&compact.b16, (size_t)run * 4);
+    if (e != cudaSuccess) {  // not enough memory for both streams at once: keep the built one
+        cudaGetLastError();
+        PRC_CUDA(field_identity_layout(p, l, mask, vec_base, h->stream));
+        l.vec_base = vec_base;
+        return PRC_OK;
+    }
+    PRC_CUDA(cudaMemcpyAsync(vec_base, base.data(), base.size() * sizeof(long long), cudaMemcpyHostToDevice,
+                             h->stream));
+    l.vec_base = vec_base;
+    PRC_CUDA(field_compact(p, l, field, compact, h->stream));
+    PRC_CUDA(cudaStreamSynchronize(h->stream));
+    h->release(field.f32 ? static_cast<void*>(field.f32) : static_cast<void*>(field.b16));
+    field = compact;
+    entries = run * 4;  // 4 steps per vector
+    return PRC_OK;
+}
+
+static int compact_fields(prc_handle* h) {
+    int rc = compact_stream(h, false);
+    if (rc == PRC_OK) rc = compact_stream(h, true);
+    return rc;
 }
 
 static int create_impl(prc_handle* h, const float* density_host, prc_net* net = nullptr, bool surrogate = false,
@@ -431,11 +542,12 @@ static int create_impl(prc_handle* h, const float* density_host, prc_net* net, b
         support[i] = rho[i] >= g.support_rho;
     }
     // Source order: tiles of kTileX x kTileY x kTileZ voxels, x fastest inside a tile.  A warp
-    // handles 32 consecutive sources; compact tiles give its lanes similar ray lengths (less
-    // zero padding in the stored field than 32 voxels along x, which cross tissue boundaries
-    // more often) while each gather still touches whole 32-byte row segments.  The order
-    // changes no result: every source keeps its own weights and summation order.
-    constexpr int kTileX = 8, kTileY = 2, kTileZ = 2;
+    // handles 32 consecutive sources.  Compact tiles give its lanes similar ray lengths (less
+    // zero padding in the stored field), long rows make every gather of a step touch fewer
+    // cache lines; the order changes no result: every source keeps its own weights and
+    // summation order.
+    if (h->tile == PRC_TILE_AUTO) h->tile = kDefaultTile;
+    const int kTileX = tile_dims(h->tile)[0], kTileY = tile_dims(h->tile)[1], kTileZ = tile_dims(h->tile)[2];
     for (int z0 = 0; z0 < g.nz; z0 += kTileZ)
         for (int y0 = 0; y0 < g.ny; y0 += kTileY)
             for (int x0 = 0; x0 < g.nx; x0 += kTileX)
@@ -499,6 +611,10 @@ static int create_impl(prc_handle* h, const float* density_host, prc_net* net, b
         rc = build_target_major(h, active, elem);
         if (rc != PRC_OK) return rc;
         if (h->far_t.on()) h->cache_mode = PRC_CACHE_FULL;
+        if (!batch_member) {  // a batch compacts after adding its target-major copies
+            rc = compact_fields(h);
+            if (rc != PRC_OK) return rc;
+        }
         PRC_CUDA(cudaStreamSynchronize(h->stream));
         return check_device_error(h);
     }
@@ -575,13 +691,17 @@ static int create_impl(prc_handle* h, const float* density_host, prc_net* net, b
         if (rc != PRC_OK) return rc;
         if (h->far_t.on()) h->cache_mode = PRC_CACHE_FULL;
     }
+    if (!batch_member) {  // a batch compacts after adding its target-major copies
+        const int rc = compact_fields(h);
+        if (rc != PRC_OK) return rc;
+    }
     PRC_CUDA(cudaStreamSynchronize(h->stream));
     return check_device_error(h);
 }
 
-static int create_common(const prc_geometry* geo, const char* isotope, const prc_options* opts_in,
+static int create_handle(const prc_geometry* geo, const char* isotope, const prc_options* opts_in,
                          const float* density_host, prc_net* net, bool surrogate, float target_scale,
-                         float fallback_nrmse, int64_t* fallbacks, prc_handle** out, bool batch_member = false) {
+                         float fallback_nrmse, int64_t* fallbacks, prc_handle** out, bool batch_member) {
     if (!out) return fail(PRC_ERR_ARGUMENT, "Invalid argument: null handle pointer");
     *out = nullptr;
     if (!geo || !density_host) return fail(PRC_ERR_ARGUMENT, "Invalid argument: null geometry or density");
@@ -594,7 +714,8 @@ static int create_common(const prc_geometry* geo, const char* isotope, const prc
         (o.rays & 1) || o.rays > INT_MAX - 31 || !(o.support_rho >= 0) || !(o.air_cap_mm > 0) ||
         !std::isfinite(o.support_rho) || !std::isfinite(o.air_cap_mm) ||
         (o.precision != PRC_PRECISION_FP32 && o.precision != PRC_PRECISION_BF16) || o.cache < PRC_CACHE_NONE ||
-        o.cache > PRC_CACHE_SOURCE_MAJOR || !(target_scale > 0) || !(fallback_nrmse >= 0))
+        o.cache > PRC_CACHE_SOURCE_MAJOR || o.tile < PRC_TILE_AUTO || o.tile > PRC_TILE_16x1x2 ||
+        !(target_scale > 0) || !(fallback_nrmse >= 0))
         return fail(PRC_ERR_ARGUMENT, "Invalid geometry or solver parameters");
     if (geo->nx > INT_MAX / geo->ny || geo->nx * geo->ny > INT_MAX / geo->nz)
         return fail(PRC_ERR_LIMIT, "Volume exceeds the INT_MAX voxel index limit");
@@ -605,6 +726,7 @@ static int create_common(const prc_geometry* geo, const char* isotope, const prc
     }
     std::strncpy(h->isotope, isotope, sizeof(h->isotope) - 1);
     h->opts = o;
+    h->tile = o.tile;
     h->g = Grid{geo->nx, geo->ny, geo->nz, geo->dx, geo->dy, geo->dz, h->model.cutoff, o.support_rho, o.air_cap_mm};
     h->n = (size_t)geo->nx * geo->ny * geo->nz;
     const int rc = create_impl(h, density_host, net, surrogate, target_scale, fallback_nrmse, fallbacks, batch_member);
@@ -616,6 +738,115 @@ static int create_common(const prc_geometry* geo, const char* isotope, const prc
     }
     *out = h;
     return PRC_OK;
+}
+
+
+// ---- source-tile autotuner (PRC_TILE_AUTO) ---------------------------------------------------
+// The tile shape trades the field's zero padding (compact tiles: the 32 lanes of a group stop
+// their rays at similar steps) against the cache lines every gather of a step touches (long
+// rows).  Which wins depends on the grid, the isotope's range and the stored precision, so the
+// first handle of each configuration builds the stored field with every candidate shape on the
+// central slab of at most kTuneSlices z-slices of its own density (the same rays, ranges and
+// tissue mix at a fraction of the build time), times one forward and one adjoint projection
+// with CUDA events after a warm-up pair, and keeps the fastest; later handles of the
+// configuration reuse the choice.  Forms without a stored field (near cache, traced) and
+// surrogate fields take kDefaultTile.
+static constexpr int kTileCandidates[] = {PRC_TILE_32x1x1, PRC_TILE_16x2x1, PRC_TILE_8x2x2};
+static constexpr int kTuneSlices = 32;
+static std::mutex g_tile_mutex;
+static std::map<std::string, int> g_tile_choice;
+
+static std::string tile_key(const prc_geometry* geo, const char* isotope, const prc_options& o) {
+    char key[256];
+    snprintf(key, sizeof(key), "%d %d %d %a %a %a %s %d %a %a %d %d %d", geo->nx, geo->ny, geo->nz, geo->dx, geo->dy,
+             geo->dz, isotope ? isotope : "", o.rays, o.support_rho, o.air_cap_mm, o.exact_range, o.cache,
+             o.precision);
+    return key;
+}
+
+// Device milliseconds of one forward and one adjoint projection of the handle (after a warm-up
+// pair), on zero volumes: the gathers run whatever the values.
+static int time_projection_pair(prc_handle* h, float* ms) {
+    float *in = nullptr, *out = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    struct Cleanup {
+        float*& in;
+        float*& out;
+        cudaEvent_t& e0;
+        cudaEvent_t& e1;
+        ~Cleanup() {
+            if (in) cudaFree(in);
+            if (out) cudaFree(out);
+            if (e0) cudaEventDestroy(e0);
+            if (e1) cudaEventDestroy(e1);
+        }
+    } cleanup{in, out, e0, e1};
+    PRC_CUDA(cudaMalloc(&in, h->n * sizeof(float)));
+    PRC_CUDA(cudaMalloc(&out, h->n * sizeof(float)));
+    PRC_CUDA(cudaMemsetAsync(in, 0, h->n * sizeof(float), h->stream));
+    PRC_CUDA(cudaEventCreate(&e0));
+    PRC_CUDA(cudaEventCreate(&e1));
+    for (int pass = 0; pass < 2; ++pass) {
+        if (pass == 1) PRC_CUDA(cudaEventRecord(e0, h->stream));
+        int rc = prc_forward(h, in, out, h->stream);
+        if (rc == PRC_OK) rc = prc_adjoint(h, in, out, h->stream);
+        if (rc != PRC_OK) return rc;
+    }
+    PRC_CUDA(cudaEventRecord(e1, h->stream));
+    PRC_CUDA(cudaEventSynchronize(e1));
+    PRC_CUDA(cudaEventElapsedTime(ms, e0, e1));
+    return check_device_error(h);
+}
+
+static int choose_tile(const prc_geometry* geo, const char* isotope, const prc_options& o, const float* density_host,
+                       bool surrogate) {
+    if (surrogate || (o.cache != PRC_CACHE_FULL && o.cache != PRC_CACHE_SOURCE_MAJOR)) return kDefaultTile;
+    const std::string key = tile_key(geo, isotope, o);
+    {
+        std::lock_guard<std::mutex> lock(g_tile_mutex);
+        const auto it = g_tile_choice.find(key);
+        if (it != g_tile_choice.end()) return it->second;
+    }
+    prc_geometry slab = *geo;
+    const float* slab_density = density_host;
+    if (geo->nz > kTuneSlices) {
+        slab.nz = kTuneSlices;
+        slab_density += (size_t)(geo->nz - kTuneSlices) / 2 * geo->nx * geo->ny;
+    }
+    int best = kDefaultTile;
+    float best_ms = 0.0f;
+    for (const int cand : kTileCandidates) {
+        prc_options oc = o;
+        oc.tile = cand;
+        prc_handle* h = nullptr;
+        if (create_handle(&slab, isotope, &oc, slab_density, nullptr, false, 1.0f, 0.0f, nullptr, &h, false) != PRC_OK)
+            continue;  // e.g. not enough memory for this shape's field: not a candidate
+        float ms = 0.0f;
+        const bool field = h->far_field.on();
+        const int rc = field ? time_projection_pair(h, &ms) : PRC_ERR_STATE;
+        prc_destroy(h);
+        if (!field) break;  // no stored field: the shape does not matter
+        if (rc == PRC_OK && (best_ms == 0.0f || ms < best_ms)) best = cand, best_ms = ms;
+    }
+    g_last_error.clear();
+    std::lock_guard<std::mutex> lock(g_tile_mutex);
+    g_tile_choice[key] = best;
+    return best;
+}
+
+static int create_common(const prc_geometry* geo, const char* isotope, const prc_options* opts_in,
+                         const float* density_host, prc_net* net, bool surrogate, float target_scale,
+                         float fallback_nrmse, int64_t* fallbacks, prc_handle** out, bool batch_member = false) {
+    prc_options o;
+    prc_default_options(&o);
+    if (opts_in) o = *opts_in;
+    if (o.tile == PRC_TILE_AUTO && geo && density_host && out && o.cache >= PRC_CACHE_NONE &&
+        o.cache <= PRC_CACHE_SOURCE_MAJOR) {
+        RangeModel m;
+        if (m.resolve(isotope ? isotope : "")) o.tile = choose_tile(geo, isotope, o, density_host, surrogate);
+    }
+    return create_handle(geo, isotope, &o, density_host, net, surrogate, target_scale, fallback_nrmse, fallbacks, out,
+                         batch_member);
 }
 
 int prc_create(const prc_geometry* geo, const char* isotope, const prc_options* opts, const float* density_host,
@@ -728,6 +959,10 @@ int prc_adjoint(prc_handle* h, const float* d_in, float* d_out, void* stream) {
     return PRC_OK;
 }
 
+// The mixed-precision form keeps the volumes MAP-EM gathers in bf16: with the bf16 field in both
+// majors (the forward is a gather whose epilogue takes the ratio).
+static bool half_volumes(const prc_handle* h) { return h->far_t.b16 && h->far_field.b16; }
+
 static int ensure_em(prc_handle* h) {
     if (h->g_em) return PRC_OK;
     PRC_CUDA(h->alloc(&h->g_em, h->n));
@@ -735,7 +970,18 @@ static int ensure_em(prc_handle* h) {
     PRC_CUDA(h->alloc(&h->scalars, 1));
     PRC_CUDA(h->alloc(&h->red.partials, (size_t)kReduceBlocks * 4));
     PRC_CUDA(h->alloc(&h->red.counter, 1));
+    PRC_CUDA(h->alloc(&h->geo_w, 27));
+    PRC_CUDA(em_geometry_weights(h->g, h->geo_w, h->stream));
+    if (half_volumes(h)) {
+        PRC_CUDA(h->alloc(&h->u16, h->n));
+        PRC_CUDA(h->alloc(&h->ratio16, h->n));
+    }
     return PRC_OK;
+}
+
+// Device address of a float member of the handle's device-resident EmScalars.
+static const float* scalar_field(const prc_handle* h, size_t offset) {
+    return reinterpret_cast<const float*>(reinterpret_cast<const char*>(h->scalars) + offset);
 }
 
 static int em_begin_impl(prc_handle* h, const float* d_g, bool initialize, cudaStream_t s) {
@@ -765,20 +1011,61 @@ int prc_em_iterate(prc_handle* h, int n_iter, float beta, float gamma, int accel
         return fail(PRC_ERR_ARGUMENT, "Invalid geometry or solver parameters");
     const cudaStream_t s = h->pick(stream);
     const EmVolumes v = h->em_volumes();
+    // With the target-major field the forward projection is a gather whose preparation pass
+    // also makes the Biggs-Andrews prediction and whose epilogue takes the EM ratio, so an
+    // iteration is five launches: prep(+extrapolate), forward(+ratio), adjoint, RDP update,
+    // finish.  The scatter and traced forms keep the separate extrapolate and ratio passes.
+    const bool fused = h->far_t.on();
+    const bool half = half_volumes(h);
     for (int it = 0; it < n_iter; ++it) {  // prc.cu:675-700
         const float* start = h->f;
-        if (accelerate) {
-            PRC_CUDA(em_extrapolate(v, h->f, h->prev, h->y, s));
+        if (fused) {
+            const float* lambda = accelerate ? scalar_field(h, offsetof(EmScalars, lambda)) : nullptr;
+            if (half) {
+                PRC_CUDA(forward_prep_half(h->params, h->W, h->f, h->prev, lambda, h->y, h->u16, s));
+            } else if (accelerate) {
+                PRC_CUDA(forward_prep_extrapolate(h->params, h->W, h->f, h->prev, lambda, h->y, h->u, h->est, s));
+            } else {
+                PRC_CUDA(forward_prep(h->params, h->W, h->f, h->u, h->est, s));
+            }
+            if (accelerate) start = h->y;
             ++h->launches;
-            start = h->y;
+            OpArgs a = h->op_args();
+            a.in = h->u;
+            a.out = h->est;
+            if (half) a.in16 = h->u16, a.out16 = h->ratio16;
+            a.ratio_g = h->g_em;
+            a.ratio_eps = scalar_field(h, offsetof(EmScalars, eps));
+            PRC_CUDA(timing_mark(h, 0, s));
+            PRC_CUDA(project(Op::Forward, h->params, a, h->trace_near, s));
+            PRC_CUDA(timing_mark(h, 0, s));
+            ++h->launches;
+        } else {
+            if (accelerate) {
+                PRC_CUDA(em_extrapolate(v, h->f, h->prev, h->y, s));
+                ++h->launches;
+                start = h->y;
+            }
+            const int rc = prc_forward(h, start, h->est, s);
+            if (rc != PRC_OK) return rc;
+            PRC_CUDA(em_ratio(v, h->g_em, h->est, s));
+            ++h->launches;
         }
-        int rc = prc_forward(h, start, h->est, s);
-        if (rc != PRC_OK) return rc;
-        PRC_CUDA(em_ratio(v, h->g_em, h->est, s));
-        ++h->launches;
-        rc = prc_adjoint(h, h->est, h->prev, s);  // prediction has consumed prev
-        if (rc != PRC_OK) return rc;
-        PRC_CUDA(em_update(v, h->g, start, h->prev, h->est, beta, gamma, s));
+        if (half) {  // the adjoint gathers the bf16 ratio
+            OpArgs a = h->op_args();
+            a.in16 = h->ratio16;
+            a.out = h->prev;  // prediction has consumed prev
+            PRC_CUDA(timing_mark(h, 1, s));
+            PRC_CUDA(project(Op::Adjoint, h->params, a, h->trace_near, s));
+            PRC_CUDA(timing_mark(h, 1, s));
+            ++h->launches;
+        } else {
+            const int rc = prc_adjoint(h, h->est, h->prev, s);  // prediction has consumed prev
+            if (rc != PRC_OK) return rc;
+        }
+        // est is 0 off the support, which is what the update leaves there: every MAP-EM volume
+        // starts at 0 there and no pass writes anything but 0 off the support
+        PRC_CUDA(em_update_active(v, h->g, h->active, h->n_active, h->geo_w, start, h->prev, h->est, beta, gamma, s));
         ++h->launches;
         if (beta > 0.0f || accelerate) {
             PRC_CUDA(em_finish(v, h->est, accelerate ? h->y : nullptr, h->h_prev, beta > 0.0f, s));
@@ -904,6 +1191,12 @@ int prc_wait_selftest(prc_handle* h, int rounds) {
     if (!h || rounds < 1 || rounds > (1 << 20)) return fail(PRC_ERR_ARGUMENT, "Invalid argument");
     PRC_CUDA(wait_selftest(rounds, h->error, h->stream));
     return prc_synchronize(h);
+}
+
+int prc_tile(const prc_handle* h, int* tile) {
+    if (!h || !tile) return fail(PRC_ERR_ARGUMENT, "Invalid argument");
+    *tile = h->tile;
+    return PRC_OK;
 }
 
 int prc_launch_count(const prc_handle* h, int64_t* n) {
@@ -1252,6 +1545,15 @@ int prc_batch_create(int n_frames, const prc_frame* frames, const prc_options* o
                 return rc;
             }
             if (h->far_t.on()) h->cache_mode = PRC_CACHE_FULL;
+        }
+    }
+    for (int i = 0; i < n_frames; ++i) {  // every stream complete: drop the all-zero lane vectors
+        const int rc = compact_fields(b->frames[i]);
+        if (rc != PRC_OK) {
+            const std::string msg = g_last_error;
+            prc_batch_destroy(b);
+            g_last_error = "frame " + std::to_string(i) + ": " + msg;
+            return rc;
         }
     }
     *out = b;

@@ -212,11 +212,11 @@ void read_failed(const std::string& path, size_t n) {
 }
 
 // Writes an all-finite image; otherwise returns the reference's message and writes nothing.
-std::string save_image_ok(const std::string& path, const std::vector<float>& host) {  // prc.cu:349-360
-    for (float value : host)
-        if (!std::isfinite(value)) return "Non-finite output: " + path;
+std::string save_image_ok(const std::string& path, const float* host, size_t n) {  // prc.cu:349-360
+    for (size_t i = 0; i < n; ++i)
+        if (!std::isfinite(host[i])) return "Non-finite output: " + path;
     FILE* fp = fopen(path.c_str(), "wb");
-    if (!fp || fwrite(host.data(), sizeof(float), host.size(), fp) != host.size()) {
+    if (!fp || fwrite(host, sizeof(float), n, fp) != n) {
         if (fp) fclose(fp);
         return "Cannot write " + path;
     }
@@ -224,8 +224,8 @@ std::string save_image_ok(const std::string& path, const std::vector<float>& hos
     return "";
 }
 
-void save_image(const std::string& path, const std::vector<float>& host) {
-    const std::string err = save_image_ok(path, host);
+void save_image(const std::string& path, const float* host, size_t n) {
+    const std::string err = save_image_ok(path, host, n);
     if (!err.empty()) {
         fprintf(stderr, "%s\n", err.c_str());
         die();
@@ -235,9 +235,35 @@ void save_image(const std::string& path, const std::vector<float>& host) {
 // Checkpoints (--save-every) are written by a helper thread while the GPU runs the next
 // iterations; a write error is reported, with the reference's message, before anything else is
 // written.
+// A host image buffer in pinned (page-locked) memory when the runtime can give it, so the
+// device-to-host copies run at full speed; pageable memory otherwise.
+struct HostImage {
+    float* data = nullptr;
+    size_t n = 0;
+    bool pinned = false;
+    std::vector<float> fallback;
+    void resize(size_t count) {
+        if (n == count) return;
+        release();
+        n = count;
+        void* p = nullptr;
+        if (prc_host_alloc(count * sizeof(float), &p) == PRC_OK) {
+            data = static_cast<float*>(p), pinned = true;
+        } else {
+            fallback.resize(count), data = fallback.data(), pinned = false;
+        }
+    }
+    void release() {
+        if (pinned) prc_host_free(data);
+        fallback.clear();
+        data = nullptr, n = 0, pinned = false;
+    }
+    ~HostImage() { release(); }
+};
+
 struct CheckpointWriter {
     std::thread thread;
-    std::vector<float> image;
+    HostImage image;
     std::string error;
     void finish() {
         if (thread.joinable()) thread.join();
@@ -247,7 +273,7 @@ struct CheckpointWriter {
         }
     }
     void start(const std::string& path) {
-        thread = std::thread([this, path] { error = save_image_ok(path, image); });
+        thread = std::thread([this, path] { error = save_image_ok(path, image.data, image.n); });
     }
 };
 
@@ -258,9 +284,9 @@ void check(int rc) {
     }
 }
 
-double host_sum(const std::vector<float>& v) {
+double host_sum(const float* v, size_t n) {
     double s = 0.0;
-    for (float x : v) s += x;
+    for (size_t i = 0; i < n; ++i) s += v[i];
     return s;
 }
 
@@ -280,25 +306,67 @@ int main(int argc, char** argv) {
     const int nx = o.dims[0], ny = o.dims[1], nz = o.dims[2];
     const size_t n = (size_t)nx * ny * nz;
 
+    // Host I/O (prc.cu:591-622, restructured): both files are read at once; as soon as the
+    // density is complete and finite, a builder thread makes the first CUDA contact and builds
+    // the projector (prc_create: clamp, support, source order, uploads, layout, normalisation)
+    // while this thread finishes the input file and validates the activity.  The messages and
+    // their precedence are the reference's: size errors density first, then the first voxel
+    // where density or activity is non-finite, then "No activity".  Any of them stops the run
+    // with nothing written, the builder's result discarded (a hidden GPU makes it fail quietly).
     const double t0 = now_s();
     std::vector<float> rho(n), img(n);
     bool img_ok = false;
-    std::thread reader([&] { img_ok = read_raw_ok(o.input, &img); });  // both files at once
+    std::thread reader([&] { img_ok = read_raw_ok(o.input, &img); });
     const bool rho_ok = read_raw_ok(o.density, &rho);
+    bool rho_finite = rho_ok;
+    for (size_t i = 0; rho_finite && i < n; ++i) rho_finite = std::isfinite(rho[i]);
+
+    prc_geometry geo{nx, ny, nz, o.voxel[0], o.voxel[1], o.voxel[2]};
+    prc_options opts;
+    prc_default_options(&opts);
+    opts.rays = o.rays;
+    opts.support_rho = o.support_rho;
+    opts.air_cap_mm = o.air_cap_mm;
+    opts.exact_range = o.exact_range;
+    opts.cache = o.trace_near_every_pass ? PRC_CACHE_NONE : o.cache;
+    opts.precision = o.bf16 ? PRC_PRECISION_BF16 : PRC_PRECISION_FP32;
+    struct Build {
+        prc_handle* h = nullptr;
+        int rc = PRC_OK;
+        std::string error;
+        double seconds = 0.0;
+    } build;
+    std::thread builder;
+    if (rho_finite) {
+        builder = std::thread([&] {
+            const double tb = now_s();
+            build.rc = prc_create(&geo, o.isotope.c_str(), &opts, rho.data(), &build.h);
+            if (build.rc != PRC_OK) build.error = prc_last_error();
+            build.seconds = now_s() - tb;
+        });
+    }
+    auto stop = [&]() -> int {  // a validation failure: discard the build
+        if (builder.joinable()) builder.join();
+        if (build.h) prc_destroy(build.h);
+        return EXIT_FAILURE;
+    };
     reader.join();
     if (!rho_ok) read_failed(o.density, n);  // the reference's order: density first
-    if (!img_ok) read_failed(o.input, n);
+    if (!img_ok) {
+        stop();
+        read_failed(o.input, n);
+    }
     size_t n_active = 0;
     double input_sum = 0.0, support_sum = 0.0;
     for (size_t i = 0; i < n; ++i) {  // prc.cu:598-613
         if (!std::isfinite(rho[i]) || !std::isfinite(img[i])) {
             fprintf(stderr, "Non-finite density or activity at voxel %zu\n", i);
-            return EXIT_FAILURE;
+            return stop();
         }
-        rho[i] = std::max(rho[i], kMinDensity);
+        const float r = std::max(rho[i], kMinDensity);
         img[i] = std::max(img[i], 0.0f);
         input_sum += img[i];
-        if (rho[i] >= o.support_rho) {
+        if (r >= o.support_rho) {
             ++n_active;
             support_sum += img[i];
         } else {
@@ -311,39 +379,36 @@ int main(int argc, char** argv) {
            100.0 * n_active / n, support_sum, input_sum, input_sum > 0 ? 100.0 * support_sum / input_sum : 0.0);
     if (support_sum == 0.0) {
         fprintf(stderr, "No activity in voxels with density >= %g: nothing to do\n", o.support_rho);
-        return EXIT_FAILURE;
+        return stop();
     }
 
-    // First CUDA contact.
-    prc_geometry geo{nx, ny, nz, o.voxel[0], o.voxel[1], o.voxel[2]};
-    prc_options opts;
-    prc_default_options(&opts);
-    opts.rays = o.rays;
-    opts.support_rho = o.support_rho;
-    opts.air_cap_mm = o.air_cap_mm;
-    opts.exact_range = o.exact_range;
-    opts.cache = o.trace_near_every_pass ? PRC_CACHE_NONE : o.cache;
-    opts.precision = o.bf16 ? PRC_PRECISION_BF16 : PRC_PRECISION_FP32;
+    // The projector (its build overlapped the input's read and validation).
     double t = now_s();
-    prc_handle* h = nullptr;
-    check(prc_create(&geo, o.isotope.c_str(), &opts, rho.data(), &h));
+    builder.join();
+    if (build.rc != PRC_OK) {
+        fprintf(stderr, "%s\n", build.error.c_str());
+        return EXIT_FAILURE;
+    }
+    prc_handle* h = build.h;
     int64_t bytes = 0, far_entries = 0, far_t_entries = 0;
     int mode = 0;
     prc_device_bytes(h, &bytes);
     prc_cache_mode(h, &mode, &far_entries, &far_t_entries);
     printf("normalisation (%d near-block + %d far-field rays): %.2f s, cache %s, device memory %.0f MiB\n", kNearRays,
-           o.rays, now_s() - t,
+           o.rays, build.seconds,
            mode == PRC_CACHE_FULL ? "field (source+target major)" : mode == PRC_CACHE_SOURCE_MAJOR ? "field (source major)"
            : mode == PRC_CACHE_NEAR ? "near" : "none",
            bytes / 1048576.0);
 
-    std::vector<float> out(n);
+    HostImage out;
+    out.resize(n);
     if (o.mode == "forward" || o.mode == "adjoint") {  // prc.cu:648-657
         t = now_s();
-        check(o.mode == "forward" ? prc_forward_host(h, img.data(), out.data()) : prc_adjoint_host(h, img.data(), out.data()));
+        check(o.mode == "forward" ? prc_forward_host(h, img.data(), out.data) : prc_adjoint_host(h, img.data(), out.data));
         printf("%s: %.3f s\n", o.mode.c_str(), now_s() - t);
-        save_image(o.output, out);
-        printf("sum in %.6g, sum out %.6g, total %.2f s\n", support_sum, host_sum(out), now_s() - t0);
+        save_image(o.output, out.data, n);
+        printf("sum in %.6g, sum out %.6g, total %.2f s\n", support_sum, host_sum(out.data, n), now_s() - t0);
+        out.release();
         prc_destroy(h);
         return EXIT_SUCCESS;
     }
@@ -352,7 +417,7 @@ int main(int argc, char** argv) {
     printf("MAP-EM: %d iterations, beta %.4g, gamma %.3g\n", o.iterations, o.beta, o.gamma);
     t = now_s();
     if (o.iterations == 0) {
-        check(prc_em_run_host(h, img.data(), out.data(), 0, o.beta, o.gamma, !o.plain));
+        check(prc_em_run_host(h, img.data(), out.data, 0, o.beta, o.gamma, !o.plain));
     } else {
         check(prc_em_begin_host(h, img.data()));
         t = now_s();
@@ -368,23 +433,25 @@ int main(int argc, char** argv) {
                 snprintf(tag, sizeof(tag), "_it%03d", it);
                 writer.finish();  // the previous checkpoint is on disk; its buffer is free
                 writer.image.resize(n);
-                check(prc_em_estimate_host(h, writer.image.data()));
+                check(prc_em_estimate_host(h, writer.image.data));
                 writer.start(with_suffix(o.output, tag));
             }
         }
         writer.finish();
-        check(prc_em_estimate_host(h, out.data()));
+        check(prc_em_estimate_host(h, out.data));
     }
     const double t_iter = now_s() - t;
-    save_image(o.output, out);
+    save_image(o.output, out.data, n);
     if (o.reproject) {
-        std::vector<float> reproj(n);
-        check(prc_forward_host(h, out.data(), reproj.data()));
-        save_image(with_suffix(o.output, "_REPROJ"), reproj);
+        HostImage reproj;
+        reproj.resize(n);
+        check(prc_forward_host(h, out.data, reproj.data));
+        save_image(with_suffix(o.output, "_REPROJ"), reproj.data, n);
     }
-    printf("sum blurred (tissue) %.6g, sum corrected %.6g\n", support_sum, host_sum(out));
+    printf("sum blurred (tissue) %.6g, sum corrected %.6g\n", support_sum, host_sum(out.data, n));
     printf("iterations %.2f s (%.2f s each), total %.2f s\n", t_iter, o.iterations ? t_iter / o.iterations : 0.0,
            now_s() - t0);
+    out.release();
     prc_destroy(h);
     return EXIT_SUCCESS;
 }

@@ -22,6 +22,7 @@
 #include "engine.h"
 
 #include <cstdio>
+#include <type_traits>
 
 namespace prc {
 namespace {
@@ -143,7 +144,14 @@ __device__ __forceinline__ void march(const ProjParams& p, const RayStep& R, boo
 enum NearMode : int { kTraceNear = 0, kCacheF32 = 1, kCacheBF16 = 2 };
 // Far-field source: marched rays, the source-major field (adjoint; forward by scatter), or the
 // target-major field (forward by gather; the *T modes).
-enum FarMode : int { kMarch = 0, kFieldF32 = 1, kFieldBF16 = 2, kFieldF32T = 3, kFieldBF16T = 4 };
+// kFieldBF16H / kFieldBF16TH: the bf16 field gathering a bf16 volume (a.in16) -- inside
+// MAP-EM the mixed-precision form keeps the gathered volumes (u = y / W and the EM ratio) in
+// bf16, and its forward epilogue writes the ratio as bf16 (a.out16).
+enum FarMode : int { kMarch = 0, kFieldF32 = 1, kFieldBF16 = 2, kFieldF32T = 3, kFieldBF16T = 4, kFieldBF16H = 5,
+                     kFieldBF16TH = 6 };
+__host__ __device__ constexpr bool target_major(int m) { return m == kFieldF32T || m == kFieldBF16T || m == kFieldBF16TH; }
+__host__ __device__ constexpr bool half_volume(int m) { return m == kFieldBF16H || m == kFieldBF16TH; }
+__host__ __device__ constexpr int field_base(int m) { return m == kFieldF32 || m == kFieldF32T ? kFieldF32 : kFieldBF16; }
 
 // ---- stored coefficient field ----------------------------------------------------------------
 // Stream of one group: template row 0 is the near block (125 offsets, padded to kNearRow
@@ -155,17 +163,15 @@ enum FarMode : int { kMarch = 0, kFieldF32 = 1, kFieldBF16 = 2, kFieldF32T = 3, 
 // walking the stream.
 constexpr int kPack = 4;
 constexpr int kNearRow = 128;  // 125 block offsets rounded up to whole packs
-// TMA ring of the field stream: kStages chunks of kChunk bytes per warp.
-#ifndef PRC_FIELD_STAGES
-#define PRC_FIELD_STAGES 2
+// Shared memory the stored-field launches reserve per warp although they use none: it sets the
+// L1 / shared-memory split and so how many warps share an SM's L1 (on the 128x128x159 torso a
+// launch without it, with the largest L1, measured 1.7-2x slower).
+#ifndef PRC_FIELD_SMEM_PER_WARP
+#define PRC_FIELD_SMEM_PER_WARP 4096
 #endif
-#ifndef PRC_FIELD_CHUNK
-#define PRC_FIELD_CHUNK 2048
-#endif
-constexpr int kStages = PRC_FIELD_STAGES;
-constexpr int kChunk = PRC_FIELD_CHUNK;
-constexpr size_t kFieldSmemBytes = size_t(kWarps) * kStages * kChunk;
-// try_wait rounds before a field copy is declared lost (each round is a bounded hardware wait).
+constexpr size_t kFieldSmemPerWarp = PRC_FIELD_SMEM_PER_WARP;
+constexpr size_t kFieldSmemBytes = size_t(kWarps) * kFieldSmemPerWarp;
+// try_wait rounds before a bounded mbarrier wait gives up (each round is a bounded hardware wait).
 constexpr int kWaitRounds = 1 << 20;
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
@@ -178,17 +184,8 @@ __device__ __forceinline__ void fence_mbarrier_init() {
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
-__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
-}
-// 1D bulk copy global -> this CTA's shared memory, completion counted on an mbarrier.
-// Source and destination are 16-byte aligned and bytes is a multiple of 16.
-__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                     smem_u32(dst)),
-                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
-                 : "memory");
 }
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity, int rounds = kWaitRounds) {
     for (int i = 0; i < rounds; ++i) {
@@ -203,11 +200,18 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity
     return false;
 }
 
-// An 8-byte vector of the bf16 field, read once per projection: loaded without allocating in
-// L1, which keeps L1 for the volume being gathered.
+// A vector of the stored field (8 bytes bf16, 16 bytes fp32), read once per projection: loaded
+// without allocating in L1, which keeps L1 for the volume being gathered.
 __device__ __forceinline__ uint2 ld_stream(const uint2* q) {
     uint2 x;
     asm("ld.global.nc.L1::no_allocate.v2.u32 {%0, %1}, [%2];" : "=r"(x.x), "=r"(x.y) : "l"(q));
+    return x;
+}
+__device__ __forceinline__ float4 ld_stream(const float4* q) {
+    float4 x;
+    asm("ld.global.nc.L1::no_allocate.v4.f32 {%0, %1, %2, %3}, [%4];"
+        : "=f"(x.x), "=f"(x.y), "=f"(x.z), "=f"(x.w)
+        : "l"(q));
     return x;
 }
 
@@ -274,11 +278,10 @@ __global__ void order_near_kernel(const RayStep* near, short* order, int* start)
 // then also holds the near block).  Norm always marches and writes W, and the near cache or
 // the stored field when they are allocated; Layout marches to size the field.
 // The work of one warp (group `group`, warp `warp` of its block): dyn_smem is the block's
-// dynamic shared memory (near tiles or field rings are indexed by warp), bars the warp's
-// kStages mbarriers.
+// dynamic shared memory (near tiles are indexed by warp).
 template <Op OP, bool EXACT, int NEAR_MODE, int FAR_MODE>
 __device__ __forceinline__ void project_group(const ProjParams& p, const OpArgs& a, int group, int warp,
-                                              unsigned char* dyn_smem, uint64_t* bars) {
+                                              unsigned char* dyn_smem) {
     const int lane = threadIdx.x & 31;
     if (group * kLanes >= p.n_active) return;  // the whole warp leaves together
     const int src = group * kLanes + lane;
@@ -288,7 +291,7 @@ __device__ __forceinline__ void project_group(const ProjParams& p, const OpArgs&
     float scale = 0.0f, acc = 0.0f;
     unsigned long long cnt = 0;
     if constexpr (OP == Op::Forward) {  // prc.cu:244-248
-        if (FAR_MODE >= kFieldF32T) {
+        if (target_major(FAR_MODE)) {
             live = valid;  // gather form: lanes are targets, a.in holds u = f / W
         } else {
             const float fs = valid ? __ldg(a.in + s) : 0.0f, ws = valid ? __ldg(a.W + src) : 0.0f;
@@ -396,176 +399,98 @@ __device__ __forceinline__ void project_group(const ProjParams& p, const OpArgs&
             }
         }
     } else {
-        // Stored field.  fp32: streamed by TMA -- lane 0 keeps kStages bulk copies of kChunk bytes in
-        // flight into this warp's shared-memory ring (cp.async.bulk, completion counted by an
-        // mbarrier), so the weights arrive as contiguous DRAM bursts without holding
-        // registers.  A chunk is consumed in batches of kBatch packs: the packs' template
-        // offsets (one int4 broadcast each, addressed by the pack descriptors), the weights
-        // from shared memory, then one predicated gather per nonzero weight -- zero padding
-        // costs no memory traffic -- or one scatter per nonzero weight without the
-        // target-major copy.  Entries of lanes that are not sources are zero by construction.
-        // The template offsets are fetched one batch ahead and the descriptors two batches
-        // ahead, so the descriptor -> template -> gather chain exposes one memory latency per
-        // batch instead of three.
-        constexpr bool kGatherT = OP == Op::Forward && FAR_MODE >= kFieldF32T;
-        constexpr int kBase = FAR_MODE >= kFieldF32T ? FAR_MODE - 2 : FAR_MODE;  // kFieldF32 / kFieldBF16
-        constexpr int kElem = kBase == kFieldF32 ? 4 : 2;
-        constexpr int kPackBytes = kPack * kLanes * kElem;
-        constexpr int kPacksPerChunk = kChunk / kPackBytes;
+        // Stored field, compacted: pack P of the group keeps the vectors of the lanes in mask[P],
+        // in lane order from a running vector offset.  Each lane loads its own vector straight
+        // from HBM (16 bytes fp32, 8 bytes bf16; a warp's loads of one pack are contiguous)
+        // without allocating in L1, which keeps L1 for the volume being gathered.  A batch is
+        // kBatch packs: the packs' template offsets (one int4 broadcast each, addressed by the
+        // pack descriptors), the weights, then one predicated gather per nonzero weight -- zero
+        // padding costs no memory traffic -- or one scatter per nonzero weight without the
+        // target-major copy.  Weights and template offsets are loaded one batch ahead and the
+        // descriptors and masks two batches ahead, so the descriptor -> template -> gather chain
+        // exposes one memory latency per batch instead of three.
+        constexpr bool kGatherT = OP == Op::Forward && target_major(FAR_MODE);
+        constexpr int kBase = field_base(FAR_MODE);  // kFieldF32 / kFieldBF16
         constexpr int kBatch = 4;  // packs per batch: 16 steps in flight per lane
+        using Vec = typename std::conditional<kBase == kFieldF32, float4, uint2>::type;
         const StreamLayout& lay = kGatherT ? p.tgt : p.src;
         const FarField& fld = kGatherT ? a.farT : a.far;
         const int* tmpl = kGatherT ? p.tmpl_neg : p.tmpl;
         const long long e0 = lay.group_base[group], e1 = lay.group_base[group + 1];
-        const int* desc = lay.desc + e0 / (kPack * kLanes);
+        const long long pk0 = e0 / (kPack * kLanes);
+        const int* desc = lay.desc + pk0;
+        const unsigned* mask = lay.mask + pk0;
         const int n_packs = (int)((e1 - e0) / (kPack * kLanes));
+        const Vec* vec = reinterpret_cast<const Vec*>(kBase == kFieldF32 ? static_cast<const void*>(fld.f32)
+                                                                          : static_cast<const void*>(fld.b16)) +
+                         lay.vec_base[group];
+        const unsigned below = (1u << lane) - 1u;  // lanes stored before this one in a pack
         // Gathered voxel: source + offset (adjoint) or target - offset (forward).  A 32-bit index
         // (one wide multiply-add per address); the sum wraps only on padding steps (w = 0),
         // whose loads are predicated off, since voxel indices stay below INT_MAX.
         auto gather_index = [&](int o) { return (int)((unsigned)s + (unsigned)o); };
-        if constexpr (kBase == kFieldBF16) {
-            // bf16 form: each lane loads its own 8-byte vectors straight from HBM (a warp's loads
-            // of one pack coalesce into 256 contiguous bytes) one batch ahead of their use.  This
-            // form is bound by L1 wavefronts, not bytes, and skipping the shared-memory ring
-            // (its copies in and its reads out) measured 5 % faster than the TMA stream.
-            const uint2* vec = reinterpret_cast<const uint2*>(fld.b16) + e0 / kPack + lane;
-            auto load_vec = [&](int P) {
-                uint2 x = make_uint2(0u, 0u);
-                if (P < n_packs) x = ld_stream(vec + (size_t)P * kLanes);
-                return x;
-            };
-            auto desc_at = [&](int P) { return P < n_packs ? __ldg(desc + P) : 0; };
-            int4 tn[kBatch];
-            uint2 wn[kBatch];
-            int dq[kBatch];
-#pragma unroll
-            for (int k = 0; k < kBatch; ++k) wn[k] = load_vec(k);
-#pragma unroll
-            for (int k = 0; k < kBatch; ++k) tn[k] = __ldg(reinterpret_cast<const int4*>(tmpl + desc_at(k)));
-#pragma unroll
-            for (int k = 0; k < kBatch; ++k) dq[k] = desc_at(kBatch + k);
-            for (int P0 = 0; P0 < n_packs; P0 += kBatch) {
-                int o[kBatch * kPack];
-                float w[kBatch * kPack];
-                int4 tc[kBatch];
-                uint2 wc[kBatch];
-#pragma unroll
-                for (int k = 0; k < kBatch; ++k) tc[k] = tn[k], wc[k] = wn[k];
-#pragma unroll
-                for (int k = 0; k < kBatch; ++k) tn[k] = __ldg(reinterpret_cast<const int4*>(tmpl + dq[k]));
-#pragma unroll
-                for (int k = 0; k < kBatch; ++k) wn[k] = load_vec(P0 + kBatch + k);
-#pragma unroll
-                for (int k = 0; k < kBatch; ++k) dq[k] = desc_at(P0 + 2 * kBatch + k);
-#pragma unroll
-                for (int k = 0; k < kBatch; ++k) {
-                    o[k * kPack] = tc[k].x, o[k * kPack + 1] = tc[k].y, o[k * kPack + 2] = tc[k].z, o[k * kPack + 3] = tc[k].w;
-                    w[k * kPack] = __uint_as_float(wc[k].x << 16), w[k * kPack + 1] = __uint_as_float(wc[k].x & 0xffff0000u);
-                    w[k * kPack + 2] = __uint_as_float(wc[k].y << 16), w[k * kPack + 3] = __uint_as_float(wc[k].y & 0xffff0000u);
-                }
-                if constexpr (OP == Op::Adjoint || kGatherT) {
-                    float v[kBatch * kPack];
-#pragma unroll
-                    for (int u = 0; u < kBatch * kPack; ++u) v[u] = w[u] > 0.0f ? __ldg(a.in + gather_index(o[u])) : 0.0f;
-#pragma unroll
-                    for (int u = 0; u < kBatch * kPack; ++u) acc = fmaf(w[u], v[u], acc);
-                } else {
-#pragma unroll
-                    for (int u = 0; u < kBatch * kPack; ++u)
-                        if (live && w[u] > 0.0f) deposit(s + o[u], w[u]);
-                }
+        auto desc_at = [&](int P) { return P < n_packs ? __ldg(desc + P) : 0; };
+        auto mask_at = [&](int P) { return P < n_packs ? __ldg(mask + P) : 0u; };
+        int off = 0;  // running vector offset of the next pack to load (the same in every lane)
+        auto load_vec = [&](unsigned m) {
+            Vec x;
+            if constexpr (kBase == kFieldF32) x = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            else x = make_uint2(0u, 0u);
+            if ((m >> lane) & 1u) x = ld_stream(vec + off + __popc(m & below));
+            off += __popc(m);
+            return x;
+        };
+        auto unpack = [](const Vec& x, float* w) {
+            if constexpr (kBase == kFieldF32) {
+                w[0] = x.x, w[1] = x.y, w[2] = x.z, w[3] = x.w;
+            } else {
+                w[0] = __uint_as_float(x.x << 16), w[1] = __uint_as_float(x.x & 0xffff0000u);
+                w[2] = __uint_as_float(x.y << 16), w[3] = __uint_as_float(x.y & 0xffff0000u);
             }
-        } else {
-            unsigned char* ring = dyn_smem + (size_t)warp * kStages * kChunk;
-            const char* src_bytes = (kBase == kFieldF32 ? reinterpret_cast<const char*>(fld.f32)
-                                                        : reinterpret_cast<const char*>(fld.b16)) + e0 * kElem;
-            const long long total = (e1 - e0) * kElem;
-            const int n_chunks = (n_packs + kPacksPerChunk - 1) / kPacksPerChunk;
-            auto issue = [&](int c) {  // lane 0 only
-                const int stage = c % kStages;
-                const unsigned bytes = (unsigned)min((long long)kChunk, total - (long long)c * kChunk);
-                mbar_expect_tx(&bars[stage], bytes);
-                bulk_copy_g2s(ring + stage * kChunk, src_bytes + (long long)c * kChunk, bytes, &bars[stage]);
-            };
-            if (lane == 0) {
-                for (int k = 0; k < kStages; ++k) mbar_init(&bars[k], 1);
-                fence_mbarrier_init();
-                for (int c = 0; c < n_chunks && c < kStages; ++c) issue(c);
+        };
+        int4 tn[kBatch];
+        Vec wn[kBatch];
+        int dq[kBatch];
+        unsigned mq[kBatch];
+#pragma unroll
+        for (int k = 0; k < kBatch; ++k) wn[k] = load_vec(mask_at(k));
+#pragma unroll
+        for (int k = 0; k < kBatch; ++k) tn[k] = __ldg(reinterpret_cast<const int4*>(tmpl + desc_at(k)));
+#pragma unroll
+        for (int k = 0; k < kBatch; ++k) dq[k] = desc_at(kBatch + k), mq[k] = mask_at(kBatch + k);
+        for (int P0 = 0; P0 < n_packs; P0 += kBatch) {
+            int o[kBatch * kPack];
+            float w[kBatch * kPack];
+            int4 tc[kBatch];
+            Vec wc[kBatch];
+#pragma unroll
+            for (int k = 0; k < kBatch; ++k) tc[k] = tn[k], wc[k] = wn[k];
+#pragma unroll
+            for (int k = 0; k < kBatch; ++k) tn[k] = __ldg(reinterpret_cast<const int4*>(tmpl + dq[k]));
+#pragma unroll
+            for (int k = 0; k < kBatch; ++k) wn[k] = load_vec(mq[k]);
+#pragma unroll
+            for (int k = 0; k < kBatch; ++k) dq[k] = desc_at(P0 + 2 * kBatch + k), mq[k] = mask_at(P0 + 2 * kBatch + k);
+#pragma unroll
+            for (int k = 0; k < kBatch; ++k) {
+                o[k * kPack] = tc[k].x, o[k * kPack + 1] = tc[k].y, o[k * kPack + 2] = tc[k].z, o[k * kPack + 3] = tc[k].w;
+                unpack(wc[k], w + k * kPack);
             }
-            __syncwarp();
-            static_assert(kPacksPerChunk % kBatch == 0, "batches stay inside a chunk");
-            auto desc_at = [&](int P) { return P < n_packs ? __ldg(desc + P) : 0; };
-            int4 tn[kBatch];
-            int dq[kBatch];
-    #pragma unroll
-            for (int k = 0; k < kBatch; ++k) tn[k] = __ldg(reinterpret_cast<const int4*>(tmpl + desc_at(k)));
-    #pragma unroll
-            for (int k = 0; k < kBatch; ++k) dq[k] = desc_at(kBatch + k);
-            bool ok = true;
-            for (int c = 0; c < n_chunks; ++c) {
-                const int packs = min(kPacksPerChunk, n_packs - c * kPacksPerChunk);
-                const int stage = c % kStages;
-                if (!mbar_wait_bounded(&bars[stage], (c / kStages) & 1)) {
-                    ok = false;
-                    break;
+            if constexpr (OP == Op::Adjoint || kGatherT) {
+                float v[kBatch * kPack];
+#pragma unroll
+                for (int u = 0; u < kBatch * kPack; ++u) {
+                    if constexpr (half_volume(FAR_MODE))
+                        v[u] = w[u] > 0.0f ? __bfloat162float(__ldg(a.in16 + gather_index(o[u]))) : 0.0f;
+                    else
+                        v[u] = w[u] > 0.0f ? __ldg(a.in + gather_index(o[u])) : 0.0f;
                 }
-                const unsigned char* chunk = ring + stage * kChunk;
-                for (int b = 0; b < packs; b += kBatch) {
-                    const int P0 = c * kPacksPerChunk + b;
-                    int o[kBatch * kPack];
-                    float w[kBatch * kPack];
-                    int4 tc[kBatch];
-    #pragma unroll
-                    for (int k = 0; k < kBatch; ++k) tc[k] = tn[k];
-    #pragma unroll
-                    for (int k = 0; k < kBatch; ++k) tn[k] = __ldg(reinterpret_cast<const int4*>(tmpl + dq[k]));
-    #pragma unroll
-                    for (int k = 0; k < kBatch; ++k) dq[k] = desc_at(P0 + 2 * kBatch + k);
-    #pragma unroll
-                    for (int k = 0; k < kBatch; ++k) {
-                        const bool here = b + k < packs;
-                        const int4 t = tc[k];
-                        o[k * kPack] = t.x, o[k * kPack + 1] = t.y, o[k * kPack + 2] = t.z, o[k * kPack + 3] = t.w;
-                        if constexpr (kBase == kFieldF32) {
-                            const float4 x = here ? reinterpret_cast<const float4*>(chunk + (b + k) * kPackBytes)[lane]
-                                                  : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-                            w[k * kPack] = x.x, w[k * kPack + 1] = x.y, w[k * kPack + 2] = x.z, w[k * kPack + 3] = x.w;
-                        } else {
-                            const uint2 x = here ? reinterpret_cast<const uint2*>(chunk + (b + k) * kPackBytes)[lane]
-                                                 : make_uint2(0u, 0u);
-                            w[k * kPack] = __uint_as_float(x.x << 16), w[k * kPack + 1] = __uint_as_float(x.x & 0xffff0000u);
-                            w[k * kPack + 2] = __uint_as_float(x.y << 16), w[k * kPack + 3] = __uint_as_float(x.y & 0xffff0000u);
-                        }
-                    }
-                    if constexpr (OP == Op::Adjoint || kGatherT) {
-                        float v[kBatch * kPack];
-    #pragma unroll
-                        for (int u = 0; u < kBatch * kPack; ++u) v[u] = w[u] > 0.0f ? __ldg(a.in + gather_index(o[u])) : 0.0f;
-    #pragma unroll
-                        for (int u = 0; u < kBatch * kPack; ++u) acc = fmaf(w[u], v[u], acc);
-                    } else {
-    #pragma unroll
-                        for (int u = 0; u < kBatch * kPack; ++u)
-                            if (live && w[u] > 0.0f) deposit(s + o[u], w[u]);
-                    }
-                }
-                __syncwarp();
-                if (lane == 0 && c + kStages < n_chunks) {
-                    fence_proxy_async();  // this stage's reads precede the copy that overwrites it
-                    issue(c + kStages);
-                }
-            }
-            if (!ok) {
-                // A copy did not complete in time: report it, and give the copies still in flight
-                // a bounded chance to land before this warp's shared memory is released.
-                if (lane == 0) {
-                    atomicOr(a.error, 1u);
-                    for (int k = 0; k < kStages; ++k) {
-                        mbar_wait_bounded(&bars[k], 0);
-                        mbar_wait_bounded(&bars[k], 1);
-                    }
-                }
-                __syncwarp();
+#pragma unroll
+                for (int u = 0; u < kBatch * kPack; ++u) acc = fmaf(w[u], v[u], acc);
+            } else {
+#pragma unroll
+                for (int u = 0; u < kBatch * kPack; ++u)
+                    if (live && w[u] > 0.0f) deposit(s + o[u], w[u]);
             }
         }
     }
@@ -577,20 +502,30 @@ __device__ __forceinline__ void project_group(const ProjParams& p, const OpArgs&
     } else if constexpr (OP == Op::Adjoint) {
         if (live) a.out[s] = acc / __ldg(a.W + src);  // prc.cu:266
     } else if constexpr (OP == Op::Forward) {
-        if (FAR_MODE >= kFieldF32T && valid) a.out[s] = acc;
+        if (target_major(FAR_MODE) && valid) {
+            // inside MAP-EM the EM ratio of the tissue voxel is taken here (prc.cu:270-274)
+            if constexpr (half_volume(FAR_MODE))
+                a.out16[s] = __float2bfloat16_rn(__ldg(a.ratio_g + s) / fmaxf(acc, __ldg(a.ratio_eps)));
+            else
+                a.out[s] = a.ratio_g ? __ldg(a.ratio_g + s) / fmaxf(acc, __ldg(a.ratio_eps)) : acc;
+        }
     } else if constexpr (OP == Op::Count) {
         for (int off = 16; off > 0; off >>= 1) cnt += __shfl_xor_sync(kFull, cnt, off);
         if (lane == 0) atomicAdd(a.count, cnt);
     }
 }
 
+// Stored-field launches are held to the registers of PRC_FIELD_MIN_BLOCKS blocks of 256 threads
+// per SM (4: 64 registers): the gather stream needs warps in flight more than registers.
+#ifndef PRC_FIELD_MIN_BLOCKS
+#define PRC_FIELD_MIN_BLOCKS 4
+#endif
 template <Op OP, bool EXACT, int NEAR_MODE, int FAR_MODE>
-__global__ void __launch_bounds__(kMaxBlock) project_kernel(const ProjParams p, const OpArgs a) {
+__global__ void __launch_bounds__(kMaxBlock, FAR_MODE == kMarch ? 1 : PRC_FIELD_MIN_BLOCKS)
+    project_kernel(const ProjParams p, const OpArgs a) {
     extern __shared__ __align__(128) unsigned char dyn_smem[];
-    __shared__ uint64_t field_bars[kMaxWarps][kStages];
     const int warp = threadIdx.x >> 5;
-    project_group<OP, EXACT, NEAR_MODE, FAR_MODE>(p, a, blockIdx.x * (blockDim.x >> 5) + warp, warp, dyn_smem,
-                                                  field_bars[warp]);
+    project_group<OP, EXACT, NEAR_MODE, FAR_MODE>(p, a, blockIdx.x * (blockDim.x >> 5) + warp, warp, dyn_smem);
 }
 
 // Batched launch over many volumes: block b belongs to the item (volume) whose first_block is
@@ -598,7 +533,6 @@ __global__ void __launch_bounds__(kMaxBlock) project_kernel(const ProjParams p, 
 template <Op OP>
 __global__ void __launch_bounds__(kMaxBlock) project_batch_kernel(const BatchItem* items, int n_items) {
     extern __shared__ __align__(128) unsigned char dyn_smem[];
-    __shared__ uint64_t field_bars[kMaxWarps][kStages];
     int lo = 0, hi = n_items - 1;
     while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
@@ -610,15 +544,14 @@ __global__ void __launch_bounds__(kMaxBlock) project_batch_kernel(const BatchIte
     const int mode = items[lo].mode;
     const int warp = threadIdx.x >> 5;
     const int group = ((int)blockIdx.x - items[lo].first_block) * (blockDim.x >> 5) + warp;
-    uint64_t* bars = field_bars[warp];
     switch (mode) {
-        case kBatchTraceMarch: project_group<OP, false, kTraceNear, kMarch>(p, a, group, warp, dyn_smem, bars); break;
-        case kBatchCacheF32March: project_group<OP, false, kCacheF32, kMarch>(p, a, group, warp, dyn_smem, bars); break;
-        case kBatchCacheBF16March: project_group<OP, false, kCacheBF16, kMarch>(p, a, group, warp, dyn_smem, bars); break;
-        case kBatchFieldF32: project_group<OP, false, kTraceNear, kFieldF32>(p, a, group, warp, dyn_smem, bars); break;
-        case kBatchFieldBF16: project_group<OP, false, kTraceNear, kFieldBF16>(p, a, group, warp, dyn_smem, bars); break;
-        case kBatchFieldF32T: project_group<OP, false, kTraceNear, kFieldF32T>(p, a, group, warp, dyn_smem, bars); break;
-        case kBatchFieldBF16T: project_group<OP, false, kTraceNear, kFieldBF16T>(p, a, group, warp, dyn_smem, bars); break;
+        case kBatchTraceMarch: project_group<OP, false, kTraceNear, kMarch>(p, a, group, warp, dyn_smem); break;
+        case kBatchCacheF32March: project_group<OP, false, kCacheF32, kMarch>(p, a, group, warp, dyn_smem); break;
+        case kBatchCacheBF16March: project_group<OP, false, kCacheBF16, kMarch>(p, a, group, warp, dyn_smem); break;
+        case kBatchFieldF32: project_group<OP, false, kTraceNear, kFieldF32>(p, a, group, warp, dyn_smem); break;
+        case kBatchFieldBF16: project_group<OP, false, kTraceNear, kFieldBF16>(p, a, group, warp, dyn_smem); break;
+        case kBatchFieldF32T: project_group<OP, false, kTraceNear, kFieldF32T>(p, a, group, warp, dyn_smem); break;
+        case kBatchFieldBF16T: project_group<OP, false, kTraceNear, kFieldBF16T>(p, a, group, warp, dyn_smem); break;
         default: break;
     }
 }
@@ -652,6 +585,70 @@ __global__ void desc_kernel(const ProjParams p, const StreamLayout l, int* desc)
     int* out = desc + l.group_base[group] / (kPack * kLanes);
     for (int row = 0; row < p.n_rows; ++row)
         for (int m = 0; m < len[row]; m += kPack) *out++ = row * p.tmpl_len + m;
+}
+
+// Compaction masks: one warp per group walks its packs; lane l's vector of pack P is kept when
+// any of its 4 weights is nonzero (bit patterns: stored weights are positive or +0).
+template <int FAR_MODE>
+__global__ void __launch_bounds__(kBlock) field_mask_kernel(const ProjParams p, const StreamLayout l, const FarField f,
+                                                            unsigned* mask, long long* group_vecs) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int group = blockIdx.x * kWarps + warp;
+    if (group * kLanes >= p.n_active) return;
+    const long long e0 = l.group_base[group], e1 = l.group_base[group + 1];
+    const long long pk0 = e0 / (kPack * kLanes);
+    const int n = (int)((e1 - e0) / (kPack * kLanes));
+    long long kept = 0;
+    for (int P = 0; P < n; ++P) {
+        const size_t v = (size_t)(e0 / kPack) + (size_t)P * kLanes + lane;
+        bool any;
+        if constexpr (FAR_MODE == kFieldF32) {
+            const uint4 x = reinterpret_cast<const uint4*>(f.f32)[v];
+            any = (x.x | x.y | x.z | x.w) != 0u;
+        } else {
+            const uint2 x = reinterpret_cast<const uint2*>(f.b16)[v];
+            any = (x.x | x.y) != 0u;
+        }
+        const unsigned m = __ballot_sync(kFull, any);
+        if (lane == 0) mask[pk0 + P] = m;
+        kept += __popc(m);
+    }
+    if (lane == 0) group_vecs[group] = kept;
+}
+
+// Moves every kept vector to its compacted place (the new stream is a separate allocation).
+template <int FAR_MODE>
+__global__ void __launch_bounds__(kBlock) field_compact_kernel(const ProjParams p, const StreamLayout l,
+                                                               const FarField from, const FarField to) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int group = blockIdx.x * kWarps + warp;
+    if (group * kLanes >= p.n_active) return;
+    const long long e0 = l.group_base[group], e1 = l.group_base[group + 1];
+    const long long pk0 = e0 / (kPack * kLanes);
+    const int n = (int)((e1 - e0) / (kPack * kLanes));
+    const unsigned below = (1u << lane) - 1u;
+    long long out = l.vec_base[group];
+    for (int P = 0; P < n; ++P) {
+        const unsigned m = l.mask[pk0 + P];
+        if ((m >> lane) & 1u) {
+            const size_t v = (size_t)(e0 / kPack) + (size_t)P * kLanes + lane;
+            const size_t w = (size_t)out + __popc(m & below);
+            if constexpr (FAR_MODE == kFieldF32) reinterpret_cast<uint4*>(to.f32)[w] = reinterpret_cast<const uint4*>(from.f32)[v];
+            else reinterpret_cast<uint2*>(to.b16)[w] = reinterpret_cast<const uint2*>(from.b16)[v];
+        }
+        out += __popc(m);
+    }
+}
+
+// The layout of an uncompacted stream in compacted terms: every lane kept.
+__global__ void field_identity_kernel(const ProjParams p, const StreamLayout l, unsigned* mask, long long* vec_base,
+                                      int n_groups) {
+    const int group = blockIdx.x * blockDim.x + threadIdx.x;
+    if (group > n_groups) return;
+    vec_base[group] = l.group_base[group] / kPack;
+    if (group == n_groups) return;
+    const long long p0 = l.group_base[group] / (kPack * kLanes), p1 = l.group_base[group + 1] / (kPack * kLanes);
+    for (long long P = p0; P < p1; ++P) mask[P] = kFull;
 }
 
 // Walks every stored source-major entry w > 0 of a group (lane = source s, template row k,
@@ -707,6 +704,92 @@ __global__ void forward_prep_kernel(const int* __restrict__ vox2src, const float
             out[i] = 0.0f;
         }
         u[i] = scale > 0.0f ? scale : 0.0f;
+    }
+}
+
+// forward_prep with the Biggs-Andrews prediction of the same voxels folded in: one pass reads f
+// and prev, writes y, and prepares u = y / W for the gather (four voxels per step when every
+// pointer is 16-byte aligned; each voxel computed by the same expressions either way).
+__global__ void forward_prep_extrapolate_kernel(const int* __restrict__ vox2src, const float* __restrict__ W,
+                                                const float* __restrict__ f, const float* __restrict__ prev,
+                                                const float* __restrict__ lambda_p, float* __restrict__ y,
+                                                float* __restrict__ u, float* __restrict__ out, size_t n) {
+    const float lambda = __ldg(lambda_p);
+    auto one = [&](size_t i, float fi, float pi, int src, float& yi, float& ui) {
+        yi = fmaxf(fi + lambda * (fi - pi), 0.5f * fi);  // prc.cu:320
+        float scale = 0.0f;
+        if (src >= 0) {
+            const float ws = __ldg(W + src);
+            scale = ws > 0.0f ? yi / ws : 0.0f;  // prc.cu:246
+        } else {
+            out[i] = 0.0f;
+        }
+        ui = scale > 0.0f ? scale : 0.0f;
+    };
+    const bool vec = ((uintptr_t)f | (uintptr_t)prev | (uintptr_t)y | (uintptr_t)u | (uintptr_t)vox2src) % 16 == 0;
+    const size_t n4 = vec ? n / 4 : 0;
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n4; q += stride) {
+        const float4 a = reinterpret_cast<const float4*>(f)[q], b = reinterpret_cast<const float4*>(prev)[q];
+        const int4 s4 = reinterpret_cast<const int4*>(vox2src)[q];
+        float4 yv, uv;
+        one(4 * q, a.x, b.x, s4.x, yv.x, uv.x);
+        one(4 * q + 1, a.y, b.y, s4.y, yv.y, uv.y);
+        one(4 * q + 2, a.z, b.z, s4.z, yv.z, uv.z);
+        one(4 * q + 3, a.w, b.w, s4.w, yv.w, uv.w);
+        reinterpret_cast<float4*>(y)[q] = yv;
+        reinterpret_cast<float4*>(u)[q] = uv;
+    }
+    for (size_t i = 4 * n4 + blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += stride) {
+        float yi, ui;
+        one(i, f[i], prev[i], vox2src[i], yi, ui);
+        y[i] = yi;
+        u[i] = ui;
+    }
+}
+
+// The preparation of the mixed-precision form: the same prediction (PREDICT) and u = y / W, with
+// u rounded to bf16 for the bf16 gather.  Every voxel's expressions are those of
+// forward_prep_extrapolate_kernel; u16 is 0 off the support.
+template <bool PREDICT>
+__global__ void forward_prep_half_kernel(const int* __restrict__ vox2src, const float* __restrict__ W,
+                                         const float* __restrict__ f, const float* __restrict__ prev,
+                                         const float* __restrict__ lambda_p, float* __restrict__ y,
+                                         __nv_bfloat16* __restrict__ u16, size_t n) {
+    const float lambda = PREDICT ? __ldg(lambda_p) : 0.0f;
+    auto one = [&](float fi, float pi, int src, float& yi) {
+        yi = PREDICT ? fmaxf(fi + lambda * (fi - pi), 0.5f * fi) : fi;  // prc.cu:320
+        float scale = 0.0f;
+        if (src >= 0) {
+            const float ws = __ldg(W + src);
+            scale = ws > 0.0f ? yi / ws : 0.0f;  // prc.cu:246
+        }
+        return __float2bfloat16_rn(scale > 0.0f ? scale : 0.0f);
+    };
+    const bool vec = ((uintptr_t)f | (uintptr_t)prev | (uintptr_t)y | (uintptr_t)vox2src) % 16 == 0 &&
+                     (uintptr_t)u16 % 8 == 0;
+    const size_t n4 = vec ? n / 4 : 0;
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n4; q += stride) {
+        const float4 a = reinterpret_cast<const float4*>(f)[q];
+        const float4 b = PREDICT ? reinterpret_cast<const float4*>(prev)[q] : a;
+        const int4 s4 = reinterpret_cast<const int4*>(vox2src)[q];
+        float4 yv;
+        __nv_bfloat162 lo, hi;
+        lo.x = one(a.x, b.x, s4.x, yv.x);
+        lo.y = one(a.y, b.y, s4.y, yv.y);
+        hi.x = one(a.z, b.z, s4.z, yv.z);
+        hi.y = one(a.w, b.w, s4.w, yv.w);
+        if (PREDICT) reinterpret_cast<float4*>(y)[q] = yv;
+        uint2 packed;
+        packed.x = *reinterpret_cast<const unsigned*>(&lo);
+        packed.y = *reinterpret_cast<const unsigned*>(&hi);
+        reinterpret_cast<uint2*>(u16)[q] = packed;
+    }
+    for (size_t i = 4 * n4 + blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += stride) {
+        float yi;
+        u16[i] = one(f[i], PREDICT ? prev[i] : f[i], vox2src[i], yi);
+        if (PREDICT) y[i] = yi;
     }
 }
 
@@ -886,9 +969,8 @@ cudaError_t launch(const ProjParams& p, const OpArgs& a, cudaStream_t s) {
     const int blocks = (groups + kWarps - 1) / kWarps;
     if (blocks == 0) return cudaSuccess;
     size_t smem = 0;
-    // The ring (the near block is in the field).  The bf16 form reads HBM directly yet keeps the
-    // allocation: launched without it (and so with the largest L1 carveout) it measured 1.7-2x
-    // slower on the 128x128x159 torso.
+    // The stored field (near block included) reads HBM directly; its launches reserve shared
+    // memory only to set the L1 split (kFieldSmemPerWarp).
     if (FAR_MODE != kMarch) smem = kFieldSmemBytes;
     else if (NEAR_MODE == kTraceNear && OP != Op::Layout)
         smem = OP == Op::Norm && a.near_acc ? size_t(kWarps) * 27 * kLanes * sizeof(float) : kNearSmemBytes;
@@ -908,6 +990,13 @@ cudaError_t launch_modes(const ProjParams& p, const OpArgs& a, bool trace_near, 
             return a.near.b16 ? launch<OP, EXACT, kCacheBF16, kMarch>(p, a, s) : launch<OP, EXACT, kCacheF32, kMarch>(p, a, s);
         return launch<OP, EXACT, kTraceNear, kMarch>(p, a, s);
     } else {
+        if constexpr (OP == Op::Forward || OP == Op::Adjoint) {
+            if (a.in16) {  // bf16 volumes inside MAP-EM (the bf16 field only)
+                if (OP == Op::Forward && a.farT.b16 && a.out16) return launch<OP, EXACT, kTraceNear, kFieldBF16TH>(p, a, s);
+                if (OP == Op::Adjoint && a.far.b16) return launch<OP, EXACT, kTraceNear, kFieldBF16H>(p, a, s);
+                return cudaErrorInvalidValue;
+            }
+        }
         if (OP == Op::Forward && a.farT.f32) return launch<OP, EXACT, kTraceNear, kFieldF32T>(p, a, s);
         if (OP == Op::Forward && a.farT.b16) return launch<OP, EXACT, kTraceNear, kFieldBF16T>(p, a, s);
         if (a.far.f32) return launch<OP, EXACT, kTraceNear, kFieldF32>(p, a, s);
@@ -954,6 +1043,31 @@ cudaError_t build_descriptors(const ProjParams& p, const StreamLayout& l, int* d
     return cudaGetLastError();
 }
 
+cudaError_t field_masks(const ProjParams& p, const StreamLayout& l, const FarField& f, unsigned* mask,
+                        long long* group_vecs, cudaStream_t s) {
+    const int groups = (p.n_active + kLanes - 1) / kLanes;
+    if (groups == 0) return cudaSuccess;
+    if (f.f32) field_mask_kernel<kFieldF32><<<(groups + kWarps - 1) / kWarps, kBlock, 0, s>>>(p, l, f, mask, group_vecs);
+    else field_mask_kernel<kFieldBF16><<<(groups + kWarps - 1) / kWarps, kBlock, 0, s>>>(p, l, f, mask, group_vecs);
+    return cudaGetLastError();
+}
+
+cudaError_t field_compact(const ProjParams& p, const StreamLayout& l, const FarField& from, const FarField& to,
+                          cudaStream_t s) {
+    const int groups = (p.n_active + kLanes - 1) / kLanes;
+    if (groups == 0) return cudaSuccess;
+    if (from.f32) field_compact_kernel<kFieldF32><<<(groups + kWarps - 1) / kWarps, kBlock, 0, s>>>(p, l, from, to);
+    else field_compact_kernel<kFieldBF16><<<(groups + kWarps - 1) / kWarps, kBlock, 0, s>>>(p, l, from, to);
+    return cudaGetLastError();
+}
+
+cudaError_t field_identity_layout(const ProjParams& p, const StreamLayout& l, unsigned* mask, long long* vec_base,
+                                  cudaStream_t s) {
+    const int groups = (p.n_active + kLanes - 1) / kLanes;
+    field_identity_kernel<<<(groups + 1 + 127) / 128, 128, 0, s>>>(p, l, mask, vec_base, groups);
+    return cudaGetLastError();
+}
+
 cudaError_t transpose_lengths(const ProjParams& p, const FarField& far, int* len_t32, cudaStream_t s) {
     const int groups = (p.n_active + kLanes - 1) / kLanes;
     if (groups == 0) return cudaSuccess;
@@ -977,11 +1091,26 @@ cudaError_t forward_prep(const ProjParams& p, const float* W, const float* f, fl
     return cudaGetLastError();
 }
 
+cudaError_t forward_prep_extrapolate(const ProjParams& p, const float* W, const float* f, const float* prev,
+                                     const float* lambda, float* y, float* u, float* out, cudaStream_t s) {
+    const size_t n = (size_t)p.nxy * p.g.nz;
+    forward_prep_extrapolate_kernel<<<592, 256, 0, s>>>(p.vox2src, W, f, prev, lambda, y, u, out, n);
+    return cudaGetLastError();
+}
+
+cudaError_t forward_prep_half(const ProjParams& p, const float* W, const float* f, const float* prev,
+                              const float* lambda, float* y, __nv_bfloat16* u16, cudaStream_t s) {
+    const size_t n = (size_t)p.nxy * p.g.nz;
+    if (lambda) forward_prep_half_kernel<true><<<592, 256, 0, s>>>(p.vox2src, W, f, prev, lambda, y, u16, n);
+    else forward_prep_half_kernel<false><<<592, 256, 0, s>>>(p.vox2src, W, f, prev, lambda, y, u16, n);
+    return cudaGetLastError();
+}
+
 int near_row_steps() { return kNearRow; }
 
 size_t batch_smem_per_warp(int mode) {
     if (mode == kBatchTraceMarch) return (size_t)kNear * kLanes * sizeof(float);
-    if (mode >= kBatchFieldF32) return (size_t)kStages * kChunk;
+    if (mode >= kBatchFieldF32) return kFieldSmemPerWarp;
     return 0;
 }
 
