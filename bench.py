@@ -979,6 +979,10 @@ def batch_record(frames: int, iterations: int, steps: int, warmup: int, surrogat
     clock_info = sampler.stop() if sampler else None
     ms = e0.elapsed_time(e1)
     frames_per_s = frames * steps / (ms / 1e3)
+    # the launch structure: one graph replay against the same launches made one by one
+    prof = batch.profile(gs, outs, iterations, BETA, GAMMA, True)
+    prof["gap_ms"] = round(prof["graph_ms"] - prof["launches_ms"], 4)
+    prof["gap_share"] = round(prof["gap_ms"] / prof["graph_ms"], 5)
     # per-frame NRMSE against the plain method (fp32 weights, reference numerics), first 4 frames
     nrmse_list = []
     for i in range(min(4, frames)):
@@ -999,7 +1003,10 @@ def batch_record(frames: int, iterations: int, steps: int, warmup: int, surrogat
                       "projector_forms": {str(k): v for k, v in modes.items()},
                       "surrogate": bool(net), "autotuned": {"warps_per_block": batch.warps},
                       "setup_s": round(setup_s, 2)},
-           "nrmse_vs_plain_first_frames": nrmse_list}
+           "nrmse_vs_plain_first_frames": nrmse_list,
+           "schedule": {"what": "one CUDA-graph replay of the run vs the same kernel launches timed one by one "
+                                "with CUDA events; the gap bounds what one persistent kernel per iteration could save",
+                        **{k: (round(v, 4) if isinstance(v, float) else v) for k, v in prof.items()}}}
     if clock_info:
         rec["clocks"] = clock_info
     batch.close()

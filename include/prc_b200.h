@@ -58,9 +58,10 @@ enum {
 /* Source tiles of the stored coefficient field: a warp owns 32 tissue voxels taken in tiles
  * of this shape (x fastest inside a tile, tiles in x, y, z order), so every gather of one step
  * touches the rows of one tile shifted by the step's offset.  PRC_TILE_AUTO lets the engine
- * choose (an autotuner that times the candidate shapes on the handle's own field, remembered
- * per grid, isotope and form for the rest of the process).  The shape changes no result:
- * every source keeps its own weights and summation order. */
+ * choose: an autotuner builds the field of a central slab of the volume with each candidate
+ * shape, times a forward and an adjoint projection, and remembers the fastest per grid,
+ * isotope and form for the rest of the process.  The shape changes no result: every source
+ * keeps its own weights and summation order. */
 enum {
     PRC_TILE_AUTO = 0,
     PRC_TILE_8x2x2 = 1,
@@ -225,6 +226,15 @@ int prc_batch_em_run(prc_batch* b, const float* const* d_g, float* const* d_out,
                      float gamma, int accelerate);
 int prc_batch_synchronize(prc_batch* b);
 void* prc_batch_stream(const prc_batch* b);
+/* The measurement behind the schedule's design (no counterpart in the reference): runs the
+ * MAP-EM schedule of prc_batch_em_run with these arguments as one replay of its captured CUDA
+ * graph (*graph_ms, device time) and once more launch by launch with CUDA events around every
+ * kernel launch (*launches_ms, the sum over its *launches launches).  graph_ms - launches_ms
+ * bounds what fusing the phases of an iteration into one persistent kernel could save.
+ * Synchronises. */
+int prc_batch_profile(prc_batch* b, const float* const* d_g, float* const* d_out, int iterations, float beta,
+                      float gamma, int accelerate, double* graph_ms, double* launches_ms, int* launches);
+
 /* The handle of frame i (owned by the batch), and the autotuned warps per block. */
 int prc_batch_frame(prc_batch* b, int i, prc_handle** out);
 int prc_batch_warps(const prc_batch* b);

@@ -100,6 +100,9 @@ _SIGNATURES = {
     "prc_batch_stream": (_P, [_P]),
     "prc_batch_frame": (ctypes.c_int, [_P, ctypes.c_int, ctypes.POINTER(_P)]),
     "prc_batch_warps": (ctypes.c_int, [_P]),
+    "prc_batch_profile": (ctypes.c_int, [_P, _P, _P, ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_int,
+                                         ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
+                                         ctypes.POINTER(ctypes.c_int)]),
     "prc_nn_gemm_bf16": (ctypes.c_int, [_P, _P, _P, ctypes.c_int, ctypes.c_int, ctypes.c_int, _P, _P]),
     "prc_nn_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(_P)]),
     "prc_nn_destroy": (None, [_P]),
@@ -410,6 +413,18 @@ class Batch:
         g = (ctypes.c_void_p * n)(*[_ptr(x) for x in d_gs])
         o = (ctypes.c_void_p * n)(*[_ptr(x) for x in d_outs])
         _check(lib().prc_batch_em_run(self._h, g, o, iterations, beta, gamma, int(accelerate)))
+
+    def profile(self, d_gs, d_outs, iterations: int, beta: float = 0.2, gamma: float = 20.0,
+                accelerate: bool = True) -> dict:
+        """Device time of one graph replay of the run and the summed device time of the same
+        launches made one by one (prc_batch_profile)."""
+        n = len(d_gs)
+        g = (ctypes.c_void_p * n)(*[_ptr(x) for x in d_gs])
+        o = (ctypes.c_void_p * n)(*[_ptr(x) for x in d_outs])
+        gm, lm, nl = ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
+        _check(lib().prc_batch_profile(self._h, g, o, iterations, beta, gamma, int(accelerate), ctypes.byref(gm),
+                                       ctypes.byref(lm), ctypes.byref(nl)))
+        return {"graph_ms": gm.value, "launches_ms": lm.value, "launches": nl.value}
 
     def synchronize(self) -> None:
         _check(lib().prc_batch_synchronize(self._h))

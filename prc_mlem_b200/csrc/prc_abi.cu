@@ -1390,12 +1390,23 @@ BatchPlan plan_batch(prc_batch* b, const float* const* d_g, float* const* d_out,
     return plan;
 }
 
+// Enqueues the schedule on the batch's stream.  With `timed`, every kernel launch (a MAP-EM
+// phase, a batched projection, a forward preparation) is bracketed by a pair of CUDA events
+// appended to it; memsets and copies are not.
 int enqueue_plan(prc_batch* b, const BatchPlan& plan, float* const* d_out, float beta, float gamma, bool accel,
-                 int warps) {
+                 int warps, std::vector<std::pair<cudaEvent_t, cudaEvent_t>>* timed = nullptr) {
     const unsigned char* base = static_cast<const unsigned char*>(b->d_tables);
     const int em_blocks = std::max(1, std::min(kReduceBlocks, 4096 / std::max(1, (int)b->frames.size())));
     for (const BatchPlan::Launch& l : plan.launches) {
         cudaError_t e = cudaSuccess;
+        const bool kernel = l.kind <= 2;
+        if (timed && kernel) {
+            std::pair<cudaEvent_t, cudaEvent_t> ev{nullptr, nullptr};
+            PRC_CUDA(cudaEventCreate(&ev.first));
+            PRC_CUDA(cudaEventCreate(&ev.second));
+            timed->push_back(ev);
+            PRC_CUDA(cudaEventRecord(ev.first, b->stream));
+        }
         switch (l.kind) {
             case 0:
                 e = em_batch_phase(l.phase, reinterpret_cast<const EmItem*>(base + l.offset), l.n_items, em_blocks, beta,
@@ -1418,6 +1429,7 @@ int enqueue_plan(prc_batch* b, const BatchPlan& plan, float* const* d_out, float
         }
         if (e != cudaSuccess) return fail(PRC_ERR_CUDA, std::string("CUDA error '") + cudaGetErrorString(e) +
                                                             "' in the batched MAP-EM schedule");
+        if (timed && kernel) PRC_CUDA(cudaEventRecord(timed->back().second, b->stream));
     }
     return PRC_OK;
 }
@@ -1617,6 +1629,42 @@ int prc_batch_em_run(prc_batch* b, const float* const* d_g, float* const* d_out,
     }
     PRC_CUDA(cudaGraphLaunch(b->exec, b->stream));
     return PRC_OK;
+}
+
+int prc_batch_profile(prc_batch* b, const float* const* d_g, float* const* d_out, int iterations, float beta,
+                      float gamma, int accelerate, double* graph_ms, double* launches_ms, int* launches) {
+    if (!graph_ms || !launches_ms || !launches) return fail(PRC_ERR_ARGUMENT, "Invalid argument");
+    int rc = prc_batch_em_run(b, d_g, d_out, iterations, beta, gamma, accelerate);  // tuned, captured, warm
+    if (rc != PRC_OK) return rc;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    PRC_CUDA(cudaEventCreate(&e0));
+    PRC_CUDA(cudaEventCreate(&e1));
+    PRC_CUDA(cudaEventRecord(e0, b->stream));
+    PRC_CUDA(cudaGraphLaunch(b->exec, b->stream));
+    PRC_CUDA(cudaEventRecord(e1, b->stream));
+    PRC_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.0f;
+    PRC_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *graph_ms = ms;
+    // the same schedule launch by launch (its tables are the graph's, uploaded again unchanged)
+    BatchPlan plan = plan_batch(b, d_g, d_out, iterations, beta, gamma, accelerate != 0, b->warps, false);
+    rc = upload_plan(b, plan);
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> timed;
+    if (rc == PRC_OK) rc = enqueue_plan(b, plan, d_out, beta, gamma, accelerate != 0, b->warps, &timed);
+    double sum = 0.0;
+    if (rc == PRC_OK) {
+        PRC_CUDA(cudaStreamSynchronize(b->stream));
+        for (auto& ev : timed) {
+            float t = 0.0f;
+            if (cudaEventElapsedTime(&t, ev.first, ev.second) == cudaSuccess) sum += t;
+        }
+    }
+    for (auto& ev : timed) cudaEventDestroy(ev.first), cudaEventDestroy(ev.second);
+    *launches_ms = sum;
+    *launches = (int)timed.size();
+    return rc;
 }
 
 int prc_batch_synchronize(prc_batch* b) {

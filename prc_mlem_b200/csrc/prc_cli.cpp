@@ -38,6 +38,7 @@ struct Settings {
     float beta = 0.2f, gamma = 20.0f, support_rho = 0.05f, air_cap_mm = 50.0f;
     bool reproject = false, trace_near_every_pass = false, exact_range = false, plain = false, bf16 = false;
     int cache = PRC_CACHE_FULL;
+    int tile = PRC_TILE_AUTO;
 };
 
 void print_usage(const char* prog, FILE* stream = stderr) {  // the usage text of prc.cu:461-484
@@ -61,6 +62,7 @@ void print_usage(const char* prog, FILE* stream = stderr) {  // the usage text o
             "  --no-accel        plain MAP-EM without Biggs-Andrews extrapolation (validation)\n"
             "  --cache MODE      none|near|source|full: weights kept on the GPU between passes (default full)\n"
             "  --bf16-weights    store the projector weights in bfloat16 (mixed precision)\n"
+            "  --tile SHAPE      auto|8x2x2|16x2x1|32x1x1|4x4x2|16x1x2: source tile of the stored field (default auto)\n"
             "Isotopes:",
             prog);
     for (int i = 0; i < prc_isotope_count(); ++i) fprintf(stream, " %s", prc_isotope_name(i));
@@ -126,6 +128,15 @@ const Spec kSpecs[] = {
          for (const auto& m : modes)
              if (!strcmp(v, m.first)) s.cache = m.second;
      }},
+    {"--tile", true,
+     [](Settings& s, const char* v, const char*) {
+         static const std::pair<const char*, int> shapes[] = {{"auto", PRC_TILE_AUTO},     {"8x2x2", PRC_TILE_8x2x2},
+                                                              {"16x2x1", PRC_TILE_16x2x1}, {"32x1x1", PRC_TILE_32x1x1},
+                                                              {"4x4x2", PRC_TILE_4x4x2},   {"16x1x2", PRC_TILE_16x1x2}};
+         s.tile = -1;  // an unknown shape fails the parameter check below
+         for (const auto& t : shapes)
+             if (!strcmp(v, t.first)) s.tile = t.second;
+     }},
 };
 
 // Default output file of each mode (prc.cu:553-554).
@@ -171,7 +182,7 @@ Settings parse(int argc, char** argv) {
         s.rays >= 2 && s.rays % 2 == 0 && s.rays <= INT_MAX - 31,
         s.iterations >= 0 && s.iterations < INT_MAX,
         s.beta >= 0 && s.gamma >= 0 && s.support_rho >= 0 && s.air_cap_mm > 0,
-        s.save_every >= 0 && s.cache >= 0,
+        s.save_every >= 0 && s.cache >= 0 && s.tile >= 0,
         s.mode == "correct" || s.mode == "forward" || s.mode == "adjoint",
     };
     if (!std::all_of(std::begin(in_range), std::end(in_range), [](bool b) { return b; })) {
@@ -330,6 +341,7 @@ int main(int argc, char** argv) {
     opts.exact_range = o.exact_range;
     opts.cache = o.trace_near_every_pass ? PRC_CACHE_NONE : o.cache;
     opts.precision = o.bf16 ? PRC_PRECISION_BF16 : PRC_PRECISION_FP32;
+    opts.tile = o.tile;
     struct Build {
         prc_handle* h = nullptr;
         int rc = PRC_OK;
