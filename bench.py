@@ -70,6 +70,8 @@ def parse():
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-frames sub-record")
     ap.add_argument("--oracle-full", action="store_true",
                     help="also run the FP64 oracle on the whole volume (minutes on the host cores)")
+    ap.add_argument("--tile", choices=("auto", "8x2x2", "16x2x1", "32x1x1", "4x4x2", "16x1x2"), default="auto",
+                    help="source tile of the headline form's stored field (default: the autotuner's choice)")
     ap.add_argument("--frames", type=int, default=32)
     ap.add_argument("--surrogate", action="store_true", help="batch: learned surrogate where it applies")
     return ap.parse_args()
@@ -229,7 +231,9 @@ def run_ours(args):
     rho, truth, spacing = make_workload(args.grid)
     t0 = time.perf_counter()
     cache, prec = FORMS[args.form]
-    P = pm.Projector(ISOTOPE, rho, spacing, rays=RAYS, support_rho=SUPPORT_RHO, cache=cache, precision=prec)
+    tile = {"auto": pm.PRC_TILE_AUTO, "8x2x2": pm.PRC_TILE_8x2x2, "16x2x1": pm.PRC_TILE_16x2x1,
+            "32x1x1": pm.PRC_TILE_32x1x1, "4x4x2": pm.PRC_TILE_4x4x2, "16x1x2": pm.PRC_TILE_16x1x2}[args.tile]
+    P = pm.Projector(ISOTOPE, rho, spacing, rays=RAYS, support_rho=SUPPORT_RHO, cache=cache, precision=prec, tile=tile)
     P.synchronize()
     setup_s = time.perf_counter() - t0
     stream = torch.cuda.ExternalStream(P.stream)
@@ -393,6 +397,7 @@ def run_ours(args):
             "field_entries": {"source_major": far_entries, "target_major": far_t_entries},
             "voxels_per_s": round(value * n_vox, 1),
             "device_gb": round(P.device_bytes / 1e9, 2),
+            "tile": "x".join(str(v) for v in pm.TILE_SHAPES.get(P.tile, (0, 0, 0))),
             "first_handle_setup_s": round(setup_s, 4),
         },
         "e2e": {"value": round(e2e_value, 3), "unit": "EM iters/s",

@@ -964,15 +964,17 @@ int prc_adjoint(prc_handle* h, const float* d_in, float* d_out, void* stream) {
 static bool half_volumes(const prc_handle* h) { return h->far_t.b16 && h->far_field.b16; }
 
 static int ensure_em(prc_handle* h) {
-    if (h->g_em) return PRC_OK;
-    PRC_CUDA(h->alloc(&h->g_em, h->n));
-    for (float*& v : h->vol) PRC_CUDA(h->alloc(&v, h->n));
-    PRC_CUDA(h->alloc(&h->scalars, 1));
-    PRC_CUDA(h->alloc(&h->red.partials, (size_t)kReduceBlocks * 4));
-    PRC_CUDA(h->alloc(&h->red.counter, 1));
-    PRC_CUDA(h->alloc(&h->geo_w, 27));
-    PRC_CUDA(em_geometry_weights(h->g, h->geo_w, h->stream));
-    if (half_volumes(h)) {
+    if (!h->g_em) {
+        PRC_CUDA(h->alloc(&h->g_em, h->n));
+        for (float*& v : h->vol) PRC_CUDA(h->alloc(&v, h->n));
+        PRC_CUDA(h->alloc(&h->scalars, 1));
+        PRC_CUDA(h->alloc(&h->red.partials, (size_t)kReduceBlocks * 4));
+        PRC_CUDA(h->alloc(&h->red.counter, 1));
+        PRC_CUDA(h->alloc(&h->geo_w, 27));
+        PRC_CUDA(em_geometry_weights(h->g, h->geo_w, h->stream));
+    }
+    // (a batch adds its target-major copies after this first call, so checked every time)
+    if (half_volumes(h) && !h->u16) {
         PRC_CUDA(h->alloc(&h->u16, h->n));
         PRC_CUDA(h->alloc(&h->ratio16, h->n));
     }
