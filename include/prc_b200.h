@@ -38,8 +38,10 @@ enum {
 
 /* Precision of the projector's stored weights (near cache and far-field coefficient field). */
 enum {
-    PRC_PRECISION_FP32 = 0, /* float weights: the reference's numerics */
-    PRC_PRECISION_BF16 = 1  /* bfloat16 stored weights, float accumulation, FP64 global sums */
+    PRC_PRECISION_FP32 = 0,        /* float weights: the reference's numerics */
+    PRC_PRECISION_BF16 = 1,        /* bfloat16 stored weights, float accumulation, FP64 global sums */
+    PRC_PRECISION_BF16_VOLUMES = 2 /* as PRC_PRECISION_BF16, and inside MAP-EM the volumes the
+                                      projections gather (y / W and the EM ratio) in bfloat16 too */
 };
 
 /* What the projector keeps in device memory between projections.  The reference caches the

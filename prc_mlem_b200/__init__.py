@@ -26,6 +26,7 @@ HEADER_PATH = PKG_DIR.parent / "include" / "prc_b200.h"
 PRC_OK = 0
 PRC_PRECISION_FP32 = 0
 PRC_PRECISION_BF16 = 1
+PRC_PRECISION_BF16_VOLUMES = 2
 PRC_CACHE_NONE = 0
 PRC_CACHE_NEAR = 1
 PRC_CACHE_FULL = 2

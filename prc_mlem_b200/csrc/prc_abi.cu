@@ -93,7 +93,7 @@ struct prc_handle {
     // MAP-EM state
     float* g_em = nullptr;
     float* geo_w = nullptr;  // the RDP's 27 neighbour distance weights
-    // mixed-precision form: the gathered volumes of MAP-EM in bf16 (u = y / W, the EM ratio)
+    // PRC_PRECISION_BF16_VOLUMES: the gathered volumes of MAP-EM in bf16 (u = y / W, the EM ratio)
     __nv_bfloat16* u16 = nullptr;
     __nv_bfloat16* ratio16 = nullptr;
     float* vol[5] = {};  // f, prev, y, h_prev, est (rotated by pointer swaps)
@@ -325,6 +325,9 @@ static int build_target_major(prc_handle* h, const std::vector<int>& active, siz
 // pack whose 4-step vector holds a nonzero weight, a new allocation holding only those vectors,
 // and the built stream released.  When the new allocation cannot be had the built stream stays
 // and every lane of every pack counts as kept (the same consumer reads both).
+#ifndef PRC_COMPACT_FIELD
+#define PRC_COMPACT_FIELD 1
+#endif
 static int compact_stream(prc_handle* h, bool target) {
     ProjParams& p = h->params;
     StreamLayout& l = target ? p.tgt : p.src;
@@ -356,7 +359,11 @@ static int compact_stream(prc_handle* h, bool target) {
     }
     base[h->n_groups] = run;
     FarField compact;
+#if PRC_COMPACT_FIELD
     cudaError_t e = field.f32 ? h->alloc(&compact.f32, (size_t)run * 4) : h->alloc(&compact.b16, (size_t)run * 4);
+#else
+    cudaError_t e = cudaErrorMemoryAllocation;  // compaction switched off at build time
+#endif
     if (e != cudaSuccess) {  // not enough memory for both streams at once: keep the built one
         cudaGetLastError();
         PRC_CUDA(field_identity_layout(p, l, mask, vec_base, h->stream));
@@ -393,7 +400,7 @@ static int build_surrogate_field(prc_handle* h, prc_net* net, float target_scale
                                  int64_t* fallbacks) {
     ProjParams& p = h->params;
     const Grid& g = h->g;
-    const bool bf16 = h->opts.precision == PRC_PRECISION_BF16;
+    const bool bf16 = h->opts.precision != PRC_PRECISION_FP32;
     const int n_rays = h->opts.rays;
     const int march_len = (int)(((long long)g.nx + g.ny + g.nz + 6) / 4 * 4);
     if (march_len >= 65535) return fail(PRC_ERR_LIMIT, "volume too large for the surrogate field");
@@ -602,7 +609,7 @@ static int create_impl(prc_handle* h, const float* density_host, prc_net* net, b
     PRC_CUDA(setup_rays(g, h->opts.rays, h->far, h->near_rays, h->stream));
     PRC_CUDA(order_near_rays(h->near_rays, h->near_order, h->near_start, h->stream));
 
-    const bool bf16 = h->opts.precision == PRC_PRECISION_BF16;
+    const bool bf16 = h->opts.precision != PRC_PRECISION_FP32;
     const size_t elem = bf16 ? 2 : 4;
     h->trace_near = true;
     if (surrogate) {
@@ -713,7 +720,7 @@ static int create_handle(const prc_geometry* geo, const char* isotope, const prc
         !std::isfinite(geo->dx) || !std::isfinite(geo->dy) || !std::isfinite(geo->dz) || o.rays < 2 ||
         (o.rays & 1) || o.rays > INT_MAX - 31 || !(o.support_rho >= 0) || !(o.air_cap_mm > 0) ||
         !std::isfinite(o.support_rho) || !std::isfinite(o.air_cap_mm) ||
-        (o.precision != PRC_PRECISION_FP32 && o.precision != PRC_PRECISION_BF16) || o.cache < PRC_CACHE_NONE ||
+        o.precision < PRC_PRECISION_FP32 || o.precision > PRC_PRECISION_BF16_VOLUMES || o.cache < PRC_CACHE_NONE ||
         o.cache > PRC_CACHE_SOURCE_MAJOR || o.tile < PRC_TILE_AUTO || o.tile > PRC_TILE_16x1x2 ||
         !(target_scale > 0) || !(fallback_nrmse >= 0))
         return fail(PRC_ERR_ARGUMENT, "Invalid geometry or solver parameters");
@@ -959,9 +966,11 @@ int prc_adjoint(prc_handle* h, const float* d_in, float* d_out, void* stream) {
     return PRC_OK;
 }
 
-// The mixed-precision form keeps the volumes MAP-EM gathers in bf16: with the bf16 field in both
-// majors (the forward is a gather whose epilogue takes the ratio).
-static bool half_volumes(const prc_handle* h) { return h->far_t.b16 && h->far_field.b16; }
+// PRC_PRECISION_BF16_VOLUMES keeps the volumes MAP-EM gathers in bf16 as well: with the bf16 field
+// in both majors (the forward is a gather whose epilogue takes the ratio).
+static bool half_volumes(const prc_handle* h) {
+    return h->opts.precision == PRC_PRECISION_BF16_VOLUMES && h->far_t.b16 && h->far_field.b16;
+}
 
 static int ensure_em(prc_handle* h) {
     if (!h->g_em) {
