@@ -22,17 +22,11 @@ struct RayStep {
     int pad;
 };
 
-// Layout of a stored field stream (see FarField).  The stream is built with every lane vector
-// in place (pack P of the stream holds 32 vectors); compaction then drops the vectors that hold
-// only zeros: pack P keeps the lanes of mask[P], stored in lane order from the group's running
-// vector offset (vec_base[G] + the stored vectors of the group's earlier packs).
+// Layout of a stored field stream (see FarField).
 struct StreamLayout {
     const unsigned short* len = nullptr;    // [n_groups][n_rows]: stored steps of row k in group G
     const long long* group_base = nullptr;  // [n_groups + 1]: element offset of group G's stream
-                                            // before compaction (pack P = offset / 128)
     const int* desc = nullptr;              // per pack: template element offset of its first step
-    const unsigned* mask = nullptr;         // per pack: lanes whose 4-step vector is stored
-    const long long* vec_base = nullptr;    // [n_groups + 1]: first stored vector of group G
 };
 
 // Everything a projector kernel needs to know about one volume.
@@ -231,17 +225,7 @@ cudaError_t project(Op op, const ProjParams& p, const OpArgs& a, bool trace_near
 cudaError_t build_template(const ProjParams& p, int* tmpl, int* tmpl_neg, cudaStream_t s);
 // Fills the pack descriptors (one int per 128 stored entries) of a stream layout.
 cudaError_t build_descriptors(const ProjParams& p, const StreamLayout& l, int* desc, cudaStream_t s);
-// Compaction of a filled stream (l.group_base as built): mask[P] = lanes of pack P whose vector
-// holds a nonzero weight, group_vecs[G] = the group's stored vectors.
-cudaError_t field_masks(const ProjParams& p, const StreamLayout& l, const FarField& f, unsigned* mask,
-                        long long* group_vecs, cudaStream_t s);
-// Copies every stored vector of `from` (built layout) to its compacted place in `to`
-// (l.mask and l.vec_base set).
-cudaError_t field_compact(const ProjParams& p, const StreamLayout& l, const FarField& from, const FarField& to,
-                          cudaStream_t s);
-// Masks of an uncompacted stream (every lane stored) and vec_base[G] = group_base[G] / 4.
-cudaError_t field_identity_layout(const ProjParams& p, const StreamLayout& l, unsigned* mask, long long* vec_base,
-                                  cudaStream_t s);
+
 // Stored steps of the near-block row (125 offsets padded to whole packs).
 int near_row_steps();
 

@@ -67,15 +67,11 @@ struct prc_handle {
     long long* group_base = nullptr;
     long long* group_total = nullptr;
     int* desc = nullptr;
-    unsigned* mask = nullptr;        // compaction: per pack kept lanes, per group first vector
-    long long* vec_base = nullptr;
     // target-major copy of the field (forward projection as a gather)
     FarField far_t;
     unsigned short* len_t = nullptr;
     long long* group_base_t = nullptr;
     int* desc_t = nullptr;
-    unsigned* mask_t = nullptr;
-    long long* vec_base_t = nullptr;
     int* vox2src = nullptr;
     float* u = nullptr;  // f / W volume for the gather form of the forward projection
     int64_t far_t_entries = 0;
@@ -106,7 +102,6 @@ struct prc_handle {
     int tile = PRC_TILE_AUTO;  // source tile in effect (PRC_TILE_*)
 
     std::vector<void*> allocations;
-    std::vector<size_t> allocation_bytes;
     // projection timing (prc_timing): start/end event pairs of forward and adjoint launches
     bool timing = false;
     std::vector<cudaEvent_t> events[2];
@@ -118,22 +113,9 @@ struct prc_handle {
         const cudaError_t e = cudaMalloc(&v, count * sizeof(T) > 0 ? count * sizeof(T) : 1);
         if (e != cudaSuccess) return e;
         allocations.push_back(v);
-        allocation_bytes.push_back(count * sizeof(T));
         bytes += (int64_t)(count * sizeof(T));
         *p = static_cast<T*>(v);
         return cudaMemsetAsync(v, 0, count * sizeof(T), stream);
-    }
-
-    // Frees one allocation of the handle early (after the stream has finished with it).
-    void release(void* v) {
-        for (size_t i = 0; i < allocations.size(); ++i)
-            if (allocations[i] == v) {
-                cudaFree(v);
-                bytes -= (int64_t)allocation_bytes[i];
-                allocations.erase(allocations.begin() + (long)i);
-                allocation_bytes.erase(allocation_bytes.begin() + (long)i);
-                return;
-            }
     }
 
     cudaStream_t pick(void* s) const { return s ? static_cast<cudaStream_t>(s) : stream; }
@@ -319,72 +301,6 @@ static int build_target_major(prc_handle* h, const std::vector<int>& active, siz
     PRC_CUDA(cudaStreamSynchronize(h->stream));
     h->far_t_entries = run;
     return PRC_OK;
-}
-
-// Compaction of one stored stream (source-major, or the target-major copy): the lanes of every
-// pack whose 4-step vector holds a nonzero weight, a new allocation holding only those vectors,
-// and the built stream released.  When the new allocation cannot be had the built stream stays
-// and every lane of every pack counts as kept (the same consumer reads both).
-#ifndef PRC_COMPACT_FIELD
-#define PRC_COMPACT_FIELD 1
-#endif
-static int compact_stream(prc_handle* h, bool target) {
-    ProjParams& p = h->params;
-    StreamLayout& l = target ? p.tgt : p.src;
-    FarField& field = target ? h->far_t : h->far_field;
-    unsigned*& mask = target ? h->mask_t : h->mask;
-    long long*& vec_base = target ? h->vec_base_t : h->vec_base;
-    int64_t& entries = target ? h->far_t_entries : h->far_entries;
-    if (!field.on() || mask) return PRC_OK;
-    const size_t packs = (size_t)entries / (4 * kLanes);
-    PRC_CUDA(h->alloc(&mask, packs));
-    PRC_CUDA(h->alloc(&vec_base, (size_t)h->n_groups + 1));
-    l.mask = mask;
-    long long* d_kept = nullptr;
-    PRC_CUDA(cudaMalloc(&d_kept, (size_t)h->n_groups * sizeof(long long)));
-    struct Free {
-        long long* p;
-        ~Free() { cudaFree(p); }
-    } free_kept{d_kept};
-    PRC_CUDA(field_masks(p, l, field, mask, d_kept, h->stream));
-    std::vector<long long> base((size_t)h->n_groups + 1);
-    PRC_CUDA(cudaMemcpyAsync(base.data(), d_kept, (size_t)h->n_groups * sizeof(long long), cudaMemcpyDeviceToHost,
-                             h->stream));
-    PRC_CUDA(cudaStreamSynchronize(h->stream));
-    long long run = 0;
-    for (int g = 0; g < h->n_groups; ++g) {
-        const long long k = base[g];
-        base[g] = run;
-        run += k;
-    }
-    base[h->n_groups] = run;
-    FarField compact;
-#if PRC_COMPACT_FIELD
-    cudaError_t e = field.f32 ? h->alloc(&compact.f32, (size_t)run * 4) : h->alloc(&compact.b16, (size_t)run * 4);
-#else
-    cudaError_t e = cudaErrorMemoryAllocation;  // compaction switched off at build time
-#endif
-    if (e != cudaSuccess) {  // not enough memory for both streams at once: keep the built one
-        cudaGetLastError();
-        PRC_CUDA(field_identity_layout(p, l, mask, vec_base, h->stream));
-        l.vec_base = vec_base;
-        return PRC_OK;
-    }
-    PRC_CUDA(cudaMemcpyAsync(vec_base, base.data(), base.size() * sizeof(long long), cudaMemcpyHostToDevice,
-                             h->stream));
-    l.vec_base = vec_base;
-    PRC_CUDA(field_compact(p, l, field, compact, h->stream));
-    PRC_CUDA(cudaStreamSynchronize(h->stream));
-    h->release(field.f32 ? static_cast<void*>(field.f32) : static_cast<void*>(field.b16));
-    field = compact;
-    entries = run * 4;  // 4 steps per vector
-    return PRC_OK;
-}
-
-static int compact_fields(prc_handle* h) {
-    int rc = compact_stream(h, false);
-    if (rc == PRC_OK) rc = compact_stream(h, true);
-    return rc;
 }
 
 static int create_impl(prc_handle* h, const float* density_host, prc_net* net = nullptr, bool surrogate = false,
@@ -618,10 +534,6 @@ static int create_impl(prc_handle* h, const float* density_host, prc_net* net, b
         rc = build_target_major(h, active, elem);
         if (rc != PRC_OK) return rc;
         if (h->far_t.on()) h->cache_mode = PRC_CACHE_FULL;
-        if (!batch_member) {  // a batch compacts after adding its target-major copies
-            rc = compact_fields(h);
-            if (rc != PRC_OK) return rc;
-        }
         PRC_CUDA(cudaStreamSynchronize(h->stream));
         return check_device_error(h);
     }
@@ -697,10 +609,6 @@ static int create_impl(prc_handle* h, const float* density_host, prc_net* net, b
         const int rc = build_target_major(h, active, elem);
         if (rc != PRC_OK) return rc;
         if (h->far_t.on()) h->cache_mode = PRC_CACHE_FULL;
-    }
-    if (!batch_member) {  // a batch compacts after adding its target-major copies
-        const int rc = compact_fields(h);
-        if (rc != PRC_OK) return rc;
     }
     PRC_CUDA(cudaStreamSynchronize(h->stream));
     return check_device_error(h);
@@ -1568,15 +1476,6 @@ int prc_batch_create(int n_frames, const prc_frame* frames, const prc_options* o
                 return rc;
             }
             if (h->far_t.on()) h->cache_mode = PRC_CACHE_FULL;
-        }
-    }
-    for (int i = 0; i < n_frames; ++i) {  // every stream complete: drop the all-zero lane vectors
-        const int rc = compact_fields(b->frames[i]);
-        if (rc != PRC_OK) {
-            const std::string msg = g_last_error;
-            prc_batch_destroy(b);
-            g_last_error = "frame " + std::to_string(i) + ": " + msg;
-            return rc;
         }
     }
     *out = b;

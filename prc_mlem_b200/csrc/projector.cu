@@ -163,13 +163,12 @@ __host__ __device__ constexpr int field_base(int m) { return m == kFieldF32 || m
 // walking the stream.
 constexpr int kPack = 4;
 constexpr int kNearRow = 128;  // 125 block offsets rounded up to whole packs
-// Shared memory the stored-field launches reserve per warp although they use none: it sets the
-// L1 / shared-memory split and so how many warps share an SM's L1 (on the 128x128x159 torso a
-// launch without it, with the largest L1, measured 1.7-2x slower).
-#ifndef PRC_FIELD_SMEM_PER_WARP
-#define PRC_FIELD_SMEM_PER_WARP 4096
-#endif
-constexpr size_t kFieldSmemPerWarp = PRC_FIELD_SMEM_PER_WARP;
+// The stored field streams through a ring of kRing shared-memory stages per warp, one batch of
+// kBatch packs (16 steps of 32 lanes: 2 KB fp32, 1 KB bf16) per stage, filled by TMA bulk copies.
+constexpr int kBatch = 4;
+constexpr int kRing = 3;
+constexpr int kStageBytes = kBatch * kPack * kLanes * 4;  // the fp32 size; bf16 uses half of it
+constexpr size_t kFieldSmemPerWarp = size_t(kRing) * kStageBytes;
 constexpr size_t kFieldSmemBytes = size_t(kWarps) * kFieldSmemPerWarp;
 // try_wait rounds before a bounded mbarrier wait gives up (each round is a bounded hardware wait).
 constexpr int kWaitRounds = 1 << 20;
@@ -187,6 +186,15 @@ __device__ __forceinline__ void fence_mbarrier_init() {
 __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
 }
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+// 1D bulk copy global -> this CTA's shared memory, completion counted on an mbarrier.
+// Source and destination are 16-byte aligned and bytes is a multiple of 16.
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity, int rounds = kWaitRounds) {
     for (int i = 0; i < rounds; ++i) {
         unsigned done;
@@ -198,21 +206,6 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity
         if (done) return true;
     }
     return false;
-}
-
-// A vector of the stored field (8 bytes bf16, 16 bytes fp32), read once per projection: loaded
-// without allocating in L1, which keeps L1 for the volume being gathered.
-__device__ __forceinline__ uint2 ld_stream(const uint2* q) {
-    uint2 x;
-    asm("ld.global.nc.L1::no_allocate.v2.u32 {%0, %1}, [%2];" : "=r"(x.x), "=r"(x.y) : "l"(q));
-    return x;
-}
-__device__ __forceinline__ float4 ld_stream(const float4* q) {
-    float4 x;
-    asm("ld.global.nc.L1::no_allocate.v4.f32 {%0, %1, %2, %3}, [%4];"
-        : "=f"(x.x), "=f"(x.y), "=f"(x.z), "=f"(x.w)
-        : "l"(q));
-    return x;
 }
 
 __device__ __forceinline__ int near_offset(const ProjParams& p, int q) {
@@ -278,10 +271,11 @@ __global__ void order_near_kernel(const RayStep* near, short* order, int* start)
 // then also holds the near block).  Norm always marches and writes W, and the near cache or
 // the stored field when they are allocated; Layout marches to size the field.
 // The work of one warp (group `group`, warp `warp` of its block): dyn_smem is the block's
-// dynamic shared memory (near tiles are indexed by warp).
+// dynamic shared memory (near tiles or field rings are indexed by warp), bars the warp's kRing
+// mbarriers.
 template <Op OP, bool EXACT, int NEAR_MODE, int FAR_MODE>
 __device__ __forceinline__ void project_group(const ProjParams& p, const OpArgs& a, int group, int warp,
-                                              unsigned char* dyn_smem) {
+                                              unsigned char* dyn_smem, uint64_t* bars) {
     const int lane = threadIdx.x & 31;
     if (group * kLanes >= p.n_active) return;  // the whole warp leaves together
     const int src = group * kLanes + lane;
@@ -399,99 +393,157 @@ __device__ __forceinline__ void project_group(const ProjParams& p, const OpArgs&
             }
         }
     } else {
-        // Stored field, compacted: pack P of the group keeps the vectors of the lanes in mask[P],
-        // in lane order from a running vector offset.  Each lane loads its own vector straight
-        // from HBM (16 bytes fp32, 8 bytes bf16; a warp's loads of one pack are contiguous)
-        // without allocating in L1, which keeps L1 for the volume being gathered.  A batch is
-        // kBatch packs: the packs' template offsets (one int4 broadcast each, addressed by the
-        // pack descriptors), the weights, then one predicated gather per nonzero weight -- zero
-        // padding costs no memory traffic -- or one scatter per nonzero weight without the
-        // target-major copy.  Weights and template offsets are loaded one batch ahead and the
-        // descriptors and masks two batches ahead, so the descriptor -> template -> gather chain
-        // exposes one memory latency per batch instead of three.
+        // Stored field.  The group's packs stream through this warp's ring of kRing shared-memory
+        // stages, one batch of kBatch packs per stage: lane 0 keeps the next batches in flight
+        // as TMA bulk copies (cp.async.bulk, completion counted on a per-stage mbarrier), so
+        // the weights occupy no registers while they travel.  The projection is bound by the
+        // latency of its gathers, so they are software-pipelined one batch deep: while batch b
+        // is reduced, the gathers of batch b + 1 are already in flight (their weights are read
+        // from the ring to predicate them -- zero padding costs no memory traffic -- and read
+        // again when the batch is reduced).  Template offsets (one int4 broadcast per pack,
+        // addressed by the pack descriptors) run one batch ahead of the gathers that use them
+        // and the descriptors two.  Every mbarrier wait is bounded; a wait that gives up raises
+        // the error flag and the warp drains its copies and stops.  Without the target-major
+        // copy the forward scatters each nonzero weight with an atomic add instead of gathering.
         constexpr bool kGatherT = OP == Op::Forward && target_major(FAR_MODE);
+        constexpr bool kGather = OP == Op::Adjoint || kGatherT;
         constexpr int kBase = field_base(FAR_MODE);  // kFieldF32 / kFieldBF16
-        constexpr int kBatch = 4;  // packs per batch: 16 steps in flight per lane
-        using Vec = typename std::conditional<kBase == kFieldF32, float4, uint2>::type;
+        constexpr int kElem = kBase == kFieldF32 ? 4 : 2;
+        constexpr int kPackBytes = kPack * kLanes * kElem;
+        constexpr int kChunk = kBatch * kPackBytes;
+        constexpr int kSteps = kBatch * kPack;
         const StreamLayout& lay = kGatherT ? p.tgt : p.src;
         const FarField& fld = kGatherT ? a.farT : a.far;
         const int* tmpl = kGatherT ? p.tmpl_neg : p.tmpl;
         const long long e0 = lay.group_base[group], e1 = lay.group_base[group + 1];
-        const long long pk0 = e0 / (kPack * kLanes);
-        const int* desc = lay.desc + pk0;
-        const unsigned* mask = lay.mask + pk0;
+        const int* desc = lay.desc + e0 / (kPack * kLanes);
         const int n_packs = (int)((e1 - e0) / (kPack * kLanes));
-        const Vec* vec = reinterpret_cast<const Vec*>(kBase == kFieldF32 ? static_cast<const void*>(fld.f32)
-                                                                          : static_cast<const void*>(fld.b16)) +
-                         lay.vec_base[group];
-        const unsigned below = (1u << lane) - 1u;  // lanes stored before this one in a pack
-        // Gathered voxel: source + offset (adjoint) or target - offset (forward).  A 32-bit index
-        // (one wide multiply-add per address); the sum wraps only on padding steps (w = 0),
-        // whose loads are predicated off, since voxel indices stay below INT_MAX.
-        auto gather_index = [&](int o) { return (int)((unsigned)s + (unsigned)o); };
-        auto desc_at = [&](int P) { return P < n_packs ? __ldg(desc + P) : 0; };
-        auto mask_at = [&](int P) { return P < n_packs ? __ldg(mask + P) : 0u; };
-        int off = 0;  // running vector offset of the next pack to load (the same in every lane)
-        auto load_vec = [&](unsigned m) {
-            Vec x;
-            if constexpr (kBase == kFieldF32) x = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            else x = make_uint2(0u, 0u);
-            if ((m >> lane) & 1u) x = ld_stream(vec + off + __popc(m & below));
-            off += __popc(m);
-            return x;
+        const int n_batches = (n_packs + kBatch - 1) / kBatch;
+        const char* src_bytes = (kBase == kFieldF32 ? reinterpret_cast<const char*>(fld.f32)
+                                                    : reinterpret_cast<const char*>(fld.b16)) + e0 * kElem;
+        const long long total = (e1 - e0) * kElem;
+        unsigned char* ring = dyn_smem + (size_t)warp * kFieldSmemPerWarp;
+        auto issue = [&](int b) {  // lane 0: batch b into its stage
+            const int stage = b % kRing;
+            const unsigned bytes = (unsigned)min((long long)kChunk, total - (long long)b * kChunk);
+            mbar_expect_tx(&bars[stage], bytes);
+            bulk_copy_g2s(ring + stage * kStageBytes, src_bytes + (long long)b * kChunk, bytes, &bars[stage]);
         };
-        auto unpack = [](const Vec& x, float* w) {
-            if constexpr (kBase == kFieldF32) {
+        if (lane == 0) {
+            for (int k = 0; k < kRing; ++k) mbar_init(&bars[k], 1);
+            fence_mbarrier_init();
+            for (int b = 0; b < n_batches && b < kRing; ++b) issue(b);
+        }
+        __syncwarp();
+        // this lane's 4 weights of pack k of batch b (zero past the group's last pack)
+        auto weights = [&](int b, int k, float* w) {
+            const unsigned char* stage = ring + (b % kRing) * kStageBytes + k * kPackBytes;
+            if (b * kBatch + k >= n_packs) {
+                w[0] = w[1] = w[2] = w[3] = 0.0f;
+            } else if constexpr (kBase == kFieldF32) {
+                const float4 x = reinterpret_cast<const float4*>(stage)[lane];
                 w[0] = x.x, w[1] = x.y, w[2] = x.z, w[3] = x.w;
             } else {
+                const uint2 x = reinterpret_cast<const uint2*>(stage)[lane];
                 w[0] = __uint_as_float(x.x << 16), w[1] = __uint_as_float(x.x & 0xffff0000u);
                 w[2] = __uint_as_float(x.y << 16), w[3] = __uint_as_float(x.y & 0xffff0000u);
             }
         };
-        int4 tn[kBatch];
-        Vec wn[kBatch];
-        int dq[kBatch];
-        unsigned mq[kBatch];
-#pragma unroll
-        for (int k = 0; k < kBatch; ++k) wn[k] = load_vec(mask_at(k));
+        auto desc_at = [&](int P) { return P < n_packs ? __ldg(desc + P) : 0; };
+        // Gathered voxel: source + offset (adjoint) or target - offset (forward).  A 32-bit index
+        // (one wide multiply-add per address); the sum wraps only on padding steps (w = 0),
+        // whose loads are predicated off, since voxel indices stay below INT_MAX.
+        auto gather = [&](int o) {
+            const int idx = (int)((unsigned)s + (unsigned)o);
+            if constexpr (half_volume(FAR_MODE)) return __bfloat162float(__ldg(a.in16 + idx));
+            else return __ldg(a.in + idx);
+        };
+        int4 tn[kBatch];  // template offsets of the next batch to gather
+        int dq[kBatch];   // descriptors of the batch after it
 #pragma unroll
         for (int k = 0; k < kBatch; ++k) tn[k] = __ldg(reinterpret_cast<const int4*>(tmpl + desc_at(k)));
 #pragma unroll
-        for (int k = 0; k < kBatch; ++k) dq[k] = desc_at(kBatch + k), mq[k] = mask_at(kBatch + k);
-        for (int P0 = 0; P0 < n_packs; P0 += kBatch) {
-            int o[kBatch * kPack];
-            float w[kBatch * kPack];
-            int4 tc[kBatch];
-            Vec wc[kBatch];
+        for (int k = 0; k < kBatch; ++k) dq[k] = desc_at(kBatch + k);
+        bool ok = true;
+        // The gathers of batch b (kGather forms): wait for its weights, predicate, load.
+        // (a warp-uniform verdict: every lane polls the barrier, all must have seen it complete)
+        auto wait_batch = [&](int b) { return __all_sync(kFull, mbar_wait_bounded(&bars[b % kRing], (b / kRing) & 1)); };
+        auto start_gathers = [&](int b, float* v) {
+            if (!wait_batch(b)) return false;
+            float w[kSteps];
 #pragma unroll
-            for (int k = 0; k < kBatch; ++k) tc[k] = tn[k], wc[k] = wn[k];
+            for (int k = 0; k < kBatch; ++k) weights(b, k, w + k * kPack);
+            int o[kSteps];
+#pragma unroll
+            for (int k = 0; k < kBatch; ++k)
+                o[k * kPack] = tn[k].x, o[k * kPack + 1] = tn[k].y, o[k * kPack + 2] = tn[k].z, o[k * kPack + 3] = tn[k].w;
+#pragma unroll
+            for (int u = 0; u < kSteps; ++u) v[u] = w[u] > 0.0f ? gather(o[u]) : 0.0f;
+            return true;
+        };
+        auto advance_template = [&](int b_next) {  // tn <- batch b_next, dq <- batch b_next + 1
 #pragma unroll
             for (int k = 0; k < kBatch; ++k) tn[k] = __ldg(reinterpret_cast<const int4*>(tmpl + dq[k]));
 #pragma unroll
-            for (int k = 0; k < kBatch; ++k) wn[k] = load_vec(mq[k]);
+            for (int k = 0; k < kBatch; ++k) dq[k] = desc_at((b_next + 1) * kBatch + k);
+        };
+        float v_cur[kSteps];
+        if constexpr (kGather) {
+            ok = n_batches == 0 || start_gathers(0, v_cur);
+            advance_template(1);
+        }
+        for (int b = 0; ok && b < n_batches; ++b) {
+            if constexpr (kGather) {
+                float v_next[kSteps];
+                if (b + 1 < n_batches) {
+                    ok = start_gathers(b + 1, v_next);
+                    advance_template(b + 2);
+                } else {
 #pragma unroll
-            for (int k = 0; k < kBatch; ++k) dq[k] = desc_at(P0 + 2 * kBatch + k), mq[k] = mask_at(P0 + 2 * kBatch + k);
-#pragma unroll
-            for (int k = 0; k < kBatch; ++k) {
-                o[k * kPack] = tc[k].x, o[k * kPack + 1] = tc[k].y, o[k * kPack + 2] = tc[k].z, o[k * kPack + 3] = tc[k].w;
-                unpack(wc[k], w + k * kPack);
-            }
-            if constexpr (OP == Op::Adjoint || kGatherT) {
-                float v[kBatch * kPack];
-#pragma unroll
-                for (int u = 0; u < kBatch * kPack; ++u) {
-                    if constexpr (half_volume(FAR_MODE))
-                        v[u] = w[u] > 0.0f ? __bfloat162float(__ldg(a.in16 + gather_index(o[u]))) : 0.0f;
-                    else
-                        v[u] = w[u] > 0.0f ? __ldg(a.in + gather_index(o[u])) : 0.0f;
+                    for (int u = 0; u < kSteps; ++u) v_next[u] = 0.0f;
                 }
+                float w[kSteps];
 #pragma unroll
-                for (int u = 0; u < kBatch * kPack; ++u) acc = fmaf(w[u], v[u], acc);
-            } else {
+                for (int k = 0; k < kBatch; ++k) weights(b, k, w + k * kPack);
 #pragma unroll
-                for (int u = 0; u < kBatch * kPack; ++u)
-                    if (live && w[u] > 0.0f) deposit(s + o[u], w[u]);
+                for (int u = 0; u < kSteps; ++u) acc = fmaf(w[u], v_cur[u], acc);
+#pragma unroll
+                for (int u = 0; u < kSteps; ++u) v_cur[u] = v_next[u];
+            } else {  // scatter over the source-major field
+                if (!wait_batch(b)) {
+                    ok = false;
+                    break;
+                }
+                float w[kSteps];
+#pragma unroll
+                for (int k = 0; k < kBatch; ++k) weights(b, k, w + k * kPack);
+#pragma unroll
+                for (int k = 0; k < kBatch; ++k) {
+                    const int4 t = tn[k];
+                    const int o4[4] = {t.x, t.y, t.z, t.w};
+#pragma unroll
+                    for (int j = 0; j < kPack; ++j)
+                        if (live && w[k * kPack + j] > 0.0f) deposit(s + o4[j], w[k * kPack + j]);
+                }
+                advance_template(b + 1);
             }
+            __syncwarp();  // every lane is done with stage b % kRing
+            if (lane == 0 && ok && b + kRing < n_batches) {
+                fence_proxy_async();  // this stage's reads precede the copy that overwrites it
+                issue(b + kRing);
+            }
+        }
+        if (!ok) {
+            // A copy did not complete in time: report it, and give the copies still in flight a
+            // bounded chance to land before this warp's shared memory is released.
+            if (lane == 0) {
+                atomicOr(a.error, 1u);
+                for (int k = 0; k < kRing; ++k) {
+                    mbar_wait_bounded(&bars[k], 0);
+                    mbar_wait_bounded(&bars[k], 1);
+                }
+            }
+            __syncwarp();
         }
     }
 
@@ -516,16 +568,18 @@ __device__ __forceinline__ void project_group(const ProjParams& p, const OpArgs&
 }
 
 // Stored-field launches are held to the registers of PRC_FIELD_MIN_BLOCKS blocks of 256 threads
-// per SM (4: 64 registers): the gather stream needs warps in flight more than registers.
+// per SM (2: the one-batch-deep gather pipeline fits without spilling).
 #ifndef PRC_FIELD_MIN_BLOCKS
-#define PRC_FIELD_MIN_BLOCKS 4
+#define PRC_FIELD_MIN_BLOCKS 2
 #endif
 template <Op OP, bool EXACT, int NEAR_MODE, int FAR_MODE>
 __global__ void __launch_bounds__(kMaxBlock, FAR_MODE == kMarch ? 1 : PRC_FIELD_MIN_BLOCKS)
     project_kernel(const ProjParams p, const OpArgs a) {
     extern __shared__ __align__(128) unsigned char dyn_smem[];
+    __shared__ uint64_t field_bars[kMaxWarps][kRing];
     const int warp = threadIdx.x >> 5;
-    project_group<OP, EXACT, NEAR_MODE, FAR_MODE>(p, a, blockIdx.x * (blockDim.x >> 5) + warp, warp, dyn_smem);
+    project_group<OP, EXACT, NEAR_MODE, FAR_MODE>(p, a, blockIdx.x * (blockDim.x >> 5) + warp, warp, dyn_smem,
+                                                  field_bars[warp]);
 }
 
 // Batched launch over many volumes: block b belongs to the item (volume) whose first_block is
@@ -533,6 +587,7 @@ __global__ void __launch_bounds__(kMaxBlock, FAR_MODE == kMarch ? 1 : PRC_FIELD_
 template <Op OP>
 __global__ void __launch_bounds__(kMaxBlock) project_batch_kernel(const BatchItem* items, int n_items) {
     extern __shared__ __align__(128) unsigned char dyn_smem[];
+    __shared__ uint64_t field_bars[kMaxWarps][kRing];
     int lo = 0, hi = n_items - 1;
     while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
@@ -544,14 +599,15 @@ __global__ void __launch_bounds__(kMaxBlock) project_batch_kernel(const BatchIte
     const int mode = items[lo].mode;
     const int warp = threadIdx.x >> 5;
     const int group = ((int)blockIdx.x - items[lo].first_block) * (blockDim.x >> 5) + warp;
+    uint64_t* bars = field_bars[warp];
     switch (mode) {
-        case kBatchTraceMarch: project_group<OP, false, kTraceNear, kMarch>(p, a, group, warp, dyn_smem); break;
-        case kBatchCacheF32March: project_group<OP, false, kCacheF32, kMarch>(p, a, group, warp, dyn_smem); break;
-        case kBatchCacheBF16March: project_group<OP, false, kCacheBF16, kMarch>(p, a, group, warp, dyn_smem); break;
-        case kBatchFieldF32: project_group<OP, false, kTraceNear, kFieldF32>(p, a, group, warp, dyn_smem); break;
-        case kBatchFieldBF16: project_group<OP, false, kTraceNear, kFieldBF16>(p, a, group, warp, dyn_smem); break;
-        case kBatchFieldF32T: project_group<OP, false, kTraceNear, kFieldF32T>(p, a, group, warp, dyn_smem); break;
-        case kBatchFieldBF16T: project_group<OP, false, kTraceNear, kFieldBF16T>(p, a, group, warp, dyn_smem); break;
+        case kBatchTraceMarch: project_group<OP, false, kTraceNear, kMarch>(p, a, group, warp, dyn_smem, bars); break;
+        case kBatchCacheF32March: project_group<OP, false, kCacheF32, kMarch>(p, a, group, warp, dyn_smem, bars); break;
+        case kBatchCacheBF16March: project_group<OP, false, kCacheBF16, kMarch>(p, a, group, warp, dyn_smem, bars); break;
+        case kBatchFieldF32: project_group<OP, false, kTraceNear, kFieldF32>(p, a, group, warp, dyn_smem, bars); break;
+        case kBatchFieldBF16: project_group<OP, false, kTraceNear, kFieldBF16>(p, a, group, warp, dyn_smem, bars); break;
+        case kBatchFieldF32T: project_group<OP, false, kTraceNear, kFieldF32T>(p, a, group, warp, dyn_smem, bars); break;
+        case kBatchFieldBF16T: project_group<OP, false, kTraceNear, kFieldBF16T>(p, a, group, warp, dyn_smem, bars); break;
         default: break;
     }
 }
@@ -585,70 +641,6 @@ __global__ void desc_kernel(const ProjParams p, const StreamLayout l, int* desc)
     int* out = desc + l.group_base[group] / (kPack * kLanes);
     for (int row = 0; row < p.n_rows; ++row)
         for (int m = 0; m < len[row]; m += kPack) *out++ = row * p.tmpl_len + m;
-}
-
-// Compaction masks: one warp per group walks its packs; lane l's vector of pack P is kept when
-// any of its 4 weights is nonzero (bit patterns: stored weights are positive or +0).
-template <int FAR_MODE>
-__global__ void __launch_bounds__(kBlock) field_mask_kernel(const ProjParams p, const StreamLayout l, const FarField f,
-                                                            unsigned* mask, long long* group_vecs) {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int group = blockIdx.x * kWarps + warp;
-    if (group * kLanes >= p.n_active) return;
-    const long long e0 = l.group_base[group], e1 = l.group_base[group + 1];
-    const long long pk0 = e0 / (kPack * kLanes);
-    const int n = (int)((e1 - e0) / (kPack * kLanes));
-    long long kept = 0;
-    for (int P = 0; P < n; ++P) {
-        const size_t v = (size_t)(e0 / kPack) + (size_t)P * kLanes + lane;
-        bool any;
-        if constexpr (FAR_MODE == kFieldF32) {
-            const uint4 x = reinterpret_cast<const uint4*>(f.f32)[v];
-            any = (x.x | x.y | x.z | x.w) != 0u;
-        } else {
-            const uint2 x = reinterpret_cast<const uint2*>(f.b16)[v];
-            any = (x.x | x.y) != 0u;
-        }
-        const unsigned m = __ballot_sync(kFull, any);
-        if (lane == 0) mask[pk0 + P] = m;
-        kept += __popc(m);
-    }
-    if (lane == 0) group_vecs[group] = kept;
-}
-
-// Moves every kept vector to its compacted place (the new stream is a separate allocation).
-template <int FAR_MODE>
-__global__ void __launch_bounds__(kBlock) field_compact_kernel(const ProjParams p, const StreamLayout l,
-                                                               const FarField from, const FarField to) {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int group = blockIdx.x * kWarps + warp;
-    if (group * kLanes >= p.n_active) return;
-    const long long e0 = l.group_base[group], e1 = l.group_base[group + 1];
-    const long long pk0 = e0 / (kPack * kLanes);
-    const int n = (int)((e1 - e0) / (kPack * kLanes));
-    const unsigned below = (1u << lane) - 1u;
-    long long out = l.vec_base[group];
-    for (int P = 0; P < n; ++P) {
-        const unsigned m = l.mask[pk0 + P];
-        if ((m >> lane) & 1u) {
-            const size_t v = (size_t)(e0 / kPack) + (size_t)P * kLanes + lane;
-            const size_t w = (size_t)out + __popc(m & below);
-            if constexpr (FAR_MODE == kFieldF32) reinterpret_cast<uint4*>(to.f32)[w] = reinterpret_cast<const uint4*>(from.f32)[v];
-            else reinterpret_cast<uint2*>(to.b16)[w] = reinterpret_cast<const uint2*>(from.b16)[v];
-        }
-        out += __popc(m);
-    }
-}
-
-// The layout of an uncompacted stream in compacted terms: every lane kept.
-__global__ void field_identity_kernel(const ProjParams p, const StreamLayout l, unsigned* mask, long long* vec_base,
-                                      int n_groups) {
-    const int group = blockIdx.x * blockDim.x + threadIdx.x;
-    if (group > n_groups) return;
-    vec_base[group] = l.group_base[group] / kPack;
-    if (group == n_groups) return;
-    const long long p0 = l.group_base[group] / (kPack * kLanes), p1 = l.group_base[group + 1] / (kPack * kLanes);
-    for (long long P = p0; P < p1; ++P) mask[P] = kFull;
 }
 
 // Walks every stored source-major entry w > 0 of a group (lane = source s, template row k,
@@ -969,8 +961,7 @@ cudaError_t launch(const ProjParams& p, const OpArgs& a, cudaStream_t s) {
     const int blocks = (groups + kWarps - 1) / kWarps;
     if (blocks == 0) return cudaSuccess;
     size_t smem = 0;
-    // The stored field (near block included) reads HBM directly; its launches reserve shared
-    // memory only to set the L1 split (kFieldSmemPerWarp).
+    // the stored field's ring (the near block is in the field)
     if (FAR_MODE != kMarch) smem = kFieldSmemBytes;
     else if (NEAR_MODE == kTraceNear && OP != Op::Layout)
         smem = OP == Op::Norm && a.near_acc ? size_t(kWarps) * 27 * kLanes * sizeof(float) : kNearSmemBytes;
@@ -1040,31 +1031,6 @@ cudaError_t build_descriptors(const ProjParams& p, const StreamLayout& l, int* d
     const int groups = (p.n_active + kLanes - 1) / kLanes;
     if (groups == 0) return cudaSuccess;
     desc_kernel<<<(groups + 127) / 128, 128, 0, s>>>(p, l, desc);
-    return cudaGetLastError();
-}
-
-cudaError_t field_masks(const ProjParams& p, const StreamLayout& l, const FarField& f, unsigned* mask,
-                        long long* group_vecs, cudaStream_t s) {
-    const int groups = (p.n_active + kLanes - 1) / kLanes;
-    if (groups == 0) return cudaSuccess;
-    if (f.f32) field_mask_kernel<kFieldF32><<<(groups + kWarps - 1) / kWarps, kBlock, 0, s>>>(p, l, f, mask, group_vecs);
-    else field_mask_kernel<kFieldBF16><<<(groups + kWarps - 1) / kWarps, kBlock, 0, s>>>(p, l, f, mask, group_vecs);
-    return cudaGetLastError();
-}
-
-cudaError_t field_compact(const ProjParams& p, const StreamLayout& l, const FarField& from, const FarField& to,
-                          cudaStream_t s) {
-    const int groups = (p.n_active + kLanes - 1) / kLanes;
-    if (groups == 0) return cudaSuccess;
-    if (from.f32) field_compact_kernel<kFieldF32><<<(groups + kWarps - 1) / kWarps, kBlock, 0, s>>>(p, l, from, to);
-    else field_compact_kernel<kFieldBF16><<<(groups + kWarps - 1) / kWarps, kBlock, 0, s>>>(p, l, from, to);
-    return cudaGetLastError();
-}
-
-cudaError_t field_identity_layout(const ProjParams& p, const StreamLayout& l, unsigned* mask, long long* vec_base,
-                                  cudaStream_t s) {
-    const int groups = (p.n_active + kLanes - 1) / kLanes;
-    field_identity_kernel<<<(groups + 1 + 127) / 128, 128, 0, s>>>(p, l, mask, vec_base, groups);
     return cudaGetLastError();
 }
 
