@@ -62,9 +62,10 @@ def parse():
                     help="only run this many forward+adjoint pairs of the headline form (profiling)")
     ap.add_argument("--form", choices=("fp32", "bf16", "traced"), default="fp32",
                     help="projector form of the headline number (default: plain fp32 stored field)")
-    ap.add_argument("--workload", choices=("torso", "batch", "surrogate"), default="torso",
+    ap.add_argument("--workload", choices=("torso", "batch", "surrogate", "tiles"), default="torso",
                     help="batch: 32 dynamic-PET frames of mixed grids and isotopes, 10 iterations each; "
-                         "surrogate: the learned surrogate's evaluation on the small phantom at 128x128x159")
+                         "surrogate: the learned surrogate's evaluation on the small phantom at 128x128x159; "
+                         "tiles: projection and MAP-EM times of every source tile shape in both precisions")
     ap.add_argument("--no-parity", action="store_true",
                     help="skip the comparison with the reference executable and the time-to-image leg")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-frames sub-record")
@@ -1099,6 +1100,51 @@ def run_surrogate_eval(args):
                       "network": "trained" if net is not None else "absent", "isotopes": results}))
 
 
+def run_tiles(args):
+    """Stored-field projections per source tile shape, fp32 and bf16 weights, on the torso: mean
+    device time of ten forward and ten adjoint projections (after three warm-up pairs) and of
+    one MAP-EM iteration (a 6-iteration correction / 6), and the stored entries."""
+    import torch
+    import prc_mlem_b200 as pm
+    torch.cuda.set_device(0)
+    rho, truth, spacing = make_workload(args.grid)
+    d = torch.from_numpy(truth).cuda()
+    out = {}
+    for prec_name, prec in (("fp32", pm.PRC_PRECISION_FP32), ("bf16", pm.PRC_PRECISION_BF16)):
+        for tile, shape in pm.TILE_SHAPES.items():
+            P = pm.Projector(ISOTOPE, rho, spacing, rays=RAYS, support_rho=SUPPORT_RHO, precision=prec, tile=tile)
+            o = torch.empty_like(d)
+            s = torch.cuda.ExternalStream(P.stream)
+            for _ in range(3):
+                P.forward(d, o)
+                P.adjoint(d, o)
+            P.synchronize()
+            rec = {}
+            for name, fn in (("forward_ms", P.forward), ("adjoint_ms", P.adjoint)):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(s)
+                for _ in range(10):
+                    fn(d, o)
+                e1.record(s)
+                e1.synchronize()
+                rec[name] = round(e0.elapsed_time(e1) / 10, 4)
+            P.forward(d, o)
+            g = o.clone()
+            P.correct(g, o, args.iterations, BETA, GAMMA, True)
+            P.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(s)
+            P.correct(g, o, args.iterations, BETA, GAMMA, True)
+            e1.record(s)
+            e1.synchronize()
+            rec["em_iteration_ms"] = round(e0.elapsed_time(e1) / args.iterations, 4)
+            rec["stored_entries"] = P.cache_mode[1]
+            out[f"{prec_name} {'x'.join(map(str, shape))}"] = rec
+            P.close()
+    nz, ny, nx = args.grid
+    print(json.dumps({"workload": f"torso {nx}x{ny}x{nz}, {ISOTOPE}, rays {RAYS}", "tiles": out}))
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -1107,6 +1153,8 @@ def main():
         run_batch(args)
     elif args.workload == "surrogate":
         run_surrogate_eval(args)
+    elif args.workload == "tiles":
+        run_tiles(args)
     else:
         run_ours(args)
 

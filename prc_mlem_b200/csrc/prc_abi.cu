@@ -134,7 +134,7 @@ struct prc_handle {
 };
 
 // The tile of handles that are not tuned (see choose_tile).
-static constexpr int kDefaultTile = PRC_TILE_32x1x1;
+static constexpr int kDefaultTile = PRC_TILE_8x2x2;
 
 // (x, y, z) extent of a PRC_TILE_* source tile; every shape holds 32 voxels.
 static const int* tile_dims(int tile) {
@@ -666,7 +666,7 @@ static int create_handle(const prc_geometry* geo, const char* isotope, const prc
 // with CUDA events after a warm-up pair, and keeps the fastest; later handles of the
 // configuration reuse the choice.  Forms without a stored field (near cache, traced) and
 // surrogate fields take kDefaultTile.
-static constexpr int kTileCandidates[] = {PRC_TILE_32x1x1, PRC_TILE_16x2x1, PRC_TILE_8x2x2};
+static constexpr int kTileCandidates[] = {PRC_TILE_8x2x2, PRC_TILE_16x2x1, PRC_TILE_32x1x1};
 static constexpr int kTuneSlices = 32;
 static std::mutex g_tile_mutex;
 static std::map<std::string, int> g_tile_choice;

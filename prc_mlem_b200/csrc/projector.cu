@@ -163,12 +163,12 @@ __host__ __device__ constexpr int field_base(int m) { return m == kFieldF32 || m
 // walking the stream.
 constexpr int kPack = 4;
 constexpr int kNearRow = 128;  // 125 block offsets rounded up to whole packs
-// The stored field streams through a ring of kRing shared-memory stages per warp, one batch of
-// kBatch packs (16 steps of 32 lanes: 2 KB fp32, 1 KB bf16) per stage, filled by TMA bulk copies.
-constexpr int kBatch = 4;
-constexpr int kRing = 3;
-constexpr int kStageBytes = kBatch * kPack * kLanes * 4;  // the fp32 size; bf16 uses half of it
-constexpr size_t kFieldSmemPerWarp = size_t(kRing) * kStageBytes;
+// TMA ring of the fp32 field stream: kStages chunks of kChunk bytes per warp.  The bf16 form
+// loads its vectors directly and keeps the reservation only for the L1 / shared-memory split it
+// gives (launched without it, with the largest L1, it measured 1.7-2x slower).
+constexpr int kStages = 2;
+constexpr int kChunk = 2048;
+constexpr size_t kFieldSmemPerWarp = size_t(kStages) * kChunk;
 constexpr size_t kFieldSmemBytes = size_t(kWarps) * kFieldSmemPerWarp;
 // try_wait rounds before a bounded mbarrier wait gives up (each round is a bounded hardware wait).
 constexpr int kWaitRounds = 1 << 20;
@@ -206,6 +206,14 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity
         if (done) return true;
     }
     return false;
+}
+
+// An 8-byte vector of the bf16 field, read once per projection: loaded without allocating in
+// L1, which keeps L1 for the volume being gathered.
+__device__ __forceinline__ uint2 ld_stream(const uint2* q) {
+    uint2 x;
+    asm("ld.global.nc.L1::no_allocate.v2.u32 {%0, %1}, [%2];" : "=r"(x.x), "=r"(x.y) : "l"(q));
+    return x;
 }
 
 __device__ __forceinline__ int near_offset(const ProjParams& p, int q) {
@@ -271,8 +279,8 @@ __global__ void order_near_kernel(const RayStep* near, short* order, int* start)
 // then also holds the near block).  Norm always marches and writes W, and the near cache or
 // the stored field when they are allocated; Layout marches to size the field.
 // The work of one warp (group `group`, warp `warp` of its block): dyn_smem is the block's
-// dynamic shared memory (near tiles or field rings are indexed by warp), bars the warp's kRing
-// mbarriers.
+// dynamic shared memory (near tiles or field rings are indexed by warp), bars the warp's
+// kStages mbarriers.
 template <Op OP, bool EXACT, int NEAR_MODE, int FAR_MODE>
 __device__ __forceinline__ void project_group(const ProjParams& p, const OpArgs& a, int group, int warp,
                                               unsigned char* dyn_smem, uint64_t* bars) {
@@ -393,157 +401,182 @@ __device__ __forceinline__ void project_group(const ProjParams& p, const OpArgs&
             }
         }
     } else {
-        // Stored field.  The group's packs stream through this warp's ring of kRing shared-memory
-        // stages, one batch of kBatch packs per stage: lane 0 keeps the next batches in flight
-        // as TMA bulk copies (cp.async.bulk, completion counted on a per-stage mbarrier), so
-        // the weights occupy no registers while they travel.  The projection is bound by the
-        // latency of its gathers, so they are software-pipelined one batch deep: while batch b
-        // is reduced, the gathers of batch b + 1 are already in flight (their weights are read
-        // from the ring to predicate them -- zero padding costs no memory traffic -- and read
-        // again when the batch is reduced).  Template offsets (one int4 broadcast per pack,
-        // addressed by the pack descriptors) run one batch ahead of the gathers that use them
-        // and the descriptors two.  Every mbarrier wait is bounded; a wait that gives up raises
-        // the error flag and the warp drains its copies and stops.  Without the target-major
-        // copy the forward scatters each nonzero weight with an atomic add instead of gathering.
+        // Stored field.  fp32: streamed by TMA -- lane 0 keeps kStages bulk copies of kChunk bytes in
+        // flight into this warp's shared-memory ring (cp.async.bulk, completion counted by an
+        // mbarrier), so the weights arrive as contiguous DRAM bursts without holding
+        // registers.  A chunk is consumed in batches of kBatch packs: the packs' template
+        // offsets (one int4 broadcast each, addressed by the pack descriptors), the weights
+        // from shared memory, then one predicated gather per nonzero weight -- zero padding
+        // costs no memory traffic -- or one scatter per nonzero weight without the
+        // target-major copy.  Entries of lanes that are not sources are zero by construction.
+        // The template offsets are fetched one batch ahead and the descriptors two batches
+        // ahead, so the descriptor -> template -> gather chain exposes one memory latency per
+        // batch instead of three.
         constexpr bool kGatherT = OP == Op::Forward && target_major(FAR_MODE);
-        constexpr bool kGather = OP == Op::Adjoint || kGatherT;
         constexpr int kBase = field_base(FAR_MODE);  // kFieldF32 / kFieldBF16
         constexpr int kElem = kBase == kFieldF32 ? 4 : 2;
         constexpr int kPackBytes = kPack * kLanes * kElem;
-        constexpr int kChunk = kBatch * kPackBytes;
-        constexpr int kSteps = kBatch * kPack;
+        constexpr int kPacksPerChunk = kChunk / kPackBytes;
+        constexpr int kBatch = 4;  // packs per batch: 16 steps in flight per lane
         const StreamLayout& lay = kGatherT ? p.tgt : p.src;
         const FarField& fld = kGatherT ? a.farT : a.far;
         const int* tmpl = kGatherT ? p.tmpl_neg : p.tmpl;
         const long long e0 = lay.group_base[group], e1 = lay.group_base[group + 1];
         const int* desc = lay.desc + e0 / (kPack * kLanes);
         const int n_packs = (int)((e1 - e0) / (kPack * kLanes));
-        const int n_batches = (n_packs + kBatch - 1) / kBatch;
-        const char* src_bytes = (kBase == kFieldF32 ? reinterpret_cast<const char*>(fld.f32)
-                                                    : reinterpret_cast<const char*>(fld.b16)) + e0 * kElem;
-        const long long total = (e1 - e0) * kElem;
-        unsigned char* ring = dyn_smem + (size_t)warp * kFieldSmemPerWarp;
-        auto issue = [&](int b) {  // lane 0: batch b into its stage
-            const int stage = b % kRing;
-            const unsigned bytes = (unsigned)min((long long)kChunk, total - (long long)b * kChunk);
-            mbar_expect_tx(&bars[stage], bytes);
-            bulk_copy_g2s(ring + stage * kStageBytes, src_bytes + (long long)b * kChunk, bytes, &bars[stage]);
-        };
-        if (lane == 0) {
-            for (int k = 0; k < kRing; ++k) mbar_init(&bars[k], 1);
-            fence_mbarrier_init();
-            for (int b = 0; b < n_batches && b < kRing; ++b) issue(b);
-        }
-        __syncwarp();
-        // this lane's 4 weights of pack k of batch b (zero past the group's last pack)
-        auto weights = [&](int b, int k, float* w) {
-            const unsigned char* stage = ring + (b % kRing) * kStageBytes + k * kPackBytes;
-            if (b * kBatch + k >= n_packs) {
-                w[0] = w[1] = w[2] = w[3] = 0.0f;
-            } else if constexpr (kBase == kFieldF32) {
-                const float4 x = reinterpret_cast<const float4*>(stage)[lane];
-                w[0] = x.x, w[1] = x.y, w[2] = x.z, w[3] = x.w;
-            } else {
-                const uint2 x = reinterpret_cast<const uint2*>(stage)[lane];
-                w[0] = __uint_as_float(x.x << 16), w[1] = __uint_as_float(x.x & 0xffff0000u);
-                w[2] = __uint_as_float(x.y << 16), w[3] = __uint_as_float(x.y & 0xffff0000u);
-            }
-        };
-        auto desc_at = [&](int P) { return P < n_packs ? __ldg(desc + P) : 0; };
         // Gathered voxel: source + offset (adjoint) or target - offset (forward).  A 32-bit index
         // (one wide multiply-add per address); the sum wraps only on padding steps (w = 0),
         // whose loads are predicated off, since voxel indices stay below INT_MAX.
+        auto gather_index = [&](int o) { return (int)((unsigned)s + (unsigned)o); };
+        // the gathered value: the fp32 volume, or the bf16 one of PRC_PRECISION_BF16_VOLUMES
         auto gather = [&](int o) {
-            const int idx = (int)((unsigned)s + (unsigned)o);
-            if constexpr (half_volume(FAR_MODE)) return __bfloat162float(__ldg(a.in16 + idx));
-            else return __ldg(a.in + idx);
+            if constexpr (half_volume(FAR_MODE)) return __bfloat162float(__ldg(a.in16 + gather_index(o)));
+            else return __ldg(a.in + gather_index(o));
         };
-        int4 tn[kBatch];  // template offsets of the next batch to gather
-        int dq[kBatch];   // descriptors of the batch after it
+        if constexpr (kBase == kFieldBF16) {
+            // bf16 form: each lane loads its own 8-byte vectors straight from HBM (a warp's loads
+            // of one pack coalesce into 256 contiguous bytes) one batch ahead of their use.  This
+            // form is bound by L1 wavefronts, not bytes, and skipping the shared-memory ring
+            // (its copies in and its reads out) measured 5 % faster than the TMA stream.
+            const uint2* vec = reinterpret_cast<const uint2*>(fld.b16) + e0 / kPack + lane;
+            auto load_vec = [&](int P) {
+                uint2 x = make_uint2(0u, 0u);
+                if (P < n_packs) x = ld_stream(vec + (size_t)P * kLanes);
+                return x;
+            };
+            auto desc_at = [&](int P) { return P < n_packs ? __ldg(desc + P) : 0; };
+            int4 tn[kBatch];
+            uint2 wn[kBatch];
+            int dq[kBatch];
 #pragma unroll
-        for (int k = 0; k < kBatch; ++k) tn[k] = __ldg(reinterpret_cast<const int4*>(tmpl + desc_at(k)));
+            for (int k = 0; k < kBatch; ++k) wn[k] = load_vec(k);
 #pragma unroll
-        for (int k = 0; k < kBatch; ++k) dq[k] = desc_at(kBatch + k);
-        bool ok = true;
-        // The gathers of batch b (kGather forms): wait for its weights, predicate, load.
-        // (a warp-uniform verdict: every lane polls the barrier, all must have seen it complete)
-        auto wait_batch = [&](int b) { return __all_sync(kFull, mbar_wait_bounded(&bars[b % kRing], (b / kRing) & 1)); };
-        auto start_gathers = [&](int b, float* v) {
-            if (!wait_batch(b)) return false;
-            float w[kSteps];
+            for (int k = 0; k < kBatch; ++k) tn[k] = __ldg(reinterpret_cast<const int4*>(tmpl + desc_at(k)));
 #pragma unroll
-            for (int k = 0; k < kBatch; ++k) weights(b, k, w + k * kPack);
-            int o[kSteps];
+            for (int k = 0; k < kBatch; ++k) dq[k] = desc_at(kBatch + k);
+            for (int P0 = 0; P0 < n_packs; P0 += kBatch) {
+                int o[kBatch * kPack];
+                float w[kBatch * kPack];
+                int4 tc[kBatch];
+                uint2 wc[kBatch];
 #pragma unroll
-            for (int k = 0; k < kBatch; ++k)
-                o[k * kPack] = tn[k].x, o[k * kPack + 1] = tn[k].y, o[k * kPack + 2] = tn[k].z, o[k * kPack + 3] = tn[k].w;
+                for (int k = 0; k < kBatch; ++k) tc[k] = tn[k], wc[k] = wn[k];
 #pragma unroll
-            for (int u = 0; u < kSteps; ++u) v[u] = w[u] > 0.0f ? gather(o[u]) : 0.0f;
-            return true;
-        };
-        auto advance_template = [&](int b_next) {  // tn <- batch b_next, dq <- batch b_next + 1
+                for (int k = 0; k < kBatch; ++k) tn[k] = __ldg(reinterpret_cast<const int4*>(tmpl + dq[k]));
 #pragma unroll
-            for (int k = 0; k < kBatch; ++k) tn[k] = __ldg(reinterpret_cast<const int4*>(tmpl + dq[k]));
+                for (int k = 0; k < kBatch; ++k) wn[k] = load_vec(P0 + kBatch + k);
 #pragma unroll
-            for (int k = 0; k < kBatch; ++k) dq[k] = desc_at((b_next + 1) * kBatch + k);
-        };
-        float v_cur[kSteps];
-        if constexpr (kGather) {
-            ok = n_batches == 0 || start_gathers(0, v_cur);
-            advance_template(1);
-        }
-        for (int b = 0; ok && b < n_batches; ++b) {
-            if constexpr (kGather) {
-                float v_next[kSteps];
-                if (b + 1 < n_batches) {
-                    ok = start_gathers(b + 1, v_next);
-                    advance_template(b + 2);
+                for (int k = 0; k < kBatch; ++k) dq[k] = desc_at(P0 + 2 * kBatch + k);
+#pragma unroll
+                for (int k = 0; k < kBatch; ++k) {
+                    o[k * kPack] = tc[k].x, o[k * kPack + 1] = tc[k].y, o[k * kPack + 2] = tc[k].z, o[k * kPack + 3] = tc[k].w;
+                    w[k * kPack] = __uint_as_float(wc[k].x << 16), w[k * kPack + 1] = __uint_as_float(wc[k].x & 0xffff0000u);
+                    w[k * kPack + 2] = __uint_as_float(wc[k].y << 16), w[k * kPack + 3] = __uint_as_float(wc[k].y & 0xffff0000u);
+                }
+                if constexpr (OP == Op::Adjoint || kGatherT) {
+                    float v[kBatch * kPack];
+#pragma unroll
+                    for (int u = 0; u < kBatch * kPack; ++u) v[u] = w[u] > 0.0f ? gather(o[u]) : 0.0f;
+#pragma unroll
+                    for (int u = 0; u < kBatch * kPack; ++u) acc = fmaf(w[u], v[u], acc);
                 } else {
 #pragma unroll
-                    for (int u = 0; u < kSteps; ++u) v_next[u] = 0.0f;
+                    for (int u = 0; u < kBatch * kPack; ++u)
+                        if (live && w[u] > 0.0f) deposit(s + o[u], w[u]);
                 }
-                float w[kSteps];
-#pragma unroll
-                for (int k = 0; k < kBatch; ++k) weights(b, k, w + k * kPack);
-#pragma unroll
-                for (int u = 0; u < kSteps; ++u) acc = fmaf(w[u], v_cur[u], acc);
-#pragma unroll
-                for (int u = 0; u < kSteps; ++u) v_cur[u] = v_next[u];
-            } else {  // scatter over the source-major field
-                if (!wait_batch(b)) {
+            }
+        } else {
+            unsigned char* ring = dyn_smem + (size_t)warp * kStages * kChunk;
+            const char* src_bytes = (kBase == kFieldF32 ? reinterpret_cast<const char*>(fld.f32)
+                                                        : reinterpret_cast<const char*>(fld.b16)) + e0 * kElem;
+            const long long total = (e1 - e0) * kElem;
+            const int n_chunks = (n_packs + kPacksPerChunk - 1) / kPacksPerChunk;
+            auto issue = [&](int c) {  // lane 0 only
+                const int stage = c % kStages;
+                const unsigned bytes = (unsigned)min((long long)kChunk, total - (long long)c * kChunk);
+                mbar_expect_tx(&bars[stage], bytes);
+                bulk_copy_g2s(ring + stage * kChunk, src_bytes + (long long)c * kChunk, bytes, &bars[stage]);
+            };
+            if (lane == 0) {
+                for (int k = 0; k < kStages; ++k) mbar_init(&bars[k], 1);
+                fence_mbarrier_init();
+                for (int c = 0; c < n_chunks && c < kStages; ++c) issue(c);
+            }
+            __syncwarp();
+            static_assert(kPacksPerChunk % kBatch == 0, "batches stay inside a chunk");
+            auto desc_at = [&](int P) { return P < n_packs ? __ldg(desc + P) : 0; };
+            int4 tn[kBatch];
+            int dq[kBatch];
+    #pragma unroll
+            for (int k = 0; k < kBatch; ++k) tn[k] = __ldg(reinterpret_cast<const int4*>(tmpl + desc_at(k)));
+    #pragma unroll
+            for (int k = 0; k < kBatch; ++k) dq[k] = desc_at(kBatch + k);
+            bool ok = true;
+            for (int c = 0; c < n_chunks; ++c) {
+                const int packs = min(kPacksPerChunk, n_packs - c * kPacksPerChunk);
+                const int stage = c % kStages;
+                if (!mbar_wait_bounded(&bars[stage], (c / kStages) & 1)) {
                     ok = false;
                     break;
                 }
-                float w[kSteps];
-#pragma unroll
-                for (int k = 0; k < kBatch; ++k) weights(b, k, w + k * kPack);
-#pragma unroll
-                for (int k = 0; k < kBatch; ++k) {
-                    const int4 t = tn[k];
-                    const int o4[4] = {t.x, t.y, t.z, t.w};
-#pragma unroll
-                    for (int j = 0; j < kPack; ++j)
-                        if (live && w[k * kPack + j] > 0.0f) deposit(s + o4[j], w[k * kPack + j]);
+                const unsigned char* chunk = ring + stage * kChunk;
+                for (int b = 0; b < packs; b += kBatch) {
+                    const int P0 = c * kPacksPerChunk + b;
+                    int o[kBatch * kPack];
+                    float w[kBatch * kPack];
+                    int4 tc[kBatch];
+    #pragma unroll
+                    for (int k = 0; k < kBatch; ++k) tc[k] = tn[k];
+    #pragma unroll
+                    for (int k = 0; k < kBatch; ++k) tn[k] = __ldg(reinterpret_cast<const int4*>(tmpl + dq[k]));
+    #pragma unroll
+                    for (int k = 0; k < kBatch; ++k) dq[k] = desc_at(P0 + 2 * kBatch + k);
+    #pragma unroll
+                    for (int k = 0; k < kBatch; ++k) {
+                        const bool here = b + k < packs;
+                        const int4 t = tc[k];
+                        o[k * kPack] = t.x, o[k * kPack + 1] = t.y, o[k * kPack + 2] = t.z, o[k * kPack + 3] = t.w;
+                        if constexpr (kBase == kFieldF32) {
+                            const float4 x = here ? reinterpret_cast<const float4*>(chunk + (b + k) * kPackBytes)[lane]
+                                                  : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                            w[k * kPack] = x.x, w[k * kPack + 1] = x.y, w[k * kPack + 2] = x.z, w[k * kPack + 3] = x.w;
+                        } else {
+                            const uint2 x = here ? reinterpret_cast<const uint2*>(chunk + (b + k) * kPackBytes)[lane]
+                                                 : make_uint2(0u, 0u);
+                            w[k * kPack] = __uint_as_float(x.x << 16), w[k * kPack + 1] = __uint_as_float(x.x & 0xffff0000u);
+                            w[k * kPack + 2] = __uint_as_float(x.y << 16), w[k * kPack + 3] = __uint_as_float(x.y & 0xffff0000u);
+                        }
+                    }
+                    if constexpr (OP == Op::Adjoint || kGatherT) {
+                        float v[kBatch * kPack];
+    #pragma unroll
+                        for (int u = 0; u < kBatch * kPack; ++u) v[u] = w[u] > 0.0f ? gather(o[u]) : 0.0f;
+    #pragma unroll
+                        for (int u = 0; u < kBatch * kPack; ++u) acc = fmaf(w[u], v[u], acc);
+                    } else {
+    #pragma unroll
+                        for (int u = 0; u < kBatch * kPack; ++u)
+                            if (live && w[u] > 0.0f) deposit(s + o[u], w[u]);
+                    }
                 }
-                advance_template(b + 1);
-            }
-            __syncwarp();  // every lane is done with stage b % kRing
-            if (lane == 0 && ok && b + kRing < n_batches) {
-                fence_proxy_async();  // this stage's reads precede the copy that overwrites it
-                issue(b + kRing);
-            }
-        }
-        if (!ok) {
-            // A copy did not complete in time: report it, and give the copies still in flight a
-            // bounded chance to land before this warp's shared memory is released.
-            if (lane == 0) {
-                atomicOr(a.error, 1u);
-                for (int k = 0; k < kRing; ++k) {
-                    mbar_wait_bounded(&bars[k], 0);
-                    mbar_wait_bounded(&bars[k], 1);
+                __syncwarp();
+                if (lane == 0 && c + kStages < n_chunks) {
+                    fence_proxy_async();  // this stage's reads precede the copy that overwrites it
+                    issue(c + kStages);
                 }
             }
-            __syncwarp();
+            if (!ok) {
+                // A copy did not complete in time: report it, and give the copies still in flight
+                // a bounded chance to land before this warp's shared memory is released.
+                if (lane == 0) {
+                    atomicOr(a.error, 1u);
+                    for (int k = 0; k < kStages; ++k) {
+                        mbar_wait_bounded(&bars[k], 0);
+                        mbar_wait_bounded(&bars[k], 1);
+                    }
+                }
+                __syncwarp();
+            }
         }
     }
 
@@ -567,16 +600,10 @@ __device__ __forceinline__ void project_group(const ProjParams& p, const OpArgs&
     }
 }
 
-// Stored-field launches are held to the registers of PRC_FIELD_MIN_BLOCKS blocks of 256 threads
-// per SM (2: the one-batch-deep gather pipeline fits without spilling).
-#ifndef PRC_FIELD_MIN_BLOCKS
-#define PRC_FIELD_MIN_BLOCKS 2
-#endif
 template <Op OP, bool EXACT, int NEAR_MODE, int FAR_MODE>
-__global__ void __launch_bounds__(kMaxBlock, FAR_MODE == kMarch ? 1 : PRC_FIELD_MIN_BLOCKS)
-    project_kernel(const ProjParams p, const OpArgs a) {
+__global__ void __launch_bounds__(kMaxBlock) project_kernel(const ProjParams p, const OpArgs a) {
     extern __shared__ __align__(128) unsigned char dyn_smem[];
-    __shared__ uint64_t field_bars[kMaxWarps][kRing];
+    __shared__ uint64_t field_bars[kMaxWarps][kStages];
     const int warp = threadIdx.x >> 5;
     project_group<OP, EXACT, NEAR_MODE, FAR_MODE>(p, a, blockIdx.x * (blockDim.x >> 5) + warp, warp, dyn_smem,
                                                   field_bars[warp]);
@@ -587,7 +614,7 @@ __global__ void __launch_bounds__(kMaxBlock, FAR_MODE == kMarch ? 1 : PRC_FIELD_
 template <Op OP>
 __global__ void __launch_bounds__(kMaxBlock) project_batch_kernel(const BatchItem* items, int n_items) {
     extern __shared__ __align__(128) unsigned char dyn_smem[];
-    __shared__ uint64_t field_bars[kMaxWarps][kRing];
+    __shared__ uint64_t field_bars[kMaxWarps][kStages];
     int lo = 0, hi = n_items - 1;
     while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
