@@ -59,11 +59,10 @@ enum {
 
 /* Source tiles of the stored coefficient field: a warp owns 32 tissue voxels taken in tiles
  * of this shape (x fastest inside a tile, tiles in x, y, z order), so every gather of one step
- * touches the rows of one tile shifted by the step's offset.  PRC_TILE_AUTO lets the engine
- * choose: an autotuner builds the field of a central slab of the volume with each candidate
- * shape, times a forward and an adjoint projection, and remembers the fastest per grid,
- * isotope and form for the rest of the process.  The shape changes no result: every source
- * keeps its own weights and summation order. */
+ * touches the rows of one tile shifted by the step's offset.  PRC_TILE_AUTO takes the shape
+ * prc_tune_tile chose for the same configuration earlier in the process, or 8x2x2 when it was
+ * never tuned; batched frames are tuned per configuration.  The shape changes no result: every
+ * source keeps its own weights and summation order. */
 enum {
     PRC_TILE_AUTO = 0,
     PRC_TILE_8x2x2 = 1,
@@ -124,6 +123,15 @@ typedef struct prc_net prc_net;
 int prc_create_surrogate(const prc_geometry* geometry, const char* isotope, const prc_options* opts,
                          const float* density_host, prc_net* net, float target_scale, float fallback_nrmse,
                          int64_t* fallbacks, prc_handle** out);
+
+/* The source-tile autotuner (no counterpart in the reference): builds the stored field of the
+ * central slab (at most 32 z-slices) of this density with each candidate tile (8x2x2, 16x2x1,
+ * 32x1x1), times one forward and one adjoint projection of each with CUDA events, and returns the
+ * fastest in *tile.  The choice is remembered for the configuration (grid, spacing, isotope,
+ * rays, support, air cap, form) for the rest of the process, so later calls and PRC_TILE_AUTO
+ * handles of it cost nothing.  Synchronises. */
+int prc_tune_tile(const prc_geometry* geometry, const char* isotope, const prc_options* opts,
+                  const float* density_host, int* tile);
 
 /* Releases every device allocation of the handle (Projector::~Projector, prc.cu:423-427). */
 void prc_destroy(prc_handle* h);

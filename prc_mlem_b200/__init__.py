@@ -88,6 +88,8 @@ _SIGNATURES = {
     "prc_synchronize": (ctypes.c_int, [_P]),
     "prc_launch_count": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int64)]),
     "prc_tile": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int)]),
+    "prc_tune_tile": (ctypes.c_int, [ctypes.POINTER(Geometry), ctypes.c_char_p, ctypes.POINTER(Options), _P,
+                                     ctypes.POINTER(ctypes.c_int)]),
     "prc_wait_selftest": (ctypes.c_int, [_P, ctypes.c_int]),
     "prc_sum_static": (ctypes.c_int, [_P, ctypes.c_int64, _P, _P]),
     "prc_create_surrogate": (ctypes.c_int, [ctypes.POINTER(Geometry), ctypes.c_char_p, ctypes.POINTER(Options), _P,
@@ -180,6 +182,22 @@ def _ptr(x) -> int:
 
 def _host(a: np.ndarray) -> np.ndarray:
     return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def tune_tile(isotope: str, density: np.ndarray, spacing, rays: int = 128, support_rho: float = 0.05,
+              air_cap_mm: float = 50.0, cache: int = PRC_CACHE_FULL, precision: int = PRC_PRECISION_FP32) -> int:
+    """The source tile the autotuner finds fastest for this configuration (prc_tune_tile); later
+    Projectors of the same configuration with tile=PRC_TILE_AUTO use it."""
+    density = _host(density)
+    nz, ny, nx = density.shape
+    geo = Geometry(nx, ny, nz, *(float(s) for s in spacing))
+    opts = default_options()
+    opts.rays, opts.support_rho, opts.air_cap_mm = rays, support_rho, air_cap_mm
+    opts.cache, opts.precision = int(cache), int(precision)
+    t = ctypes.c_int()
+    _check(lib().prc_tune_tile(ctypes.byref(geo), isotope.encode(), ctypes.byref(opts), density.ctypes.data,
+                               ctypes.byref(t)))
+    return t.value
 
 
 class Projector:

@@ -9,6 +9,8 @@
 // single host synchronisation.
 #include "engine.h"
 
+#include <algorithm>
+
 namespace prc {
 namespace {
 
@@ -269,7 +271,9 @@ __global__ void __launch_bounds__(kEmThreads) update_active_kernel(
                 if (!__ldg(support + nb)) continue;
                 const float w = w_sh[q];
                 const float fk = __ldg(f + nb), d = fj - fk, ad = fabsf(d);
-                const float D = fj + fk + gamma * ad + eps, invD = 1.0f / D;
+                // the correctly rounded reciprocal: the same value as 1.0f / D, without the
+                // general division's numerator handling
+                const float D = fj + fk + gamma * ad + eps, invD = __frcp_rn(D);
                 grad += w * d * (fj + 3.0f * fk + gamma * ad + 2.0f * eps) * invD * invD;
                 const float half_quad = (2.0f * (fj + fk + eps) + gamma * ad) * invD * invD;
                 const float hess = 2.0f * (2.0f * fk + eps) * (2.0f * fk + eps) * invD * invD * invD;
@@ -441,13 +445,15 @@ cudaError_t em_geometry_weights(const Grid& grid, float* geo_w, cudaStream_t s) 
 cudaError_t em_update_active(const EmVolumes& v, const Grid& grid, const int* active, int n_active,
                              const float* geo_w, const float* start, const float* back, float* next, float beta,
                              float gamma, cudaStream_t s) {
+    // one tissue voxel per thread where the reduction scratch allows (kReduceBlocks * 4 block
+    // partials): many warps in flight hide the latency of the neighbour loads and divisions
+    const int blocks = std::max(1, std::min(kReduceBlocks * 4, (n_active + kEmThreads - 1) / kEmThreads));
     if (beta > 0.0f)
-        update_active_kernel<true><<<kReduceBlocks, kEmThreads, 0, s>>>(start, back, v.support, next, active, n_active,
-                                                                        grid, geo_w, beta, gamma, v.scalars, v.red);
+        update_active_kernel<true><<<blocks, kEmThreads, 0, s>>>(start, back, v.support, next, active, n_active, grid,
+                                                                 geo_w, beta, gamma, v.scalars, v.red);
     else
-        update_active_kernel<false><<<kReduceBlocks, kEmThreads, 0, s>>>(start, back, v.support, next, active,
-                                                                         n_active, grid, geo_w, beta, gamma,
-                                                                         v.scalars, v.red);
+        update_active_kernel<false><<<blocks, kEmThreads, 0, s>>>(start, back, v.support, next, active, n_active,
+                                                                  grid, geo_w, beta, gamma, v.scalars, v.red);
     return cudaGetLastError();
 }
 

@@ -660,12 +660,13 @@ static int create_handle(const prc_geometry* geo, const char* isotope, const prc
 // The tile shape trades the field's zero padding (compact tiles: the 32 lanes of a group stop
 // their rays at similar steps) against the cache lines every gather of a step touches (long
 // rows).  Which wins depends on the grid, the isotope's range and the stored precision, so the
-// first handle of each configuration builds the stored field with every candidate shape on the
-// central slab of at most kTuneSlices z-slices of its own density (the same rays, ranges and
-// tissue mix at a fraction of the build time), times one forward and one adjoint projection
-// with CUDA events after a warm-up pair, and keeps the fastest; later handles of the
-// configuration reuse the choice.  Forms without a stored field (near cache, traced) and
-// surrogate fields take kDefaultTile.
+// tuner (prc_tune_tile; every frame configuration of a batch) builds the stored field with every
+// candidate shape on the central slab of at most kTuneSlices z-slices of the density (the same
+// rays, ranges and tissue mix at a fraction of the build time), times one forward and one
+// adjoint projection with CUDA events after a warm-up pair, and keeps the fastest; handles
+// created with PRC_TILE_AUTO take the remembered choice of their configuration, or kDefaultTile
+// when it was never tuned.  Forms without a stored field (near cache, traced) and surrogate
+// fields take kDefaultTile.
 static constexpr int kTileCandidates[] = {PRC_TILE_8x2x2, PRC_TILE_16x2x1, PRC_TILE_32x1x1};
 static constexpr int kTuneSlices = 32;
 static std::mutex g_tile_mutex;
@@ -713,8 +714,10 @@ static int time_projection_pair(prc_handle* h, float* ms) {
     return check_device_error(h);
 }
 
+// The remembered choice of a configuration (tune = false) or, when there is none, the tuner's
+// (tune = true) or kDefaultTile.
 static int choose_tile(const prc_geometry* geo, const char* isotope, const prc_options& o, const float* density_host,
-                       bool surrogate) {
+                       bool surrogate, bool tune) {
     if (surrogate || (o.cache != PRC_CACHE_FULL && o.cache != PRC_CACHE_SOURCE_MAJOR)) return kDefaultTile;
     const std::string key = tile_key(geo, isotope, o);
     {
@@ -722,6 +725,7 @@ static int choose_tile(const prc_geometry* geo, const char* isotope, const prc_o
         const auto it = g_tile_choice.find(key);
         if (it != g_tile_choice.end()) return it->second;
     }
+    if (!tune) return kDefaultTile;
     prc_geometry slab = *geo;
     const float* slab_density = density_host;
     if (geo->nz > kTuneSlices) {
@@ -758,10 +762,25 @@ static int create_common(const prc_geometry* geo, const char* isotope, const prc
     if (o.tile == PRC_TILE_AUTO && geo && density_host && out && o.cache >= PRC_CACHE_NONE &&
         o.cache <= PRC_CACHE_SOURCE_MAJOR) {
         RangeModel m;
-        if (m.resolve(isotope ? isotope : "")) o.tile = choose_tile(geo, isotope, o, density_host, surrogate);
+        if (m.resolve(isotope ? isotope : ""))
+            o.tile = choose_tile(geo, isotope, o, density_host, surrogate, batch_member);
     }
     return create_handle(geo, isotope, &o, density_host, net, surrogate, target_scale, fallback_nrmse, fallbacks, out,
                          batch_member);
+}
+
+int prc_tune_tile(const prc_geometry* geo, const char* isotope, const prc_options* opts_in, const float* density_host,
+                  int* tile) {
+    if (!geo || !density_host || !tile) return fail(PRC_ERR_ARGUMENT, "Invalid argument");
+    prc_options o;
+    prc_default_options(&o);
+    if (opts_in) o = *opts_in;
+    RangeModel m;
+    if (!m.resolve(isotope ? isotope : "")) return fail(PRC_ERR_ISOTOPE, std::string("Unknown isotope ") + (isotope ? isotope : "(null)"));
+    if (o.cache < PRC_CACHE_NONE || o.cache > PRC_CACHE_SOURCE_MAJOR)
+        return fail(PRC_ERR_ARGUMENT, "Invalid geometry or solver parameters");
+    *tile = choose_tile(geo, isotope, o, density_host, false, true);
+    return PRC_OK;
 }
 
 int prc_create(const prc_geometry* geo, const char* isotope, const prc_options* opts, const float* density_host,

@@ -64,7 +64,8 @@ void print_usage(const char* prog, FILE* stream = stderr) {  // the usage text o
             "  --cache MODE      none|near|source|full: weights kept on the GPU between passes (default full)\n"
             "  --bf16-weights    store the projector weights in bfloat16 (mixed precision)\n"
             "  --bf16-volumes    bfloat16 weights, and bfloat16 volumes gathered inside MAP-EM\n"
-            "  --tile SHAPE      auto|8x2x2|16x2x1|32x1x1|4x4x2|16x1x2: source tile of the stored field (default auto)\n"
+            "  --tile SHAPE      auto|tune|8x2x2|16x2x1|32x1x1|4x4x2|16x1x2: source tile of the stored field\n"
+            "                    (default auto; tune: time the candidates on a slab first)\n"
             "Isotopes:",
             prog);
     for (int i = 0; i < prc_isotope_count(); ++i) fprintf(stream, " %s", prc_isotope_name(i));
@@ -72,6 +73,8 @@ void print_usage(const char* prog, FILE* stream = stderr) {  // the usage text o
 }
 
 [[noreturn]] void die() { exit(EXIT_FAILURE); }
+
+constexpr int kTune = 100;  // --tile tune: run the tile autotuner before building
 
 // A whole-string decimal number.  The messages are the reference's, which its tests match.
 template <class T>
@@ -133,7 +136,8 @@ const Spec kSpecs[] = {
      }},
     {"--tile", true,
      [](Settings& s, const char* v, const char*) {
-         static const std::pair<const char*, int> shapes[] = {{"auto", PRC_TILE_AUTO},     {"8x2x2", PRC_TILE_8x2x2},
+         static const std::pair<const char*, int> shapes[] = {{"auto", PRC_TILE_AUTO},     {"tune", kTune},
+                                                              {"8x2x2", PRC_TILE_8x2x2},
                                                               {"16x2x1", PRC_TILE_16x2x1}, {"32x1x1", PRC_TILE_32x1x1},
                                                               {"4x4x2", PRC_TILE_4x4x2},   {"16x1x2", PRC_TILE_16x1x2}};
          s.tile = -1;  // an unknown shape fails the parameter check below
@@ -355,6 +359,11 @@ int main(int argc, char** argv) {
     if (rho_finite) {
         builder = std::thread([&] {
             const double tb = now_s();
+            if (opts.tile == kTune) {
+                int tuned = PRC_TILE_AUTO;
+                opts.tile = prc_tune_tile(&geo, o.isotope.c_str(), &opts, rho.data(), &tuned) == PRC_OK ? tuned
+                                                                                                       : PRC_TILE_AUTO;
+            }
             build.rc = prc_create(&geo, o.isotope.c_str(), &opts, rho.data(), &build.h);
             if (build.rc != PRC_OK) build.error = prc_last_error();
             build.seconds = now_s() - tb;

@@ -38,3 +38,13 @@ def test_automatic_tile_is_a_concrete_shape(fixture72):
     rho, x, y, shape, sp = fixture72
     with pm.Projector("68Ga", rho, sp, rays=32) as P:
         assert P.tile in TILES
+
+
+def test_tuned_tile_is_remembered_for_the_configuration():
+    from prc_mlem_b200 import phantoms
+    rho, truth, sp = phantoms.torso_phantom(shape=(40, 48, 48))
+    tile = pm.tune_tile("18F", rho, sp, rays=64)
+    assert tile in (pm.PRC_TILE_8x2x2, pm.PRC_TILE_16x2x1, pm.PRC_TILE_32x1x1)
+    assert pm.tune_tile("18F", rho, sp, rays=64) == tile  # remembered, not re-timed
+    with pm.Projector("18F", rho, sp, rays=64) as P:
+        assert P.tile == tile
