@@ -1121,6 +1121,8 @@ def run_tiles(args):
     out = {}
     for prec_name, prec in (("fp32", pm.PRC_PRECISION_FP32), ("bf16", pm.PRC_PRECISION_BF16)):
         for tile, shape in pm.TILE_SHAPES.items():
+            if args.tile != "auto" and "x".join(map(str, shape)) != args.tile:
+                continue
             P = pm.Projector(ISOTOPE, rho, spacing, rays=RAYS, support_rho=SUPPORT_RHO, precision=prec, tile=tile)
             o = torch.empty_like(d)
             s = torch.cuda.ExternalStream(P.stream)

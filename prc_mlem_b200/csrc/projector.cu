@@ -21,6 +21,7 @@
 // owns its column) or read from the group-interleaved cache.
 #include "engine.h"
 
+#include <algorithm>
 #include <cstdio>
 #include <type_traits>
 
@@ -28,7 +29,10 @@ namespace prc {
 namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
-constexpr int kWarps = 4;  // groups per block (default launch)
+#ifndef PRC_PROJ_WARPS
+#define PRC_PROJ_WARPS 4
+#endif
+constexpr int kWarps = PRC_PROJ_WARPS;  // groups per block (default launch)
 constexpr int kBlock = kWarps * kLanes;
 constexpr int kMaxWarps = 8;  // largest block of a (batched, autotuned) launch
 constexpr int kMaxBlock = kMaxWarps * kLanes;
@@ -417,7 +421,10 @@ __device__ __forceinline__ void project_group(const ProjParams& p, const OpArgs&
         constexpr int kElem = kBase == kFieldF32 ? 4 : 2;
         constexpr int kPackBytes = kPack * kLanes * kElem;
         constexpr int kPacksPerChunk = kChunk / kPackBytes;
-        constexpr int kBatch = 4;  // packs per batch: 16 steps in flight per lane
+#ifndef PRC_FIELD_BATCH
+#define PRC_FIELD_BATCH 4
+#endif
+        constexpr int kBatch = PRC_FIELD_BATCH;  // packs per batch: 16 steps in flight per lane
         const StreamLayout& lay = kGatherT ? p.tgt : p.src;
         const FarField& fld = kGatherT ? a.farT : a.far;
         const int* tmpl = kGatherT ? p.tmpl_neg : p.tmpl;
@@ -600,6 +607,9 @@ __device__ __forceinline__ void project_group(const ProjParams& p, const OpArgs&
     }
 }
 
+// Each warp handles exactly one group per launch, so the mbarriers of its ring are initialised
+// once and never reused: walking several groups per warp would need mbarrier.inval and a
+// fence.proxy.async before re-initialising them and refilling stages the warp has read.
 template <Op OP, bool EXACT, int NEAR_MODE, int FAR_MODE>
 __global__ void __launch_bounds__(kMaxBlock) project_kernel(const ProjParams p, const OpArgs a) {
     extern __shared__ __align__(128) unsigned char dyn_smem[];
