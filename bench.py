@@ -491,7 +491,7 @@ def compare_forms(args, rho, spacing, d_g, stream, l2_flush, value_fp32, correct
         out[name] = {"iters_per_s": round(v, 3), "nrmse_vs_fp32_field": nrmse(img, corrected_fp32),
                      "device_gb": round(Q.device_bytes / 1e9, 3), "setup_s": round(t_setup, 3)}
         if "surrogate" in kw:
-            out[name]["exact_fallback_share"] = round(Q.fallbacks / Q.n_active, 4)
+            out[name]["exact_fallback_share"] = round(Q.fallbacks / (Q.n_active * RAYS), 4)
         Q.close()
     return out, images
 
@@ -1091,7 +1091,7 @@ def run_surrogate_eval(args):
             out[name] = {"iters_per_s": round(3 * args.iterations / (e0.elapsed_time(e1) / 1e3), 2),
                          "nrmse_vs_fp32_field": nrmse(img, plain)}
             if "surrogate" in kw:
-                out[name]["exact_fallback_share"] = round(Q.fallbacks / Q.n_active, 4)
+                out[name]["exact_fallback_share"] = round(Q.fallbacks / (Q.n_active * RAYS), 4)
             Q.close()
             with pm.Projector(iso, np.ascontiguousarray(rho[sl]), spacing, rays=RAYS, support_rho=SUPPORT_RHO,
                               **kw) as C:

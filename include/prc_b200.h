@@ -115,10 +115,13 @@ int prc_create(const prc_geometry* geometry, const char* isotope, const prc_opti
  * prc_surrogate.h; NULL = the traced radial kernels of every source, i.e. the surrogate
  * representation without a network) from the density patch around the source.  No
  * counterpart in the reference.  target_scale is the factor the network was trained with.
- * With fallback_nrmse > 0 the ray tracer judges every source: where the predicted
- * coefficients differ from the traced ones by more than fallback_nrmse (relative L2) the
- * traced ones are used; *fallbacks (optional) receives their number.  The near block is
- * traced exactly.  Forward, adjoint and MAP-EM then work as for prc_create.  Synchronises. */
+ * The ray tracer judges every (source, far ray): a ray whose traced mass reaches more than 2%
+ * past the water-equivalent range of the bins, or (fallback_nrmse > 0) whose predicted
+ * coefficients differ from the traced ones by more than fallback_nrmse (relative L2 over its
+ * 16 bins), keeps its exact ray-marched weights, for all 32 sources of its stream group; the
+ * other rays store the coefficients of the water range.  *fallbacks (optional) receives the
+ * number of (source, far ray) pairs on exact weights (out of n_active x rays).  The near block
+ * is traced exactly.  Forward, adjoint and MAP-EM then work as for prc_create.  Synchronises. */
 typedef struct prc_net prc_net;
 int prc_create_surrogate(const prc_geometry* geometry, const char* isotope, const prc_options* opts,
                          const float* density_host, prc_net* net, float target_scale, float fallback_nrmse,

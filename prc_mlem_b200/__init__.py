@@ -212,7 +212,8 @@ class Projector:
                  precision: int = PRC_PRECISION_FP32, surrogate=None, target_scale: float = 1.0,
                  fallback_nrmse: float = 0.0, tile: int = PRC_TILE_AUTO):
         """surrogate: None for the plain projector; a trained network (prc_mlem_b200.surrogate.Network)
-        or the string "traced" for the radial coefficient field (prc_create_surrogate)."""
+        or the string "traced" for the radial coefficient field (prc_create_surrogate).
+        ``fallbacks`` then counts the (source, far ray) pairs the tracer kept on exact weights."""
         density = _host(density)
         if density.ndim != 3:
             raise ValueError("density must be a (nz, ny, nx) array")

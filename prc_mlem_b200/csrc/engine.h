@@ -97,9 +97,6 @@ struct OpArgs {
     unsigned int* error = nullptr;         // set non-zero when a stored-field copy timed out
     unsigned short* len = nullptr;         // Layout output
     long long* group_total = nullptr;      // Layout output: entries per group (sum of len * 32)
-    // Surrogate fields: groups whose flag is 1 keep exact traced weights (the Norm pass fills
-    // only those), the others hold radial coefficients (surrogate_fill fills only those).
-    const unsigned char* fallback_groups = nullptr;
     // Norm: fp32 accumulator of the traced near block, [group][125 offsets][32 lanes].  When set,
     // the near rays are traced one direction octant at a time into a 27-offset shared-memory tile
     // (3.4 KB per warp instead of 16 KB, so four times the warps fit on an SM).
@@ -132,12 +129,14 @@ cudaError_t build_radial_tables(const ProjParams& p, const RadialTables& t, cuda
 // voxels.  n_src must be a multiple of 32.
 cudaError_t radial_kernels(const ProjParams& p, const RadialTables& t, const int* src, int n_src,
                            int warps_per_volume, float* out, cudaStream_t s);
-// Surrogate field fill of the groups not flagged in a.fallback_groups: near block traced as in
-// the Norm pass (row 0), then 16 steps per far ray r from the coefficients
-// coef[src][r*16 + b] (bf16), dropped where the target voxel is outside the image or not
-// tissue; W_s = sum of all stored weights.
+// Surrogate field fill: near block traced as in the Norm pass (row 0); far ray r of group G
+// exactly traced into row 1 + r where fallback_rays[G * n_rays + r] is set (the Norm pass's
+// weights), otherwise its first `water_bins` radial coefficients coef[src][r*16 + b] (bf16) into
+// row 1 + n_rays + r, each dropped where its target voxel is outside the image or not tissue;
+// W_s = the sum of every stored weight.
 cudaError_t surrogate_fill(const ProjParams& p, const OpArgs& a, const RadialTables& t, const __nv_bfloat16* coef,
-                           const unsigned char* support, cudaStream_t s);
+                           const unsigned char* support, const unsigned char* fallback_rays, int water_bins,
+                           cudaStream_t s);
 // Template rows of the surrogate field: row 0 the near block, row 1 + r the 16 bin offsets.
 cudaError_t build_surrogate_template(const ProjParams& p, const RadialTables& t, int* tmpl, int* tmpl_neg,
                                      cudaStream_t s);
@@ -148,15 +147,16 @@ namespace prc {
 // Whole-volume CNN inference into bf16 coefficients coef[src][2048] (surrogate.cu).
 int surrogate_infer(prc_net* net, const float* rho, int nx, int ny, int nz, int iso, const int* active, int n_active,
                     float inv_target_scale, __nv_bfloat16* coef, cudaStream_t s);
-// Replaces the coefficients of sources [first, first + n_src) by traced ones (times scale)
-// where their relative L2 difference exceeds threshold; counts them in *replaced.
-// Sources whose far field is poorly represented are flagged: predicted and traced coefficients
-// differ by more than `threshold` (relative L2; skipped when threshold < 0), or more than
-// `beyond` of the traced mass lies past the water-equivalent cutoff distance (rays through lung
-// or air, where the radial bins are coarse).  Without a network (threshold < 0) the traced
-// coefficients are copied into coef.  flags[first + i] is set to 1 for flagged sources.
-cudaError_t surrogate_judge(__nv_bfloat16* coef, const float* traced, int n_src, int first, float threshold,
-                            float beyond, int water_bins, unsigned char* flags, cudaStream_t s);
+// The tracer's judgement of sources [first, first + n_src), ray by ray: a far ray of a source is
+// poorly represented when its predicted and traced coefficients differ by more than
+// `threshold` (relative L2 over the ray's 16 bins; skipped when threshold < 0), or when more
+// than `beyond` of its traced mass lies past the water-equivalent cutoff distance (a ray through
+// lung or out of the body, where the radial bins are coarse).  Without a network
+// (threshold < 0) the traced coefficients are copied into coef.  coef and traced hold n_rays x 16
+// bins per source; flags[(first + i) * n_rays + r] is set to 1 for a poorly represented ray r of
+// source first + i, 0 otherwise.
+cudaError_t surrogate_judge(__nv_bfloat16* coef, const float* traced, int n_src, int n_rays, int first,
+                            float threshold, float beyond, int water_bins, unsigned char* flags, cudaStream_t s);
 int radial_water_bins();
 
 // ---- batched projection over many volumes (one launch for all) --------------------------------

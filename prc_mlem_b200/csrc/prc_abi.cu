@@ -309,9 +309,11 @@ static int create_impl(prc_handle* h, const float* density_host, prc_net* net = 
 
 // The surrogate field (prc_create_surrogate).  Same stream format as the stored field; the
 // template has 1 + 2 n_rays rows: the near block, the exact steps of every far ray, and the 16
-// radial bins of every far ray.  A group whose sources the tracer judges poorly represented
-// (fallback) stores the near block and its exact ray steps (filled by the Norm pass); every
-// other group stores the near block and 16 radial coefficients per ray (surrogate_fill).
+// radial bins of every far ray.  The tracer judges every (source, far ray); a ray that some
+// source of a 32-source group represents poorly keeps its exact steps for the whole group (the
+// fallback), every other ray of the group stores the radial coefficients of its water range
+// (12 bins: the judge sends every ray with mass beyond it back).  One fill pass
+// (surrogate_fill) traces the near block, marches the fallback rays and writes the bins.
 static int build_surrogate_field(prc_handle* h, prc_net* net, float target_scale, float fallback_nrmse,
                                  int64_t* fallbacks) {
     ProjParams& p = h->params;
@@ -345,12 +347,14 @@ static int build_surrogate_field(prc_handle* h, prc_net* net, float target_scale
                                        1.0f / target_scale, coef, h->stream);
         if (rc != PRC_OK) return rc;
     }
-    // The tracer: judge of the predictions, and the coefficients themselves without a network.
-    unsigned char* flags = nullptr;
-    PRC_CUDA(cudaMalloc(&flags, h->n_active));
+    // The tracer: judge of the predictions, ray by ray, and the coefficients themselves without a
+    // network.  Rays with more than this share of their mass beyond the water range fall back.
+    const float beyond = 0.02f;
+    unsigned char* flags = nullptr;  // [n_active][n_rays]
+    PRC_CUDA(cudaMalloc(&flags, (size_t)h->n_active * n_rays));
     FreeDev free_flags{flags};
-    PRC_CUDA(cudaMemsetAsync(flags, 0, h->n_active, h->stream));
-    if (!net || fallback_nrmse > 0.0f) {
+    PRC_CUDA(cudaMemsetAsync(flags, 0, (size_t)h->n_active * n_rays, h->stream));
+    {
         const int chunk = 65536;  // sources per traced batch (multiple of 32)
         float* traced = nullptr;
         int* srcs = nullptr;
@@ -361,34 +365,39 @@ static int build_surrogate_field(prc_handle* h, prc_net* net, float target_scale
         std::vector<int> host_src(chunk);
         std::vector<int> act(h->n_active);
         PRC_CUDA(cudaMemcpy(act.data(), h->active, act.size() * sizeof(int), cudaMemcpyDeviceToHost));
-        // sources with more than this share of their far mass beyond the water range fall back
-        const float beyond = fallback_nrmse > 0.0f ? 0.02f : 2.0f;
         for (int first = 0; first < h->n_active; first += chunk) {
             const int n = std::min(chunk, h->n_active - first);
             const int padded = (n + kLanes - 1) / kLanes * kLanes;
             for (int i = 0; i < padded; ++i) host_src[i] = act[first + std::min(i, n - 1)];
             PRC_CUDA(cudaMemcpyAsync(srcs, host_src.data(), padded * sizeof(int), cudaMemcpyHostToDevice, h->stream));
             PRC_CUDA(radial_kernels(pm, tab, srcs, padded, 1 << 30, traced, h->stream));
-            PRC_CUDA(surrogate_judge(coef, traced, n, first, net ? fallback_nrmse : -1.0f, beyond,
-                                     radial_water_bins(), flags, h->stream));
+            // without the judge (fallback_nrmse == 0) a network's prediction is kept wherever
+            // its ray stays within the water range
+            PRC_CUDA(surrogate_judge(coef, traced, n, n_rays, first, net ? (fallback_nrmse > 0.0f ? fallback_nrmse : 1e30f) : -1.0f,
+                                     beyond, radial_water_bins(), flags, h->stream));
             PRC_CUDA(cudaStreamSynchronize(h->stream));
         }
     }
-    std::vector<unsigned char> src_flags(h->n_active);
+    // a group keeps a ray exact when any of its sources needs it
+    std::vector<unsigned char> src_flags((size_t)h->n_active * n_rays);
     PRC_CUDA(cudaMemcpy(src_flags.data(), flags, src_flags.size(), cudaMemcpyDeviceToHost));
-    std::vector<unsigned char> group_fb(h->n_groups, 0);
-    int64_t fb_sources = 0;
+    std::vector<unsigned char> ray_fb((size_t)h->n_groups * n_rays, 0);
     for (int i = 0; i < h->n_active; ++i)
-        if (src_flags[i]) group_fb[i / kLanes] = 1;
-    for (int gi = 0; gi < h->n_groups; ++gi)
-        if (group_fb[gi]) fb_sources += std::min(kLanes, h->n_active - gi * kLanes);
-    h->surrogate_fallbacks = fb_sources;
-    if (fallbacks) *fallbacks = fb_sources;
-    unsigned char* d_group_fb = nullptr;
-    PRC_CUDA(h->alloc(&d_group_fb, h->n_groups));
-    PRC_CUDA(cudaMemcpyAsync(d_group_fb, group_fb.data(), group_fb.size(), cudaMemcpyHostToDevice, h->stream));
+        for (int r = 0; r < n_rays; ++r)
+            if (src_flags[(size_t)i * n_rays + r]) ray_fb[(size_t)(i / kLanes) * n_rays + r] = 1;
+    int64_t fb_pairs = 0;  // (source, far ray) pairs on exact weights
+    for (int gi = 0; gi < h->n_groups; ++gi) {
+        const int lanes = std::min(kLanes, h->n_active - gi * kLanes);
+        for (int r = 0; r < n_rays; ++r) fb_pairs += ray_fb[(size_t)gi * n_rays + r] ? lanes : 0;
+    }
+    h->surrogate_fallbacks = fb_pairs;
+    if (fallbacks) *fallbacks = fb_pairs;
+    unsigned char* d_ray_fb = nullptr;
+    PRC_CUDA(h->alloc(&d_ray_fb, ray_fb.size()));
+    PRC_CUDA(cudaMemcpyAsync(d_ray_fb, ray_fb.data(), ray_fb.size(), cudaMemcpyHostToDevice, h->stream));
 
-    // Stream layout: exact lengths from a layout pass for fallback groups, 16 bins otherwise.
+    // Stream layout: the exact lengths of a layout pass for fallback rays, the water bins
+    // otherwise.
     p.n_rows = 1 + 2 * n_rays;
     p.tmpl_len = std::max(near_row_steps(), march_len);
     const size_t rows = (size_t)h->n_groups * p.n_rows;
@@ -406,14 +415,16 @@ static int build_surrogate_field(prc_handle* h, prc_net* net, float target_scale
     std::vector<unsigned short> len(rows);
     PRC_CUDA(cudaMemcpyAsync(len.data(), h->len, rows * sizeof(unsigned short), cudaMemcpyDeviceToHost, h->stream));
     PRC_CUDA(cudaStreamSynchronize(h->stream));
+    const int water_bins = (radial_water_bins() + 3) / 4 * 4;
     std::vector<long long> base(h->n_groups + 1);
     long long run = 0;
     for (int gi = 0; gi < h->n_groups; ++gi) {
         unsigned short* l = &len[(size_t)gi * p.n_rows];
         l[0] = (unsigned short)near_row_steps();
         for (int r = 0; r < n_rays; ++r) {
-            if (!group_fb[gi]) l[1 + r] = 0;
-            l[1 + n_rays + r] = group_fb[gi] ? 0 : kRadialBins;
+            const bool exact = ray_fb[(size_t)gi * n_rays + r];
+            if (!exact) l[1 + r] = 0;
+            l[1 + n_rays + r] = exact ? 0 : (unsigned short)water_bins;
         }
         base[gi] = run;
         for (int k = 0; k < p.n_rows; ++k) run += (long long)l[k] * kLanes;
@@ -429,13 +440,10 @@ static int build_surrogate_field(prc_handle* h, prc_net* net, float target_scale
     p.src.group_base = h->group_base;
     PRC_CUDA(build_descriptors(p, p.src, h->desc, h->stream));
     p.src.desc = h->desc;
-    OpArgs a = h->op_args();
-    a.fallback_groups = d_group_fb;
-    if (const int rc = run_norm(h, a); rc != PRC_OK) return rc;  // exact weights of the fallback groups
     {
-        OpArgs fa = a;
-        fa.near_acc = near_accumulator(h);  // the surrogate groups' near blocks, octant by octant
-        const cudaError_t e = surrogate_fill(p, fa, tab, coef, h->support, h->stream);
+        OpArgs fa = h->op_args();
+        fa.near_acc = near_accumulator(h);  // the near blocks, octant by octant
+        const cudaError_t e = surrogate_fill(p, fa, tab, coef, h->support, d_ray_fb, water_bins, h->stream);
         release_accumulator(h, fa.near_acc);
         PRC_CUDA(e);
     }

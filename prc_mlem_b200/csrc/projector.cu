@@ -310,7 +310,6 @@ __device__ __forceinline__ void project_group(const ProjParams& p, const OpArgs&
         if (valid && !live) a.out[s] = 0.0f;
     }
     if (!__any_sync(kFull, live)) return;
-    if (OP == Op::Norm && a.fallback_groups && !a.fallback_groups[group]) return;  // a surrogate group
     const int nx = p.g.nx, ny = p.g.ny;
     const int vx = s % nx, vy = (s / nx) % ny, vz = s / p.nxy;
 
@@ -904,16 +903,19 @@ __global__ void __launch_bounds__(kBlock) radial_kernel_kernel(ProjParams p, con
     }
 }
 
-// Surrogate field fill (see engine.h); the near block exactly as the Norm pass traces it.
+// Surrogate field fill (see engine.h); the near block exactly as the Norm pass traces it, then
+// every far ray either marched exactly (a ray the judge sent back, stored in its exact row as
+// the Norm pass stores it) or as its radial water bins.  The rows go in stream order: all exact
+// rows 1..n_rays, then all radial rows; a row the group does not use has length 0.
 template <bool EXACT, int FAR_MODE>
 __global__ void __launch_bounds__(kBlock) surrogate_fill_kernel(const ProjParams p, const OpArgs a,
                                                                 const RadialTables tab, const __nv_bfloat16* coef,
-                                                                const unsigned char* support) {
+                                                                const unsigned char* support,
+                                                                const unsigned char* fallback_rays, int water_bins) {
     extern __shared__ __align__(128) unsigned char dyn_smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int group = blockIdx.x * kWarps + warp;
     if (group * kLanes >= p.n_active) return;
-    if (a.fallback_groups && a.fallback_groups[group]) return;  // exact weights, filled by the Norm pass
     const int src = group * kLanes + lane;
     const bool valid = src < p.n_active;
     const int s = valid ? p.active[src] : 0;
@@ -921,6 +923,8 @@ __global__ void __launch_bounds__(kBlock) surrogate_fill_kernel(const ProjParams
     const int vx = s % nx, vy = (s / nx) % ny, vz = s / p.nxy;
     const FarField& f = a.far;
     const long long gbase = p.src.group_base[group];
+    const unsigned char* fb = fallback_rays + (size_t)group * p.n_rays;
+    const unsigned short* len = p.src.len + (size_t)group * p.n_rows;
     float acc = 0.0f;
     const float* near_sum;
     if (a.near_acc) {
@@ -947,20 +951,32 @@ __global__ void __launch_bounds__(kBlock) surrogate_fill_kernel(const ProjParams
         if (valid) store_weight<FAR_MODE>(f, pack_slot(gbase, q, lane), w);
     }
     long long rbase = gbase + (long long)kNearRow * kLanes;
-    for (int r = 0; r < p.n_rays; ++r) {
-        for (int b = 0; b < kRadialBins; ++b) {
-            const int xyz = tab.xyz[r * kRadialBins + b];
-            const int dx = (xyz & 1023) - 512, dy = ((xyz >> 10) & 1023) - 512, dz = ((xyz >> 20) & 1023) - 512;
-            const bool in = (unsigned)(vx + dx) < (unsigned)nx && (unsigned)(vy + dy) < (unsigned)ny &&
-                            (unsigned)(vz + dz) < (unsigned)nz;
-            float w = 0.0f;
-            if (valid && in && support[s + tab.offset[r * kRadialBins + b]])
-                w = fmaxf(__bfloat162float(coef[(size_t)src * (p.n_rays * kRadialBins) + r * kRadialBins + b]), 0.0f);
-            if (FAR_MODE == kFieldBF16) w = __bfloat162float(__float2bfloat16_rn(w));
-            acc += w;
-            if (valid) store_weight<FAR_MODE>(f, pack_slot(rbase, b, lane), w);
+    for (int r = 0; r < p.n_rays; ++r) {  // exact rows (prc.cu:220-226 as the Norm pass marches them)
+        if (fb[r]) {
+            march<false, EXACT>(p, p.far[r], valid, s, vx, vy, vz, [&](int, float w, int, int m) {
+                if (FAR_MODE == kFieldBF16) w = __bfloat162float(__float2bfloat16_rn(w));
+                acc += w;
+                store_weight<FAR_MODE>(f, pack_slot(rbase, m, lane), w);
+            });
         }
-        rbase += (long long)kRadialBins * kLanes;
+        rbase += (long long)len[1 + r] * kLanes;
+    }
+    for (int r = 0; r < p.n_rays; ++r) {  // radial rows
+        if (!fb[r]) {
+            for (int b = 0; b < water_bins; ++b) {
+                const int xyz = tab.xyz[r * kRadialBins + b];
+                const int dx = (xyz & 1023) - 512, dy = ((xyz >> 10) & 1023) - 512, dz = ((xyz >> 20) & 1023) - 512;
+                const bool in = (unsigned)(vx + dx) < (unsigned)nx && (unsigned)(vy + dy) < (unsigned)ny &&
+                                (unsigned)(vz + dz) < (unsigned)nz;
+                float w = 0.0f;
+                if (valid && in && support[s + tab.offset[r * kRadialBins + b]])
+                    w = fmaxf(__bfloat162float(coef[(size_t)src * (p.n_rays * kRadialBins) + r * kRadialBins + b]), 0.0f);
+                if (FAR_MODE == kFieldBF16) w = __bfloat162float(__float2bfloat16_rn(w));
+                acc += w;
+                if (valid) store_weight<FAR_MODE>(f, pack_slot(rbase, b, lane), w);
+            }
+        }
+        rbase += (long long)len[1 + p.n_rays + r] * kLanes;
     }
     if (valid) a.W[src] = acc;
 }
@@ -1173,7 +1189,8 @@ cudaError_t radial_kernels(const ProjParams& p, const RadialTables& t, const int
 }
 
 cudaError_t surrogate_fill(const ProjParams& p, const OpArgs& a, const RadialTables& t, const __nv_bfloat16* coef,
-                           const unsigned char* support, cudaStream_t s) {
+                           const unsigned char* support, const unsigned char* fallback_rays, int water_bins,
+                           cudaStream_t s) {
     const int groups = (p.n_active + kLanes - 1) / kLanes;
     if (groups == 0) return cudaSuccess;
     const int blocks = (groups + kWarps - 1) / kWarps;
@@ -1181,7 +1198,7 @@ cudaError_t surrogate_fill(const ProjParams& p, const OpArgs& a, const RadialTab
     auto launch_fill = [&](auto kernel) {
         cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
-        kernel<<<blocks, kBlock, smem, s>>>(p, a, t, coef, support);
+        kernel<<<blocks, kBlock, smem, s>>>(p, a, t, coef, support, fallback_rays, water_bins);
         return cudaGetLastError();
     };
     if (a.far.f32) return p.table ? launch_fill(surrogate_fill_kernel<false, kFieldF32>) : launch_fill(surrogate_fill_kernel<true, kFieldF32>);

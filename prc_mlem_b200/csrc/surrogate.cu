@@ -718,34 +718,38 @@ __global__ void padded_input_kernel(const float* rho, int nx, int ny, int nz, in
     }
 }
 
-// Judge (see surrogate_judge in engine.h); one warp per source.
-__global__ void judge_kernel(bf16* coef, const float* traced, int n_src, int first, float threshold, float beyond,
-                             int water_bins, unsigned char* flags) {
+// Judge (see surrogate_judge in engine.h); one warp per source, a half-warp per far ray (the 16
+// radial bins of a ray are one lane each).
+__global__ void judge_kernel(bf16* coef, const float* traced, int n_src, int n_rays, int first, float threshold,
+                             float beyond, int water_bins, unsigned char* flags) {
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (warp >= n_src) return;
-    bf16* c = coef + (size_t)(first + warp) * kOut;
-    const float* t = traced + (size_t)warp * kOut;
-    float num = 0.0f, den = 0.0f, mass = 0.0f, far = 0.0f;
-    for (int k = lane; k < kOut; k += 32) {
-        const float tv = t[k];
-        if (threshold >= 0.0f) {
+    const size_t per_src = (size_t)n_rays * 16;
+    bf16* c = coef + (size_t)(first + warp) * per_src;
+    const float* t = traced + (size_t)warp * per_src;
+    unsigned char* f = flags + (size_t)(first + warp) * n_rays;
+    const int bin = lane & 15;
+    for (int r0 = 0; r0 < n_rays; r0 += 2) {
+        const int r = r0 + (lane >> 4), k = r * 16 + bin;
+        const bool ray = r < n_rays;  // the second half-warp idles on an odd last ray
+        const float tv = ray ? t[k] : 0.0f;
+        float num = 0.0f;
+        if (ray && threshold >= 0.0f) {
             const float d = __bfloat162float(c[k]) - tv;
-            num += d * d;
-        } else {
+            num = d * d;
+        } else if (ray) {
             c[k] = __float2bfloat16_rn(tv);
         }
-        den += tv * tv;
-        mass += tv;
-        if ((k & 15) >= water_bins) far += tv;
+        float den = tv * tv, mass = tv, far = bin >= water_bins ? tv : 0.0f;
+        for (int off = 8; off > 0; off >>= 1) {  // within the half-warp of this ray
+            num += __shfl_xor_sync(0xffffffffu, num, off);
+            den += __shfl_xor_sync(0xffffffffu, den, off);
+            mass += __shfl_xor_sync(0xffffffffu, mass, off);
+            far += __shfl_xor_sync(0xffffffffu, far, off);
+        }
+        const bool bad = (threshold >= 0.0f && num > threshold * threshold * den) || far > beyond * mass;
+        if (ray && bin == 0) f[r] = bad ? 1 : 0;
     }
-    for (int off = 16; off > 0; off >>= 1) {
-        num += __shfl_xor_sync(0xffffffffu, num, off);
-        den += __shfl_xor_sync(0xffffffffu, den, off);
-        mass += __shfl_xor_sync(0xffffffffu, mass, off);
-        far += __shfl_xor_sync(0xffffffffu, far, off);
-    }
-    const bool bad = (threshold >= 0.0f && num > threshold * threshold * den) || far > beyond * mass;
-    if (lane == 0) flags[first + warp] = bad ? 1 : 0;
 }
 
 }  // namespace
@@ -794,10 +798,10 @@ int surrogate_infer(prc_net* net, const float* rho, int nx, int ny, int nz, int 
     return PRC_OK;
 }
 
-cudaError_t surrogate_judge(bf16* coef, const float* traced, int n_src, int first, float threshold, float beyond,
-                            int water_bins, unsigned char* flags, cudaStream_t s) {
-    judge_kernel<<<(n_src * 32 + 255) / 256, 256, 0, s>>>(coef, traced, n_src, first, threshold, beyond, water_bins,
-                                                          flags);
+cudaError_t surrogate_judge(bf16* coef, const float* traced, int n_src, int n_rays, int first, float threshold,
+                            float beyond, int water_bins, unsigned char* flags, cudaStream_t s) {
+    judge_kernel<<<(n_src * 32 + 255) / 256, 256, 0, s>>>(coef, traced, n_src, n_rays, first, threshold, beyond,
+                                                          water_bins, flags);
     return cudaGetLastError();
 }
 
