@@ -40,6 +40,9 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 METRIC = "EM iters/sec at 128x128x159 68Ga, learned vs plain projector, NRMSE<=1% vs FP64"
+# The tracer's judge of the learned surrogate keeps a predicted far ray when its error norm is at
+# most this multiple of the source's RMS ray norm (prc_create_surrogate's fallback_nrmse).
+JUDGE_THRESHOLD = 0.45
 ISOTOPE, RAYS, BETA, GAMMA, ITERS, SUPPORT_RHO, COUNTS = "68Ga", 128, 0.03, 20.0, 6, 0.05, 5e7
 L2_BYTES = 126 * 2**20
 REFERENCE_ARM_SECONDS = 150.0  # host seconds of projection the reference arm's timed steps share
@@ -642,7 +645,7 @@ def projector_forms(pm, sg, net):
         forms += [("learned_bf16", dict(precision=pm.PRC_PRECISION_BF16, surrogate=net,
                                         target_scale=sg.TARGET_SCALE)),
                   ("learned_judged_bf16", dict(precision=pm.PRC_PRECISION_BF16, surrogate=net,
-                                               target_scale=sg.TARGET_SCALE, fallback_nrmse=0.3))]
+                                               target_scale=sg.TARGET_SCALE, fallback_nrmse=JUDGE_THRESHOLD))]
     return forms
 
 
@@ -968,7 +971,7 @@ def batch_record(frames: int, iterations: int, steps: int, warmup: int, surrogat
     net = sg.load_trained() if surrogate else None
     t0 = time.perf_counter()
     batch = pm.Batch([(iso, rho, sp) for iso, rho, sp, _, _ in specs], precision=pm.PRC_PRECISION_BF16,
-                     surrogate=net, target_scale=sg.TARGET_SCALE, fallback_nrmse=0.3 if net else 0.0)
+                     surrogate=net, target_scale=sg.TARGET_SCALE, fallback_nrmse=JUDGE_THRESHOLD if net else 0.0)
     setup_s = time.perf_counter() - t0
     gs, outs = [], []
     for i, (iso, rho, sp, truth, counts) in enumerate(specs):
@@ -1066,7 +1069,7 @@ def run_surrogate_eval(args):
             forms += [("learned_bf16", dict(precision=pm.PRC_PRECISION_BF16, surrogate=net,
                                             target_scale=sg.TARGET_SCALE)),
                       ("learned_judged_bf16", dict(precision=pm.PRC_PRECISION_BF16, surrogate=net,
-                                                   target_scale=sg.TARGET_SCALE, fallback_nrmse=0.3))]
+                                                   target_scale=sg.TARGET_SCALE, fallback_nrmse=JUDGE_THRESHOLD))]
         out, plain = {}, None
         g = None
         for name, kw in forms:

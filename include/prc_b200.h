@@ -117,8 +117,9 @@ int prc_create(const prc_geometry* geometry, const char* isotope, const prc_opti
  * counterpart in the reference.  target_scale is the factor the network was trained with.
  * The ray tracer judges every (source, far ray): a ray whose traced mass reaches more than 2%
  * past the water-equivalent range of the bins, or (fallback_nrmse > 0) whose predicted
- * coefficients differ from the traced ones by more than fallback_nrmse (relative L2 over its
- * 16 bins), keeps its exact ray-marched weights, for all 32 sources of its stream group; the
+ * coefficients differ from the traced ones by more than fallback_nrmse times the source's RMS
+ * ray norm (L2 over the ray's 16 bins), keeps its exact ray-marched weights, for all 32 sources
+ * of its stream group; the
  * other rays store the coefficients of the water range.  *fallbacks (optional) receives the
  * number of (source, far ray) pairs on exact weights (out of n_active x rays).  The near block
  * is traced exactly.  Forward, adjoint and MAP-EM then work as for prc_create.  Synchronises. */

@@ -110,12 +110,14 @@ _SIGNATURES = {
     "prc_nn_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(_P)]),
     "prc_nn_destroy": (None, [_P]),
     "prc_nn_param_count": (ctypes.c_int64, []),
+    "prc_nn_patch_side": (ctypes.c_int, []),
     "prc_nn_set_params": (ctypes.c_int, [_P, _P]),
     "prc_nn_get": (ctypes.c_int, [_P, ctypes.c_int, _P]),
     "prc_nn_forward": (ctypes.c_int, [_P, _P, ctypes.c_int, _P, _P]),
     "prc_nn_backward": (ctypes.c_int, [_P, _P, ctypes.c_int, ctypes.c_float, ctypes.POINTER(ctypes.c_double), _P]),
     "prc_nn_make_samples": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_float, _P,
-                                           ctypes.c_uint64, ctypes.c_int, _P, _P, ctypes.c_float, _P]),
+                                           ctypes.c_uint64, ctypes.c_int, _P, _P, ctypes.c_float, ctypes.c_float,
+                                           _P]),
     "prc_eval_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _P, _P, _P, ctypes.c_int, _P, _P,
                                        _P, ctypes.c_double, ctypes.POINTER(ctypes.c_void_p)]),
     "prc_eval_sums": (ctypes.c_int, [_P, _P, _P, _P]),

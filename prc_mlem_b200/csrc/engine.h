@@ -148,16 +148,23 @@ namespace prc {
 int surrogate_infer(prc_net* net, const float* rho, int nx, int ny, int nz, int iso, const int* active, int n_active,
                     float inv_target_scale, __nv_bfloat16* coef, cudaStream_t s);
 // The tracer's judgement of sources [first, first + n_src), ray by ray: a far ray of a source is
-// poorly represented when its predicted and traced coefficients differ by more than
-// `threshold` (relative L2 over the ray's 16 bins; skipped when threshold < 0), or when more
-// than `beyond` of its traced mass lies past the water-equivalent cutoff distance (a ray through
-// lung or out of the body, where the radial bins are coarse).  Without a network
+// poorly represented when the L2 norm of (stored prediction - traced coefficients) over its 16
+// bins exceeds `threshold` times the source's RMS ray norm (the square root of the mean over
+// its rays of the traced squared norm; skipped when threshold < 0), or when more than `beyond`
+// of its traced mass lies past the water-equivalent cutoff distance (a ray through lung or out
+// of the body, where the radial bins are coarse).  The stored prediction is zero past the water
+// bins.  Without a network
 // (threshold < 0) the traced coefficients are copied into coef.  coef and traced hold n_rays x 16
 // bins per source; flags[(first + i) * n_rays + r] is set to 1 for a poorly represented ray r of
 // source first + i, 0 otherwise.
 cudaError_t surrogate_judge(__nv_bfloat16* coef, const float* traced, int n_src, int n_rays, int first,
                             float threshold, float beyond, int water_bins, unsigned char* flags, cudaStream_t s);
+// Radial bins of the water range (12, a multiple of 4): the coefficients a surrogate field stores
+// for a far ray.
 int radial_water_bins();
+// A far ray with more than this share of its traced mass past the water range keeps its exact
+// weights in a surrogate field (and trains no network output).
+constexpr float kBeyondShare = 0.02f;
 
 // ---- batched projection over many volumes (one launch for all) --------------------------------
 enum BatchMode : int {

@@ -348,8 +348,7 @@ static int build_surrogate_field(prc_handle* h, prc_net* net, float target_scale
         if (rc != PRC_OK) return rc;
     }
     // The tracer: judge of the predictions, ray by ray, and the coefficients themselves without a
-    // network.  Rays with more than this share of their mass beyond the water range fall back.
-    const float beyond = 0.02f;
+    // network.  Rays with more than kBeyondShare of their mass beyond the water range fall back.
     unsigned char* flags = nullptr;  // [n_active][n_rays]
     PRC_CUDA(cudaMalloc(&flags, (size_t)h->n_active * n_rays));
     FreeDev free_flags{flags};
@@ -374,7 +373,7 @@ static int build_surrogate_field(prc_handle* h, prc_net* net, float target_scale
             // without the judge (fallback_nrmse == 0) a network's prediction is kept wherever
             // its ray stays within the water range
             PRC_CUDA(surrogate_judge(coef, traced, n, n_rays, first, net ? (fallback_nrmse > 0.0f ? fallback_nrmse : 1e30f) : -1.0f,
-                                     beyond, radial_water_bins(), flags, h->stream));
+                                     kBeyondShare, radial_water_bins(), flags, h->stream));
             PRC_CUDA(cudaStreamSynchronize(h->stream));
         }
     }
@@ -415,7 +414,7 @@ static int build_surrogate_field(prc_handle* h, prc_net* net, float target_scale
     std::vector<unsigned short> len(rows);
     PRC_CUDA(cudaMemcpyAsync(len.data(), h->len, rows * sizeof(unsigned short), cudaMemcpyDeviceToHost, h->stream));
     PRC_CUDA(cudaStreamSynchronize(h->stream));
-    const int water_bins = (radial_water_bins() + 3) / 4 * 4;
+    const int water_bins = radial_water_bins();
     std::vector<long long> base(h->n_groups + 1);
     long long run = 0;
     for (int gi = 0; gi < h->n_groups; ++gi) {

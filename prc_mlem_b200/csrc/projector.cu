@@ -822,11 +822,10 @@ __global__ void forward_prep_half_kernel(const int* __restrict__ vox2src, const 
 }
 
 // ---- radial surrogate ------------------------------------------------------------------------
-// kWaterBins equal bins up to the cutoff, the rest equal up to 3.85 x cutoff.
-#ifndef PRC_RADIAL_WATER_BINS
-#define PRC_RADIAL_WATER_BINS 12
-#endif
-constexpr int kWaterBins = PRC_RADIAL_WATER_BINS;
+// kWaterBins equal bins up to the cutoff, the rest equal up to 3.85 x cutoff.  A surrogate field
+// stores the water bins of a ray (whole packs of 4 steps).
+constexpr int kWaterBins = 12;
+static_assert(kWaterBins % 4 == 0 && kWaterBins < kRadialBins, "the water bins fill whole packs");
 __device__ __forceinline__ float radial_edge(int b, float cutoff) {
     return b <= kWaterBins ? cutoff * b / kWaterBins
                            : cutoff * (1.0f + 2.85f * (b - kWaterBins) / (kRadialBins - kWaterBins));

@@ -61,18 +61,24 @@ extern "C" int prc_nn_gemm_bf16(const void* d_a, const void* d_b, float* d_c, in
 }
 
 // ================================================================================================
-// The network: 4 valid 3x3x3 convolutions (32 channels, ReLU) on a 9^3 patch, then a linear head
-// to 128 directions x 16 radial bins.  Tensors are channels-last; conv weights [cout][27][cin].
+// The network: 4 valid 3x3x3 convolutions (32 channels, ReLU) with dilations 1, 2, 3 and 4 on a
+// 21^3 patch (a voxel sees 10 voxels in every direction), then a linear head to 128 directions x
+// 16 radial bins.  Tensors are channels-last; conv weights [cout][27][cin].
 // Every GEMM below is an implicit GEMM on the tensor cores: the loaders compute the im2col (or
 // its transpose) addresses, the store functors apply bias, ReLU and the bf16 rounding.
 // ================================================================================================
 namespace {
 
 constexpr int kC = 32;           // channels of the hidden layers
-constexpr int kIn = 4;           // density + one-hot isotope (18F, 68Ga, 82Rb)
+constexpr int kIn = 8;           // density, inside-the-volume flag, one-hot isotope (18F, 68Ga, 82Rb), 3 zeros
 constexpr int kOut = 2048;       // 128 directions x 16 radial bins
 constexpr int kLayers = 5;       // 4 convolutions + head
-constexpr int kSide[5] = {9, 7, 5, 3, 1};  // spatial side of the input of layer l (l = 0..3), and a4
+constexpr int kDil[4] = {1, 2, 3, 4};       // tap spacing of convolution l
+constexpr int kSide[5] = {21, 19, 15, 9, 1};  // spatial side of the input of layer l (l = 0..3), and a4
+static_assert(kSide[0] == 1 + 2 * (kDil[0] + kDil[1] + kDil[2] + kDil[3]) && kSide[1] == kSide[0] - 2 * kDil[0] &&
+                  kSide[2] == kSide[1] - 2 * kDil[1] && kSide[3] == kSide[2] - 2 * kDil[2] &&
+                  kSide[4] == kSide[3] - 2 * kDil[3],
+              "each convolution trims its dilation from both sides");
 
 __device__ __forceinline__ void decode3(int p, int S, int& z, int& y, int& x) {
     z = p / (S * S);
@@ -80,29 +86,30 @@ __device__ __forceinline__ void decode3(int p, int S, int& z, int& y, int& x) {
     x = p % S;
 }
 
-// Forward convolution: out[(b,p)][cout] = relu(sum_{kpos,cin} x[b][p+kpos][cin] w[cout][kpos][cin] + bias)
+// Forward convolution with taps d apart:
+// out[(b,p)][cout] = relu(sum_{kpos,cin} x[b][p + d kpos][cin] w[cout][kpos][cin] + bias)
 struct ConvFwd {
     const bf16* x;
     const bf16* w;
     const float* bias;
     bf16* out;
-    int S, cin;  // input side and channels
+    int S, cin, d;  // input side, channels and dilation
     __device__ bf16 a(int m, int k) const {
-        const int So = S - 2, n3 = So * So * So, b = m / n3;
+        const int So = S - 2 * d, n3 = So * So * So, b = m / n3;
         int oz, oy, ox, kz, ky, kx;
         decode3(m % n3, So, oz, oy, ox);
         decode3(k / cin, 3, kz, ky, kx);
-        return x[((((size_t)b * S + oz + kz) * S + oy + ky) * S + ox + kx) * cin + k % cin];
+        return x[((((size_t)b * S + oz + kz * d) * S + oy + ky * d) * S + ox + kx * d) * cin + k % cin];
     }
     // 8 channels of one tap are contiguous when cin is a multiple of 8 (the 32-channel layers)
     __device__ bool vec_a() const { return cin % 8 == 0; }
     __device__ uint4 a8(int m, int k) const {
-        const int So = S - 2, n3 = So * So * So, b = m / n3;
+        const int So = S - 2 * d, n3 = So * So * So, b = m / n3;
         int oz, oy, ox, kz, ky, kx;
         decode3(m % n3, So, oz, oy, ox);
         decode3(k / cin, 3, kz, ky, kx);
-        return *reinterpret_cast<const uint4*>(x + ((((size_t)b * S + oz + kz) * S + oy + ky) * S + ox + kx) * cin +
-                                               k % cin);
+        return *reinterpret_cast<const uint4*>(
+            x + ((((size_t)b * S + oz + kz * d) * S + oy + ky * d) * S + ox + kx * d) * cin + k % cin);
     }
     __device__ bf16 b(int n, int k) const { return w[(size_t)n * 27 * cin + k]; }
     __device__ void store(int m, int n, float v) const {
@@ -111,29 +118,29 @@ struct ConvFwd {
 };
 
 // Data gradient of a convolution, masked by the previous layer's ReLU:
-// dz_prev[(b,pin)][cin] = (x[b][pin][cin] > 0) * sum_{kpos,cout} dz[b][pin-kpos][cout] w[cout][kpos][cin]
+// dz_prev[(b,pin)][cin] = (x[b][pin][cin] > 0) * sum_{kpos,cout} dz[b][pin - d kpos][cout] w[cout][kpos][cin]
 struct ConvDx {
     const bf16* dz;
     const bf16* w;
     const bf16* x;
     bf16* dz_prev;
-    int S;  // input side (output side S - 2); cin = cout = 32
+    int S, d;  // input side (output side S - 2d) and dilation; cin = cout = 32
     __device__ bf16 a(int m, int k) const {
-        const int So = S - 2, n3 = S * S * S, b = m / n3;
+        const int So = S - 2 * d, n3 = S * S * S, b = m / n3;
         int iz, iy, ix, kz, ky, kx;
         decode3(m % n3, S, iz, iy, ix);
         decode3(k / kC, 3, kz, ky, kx);
-        const int oz = iz - kz, oy = iy - ky, ox = ix - kx;
+        const int oz = iz - kz * d, oy = iy - ky * d, ox = ix - kx * d;
         if (oz < 0 || oy < 0 || ox < 0 || oz >= So || oy >= So || ox >= So) return __float2bfloat16(0.0f);
         return dz[((((size_t)b * So + oz) * So + oy) * So + ox) * kC + k % kC];
     }
     __device__ bool vec_a() const { return true; }
     __device__ uint4 a8(int m, int k) const {
-        const int So = S - 2, n3 = S * S * S, b = m / n3;
+        const int So = S - 2 * d, n3 = S * S * S, b = m / n3;
         int iz, iy, ix, kz, ky, kx;
         decode3(m % n3, S, iz, iy, ix);
         decode3(k / kC, 3, kz, ky, kx);
-        const int oz = iz - kz, oy = iy - ky, ox = ix - kx;
+        const int oz = iz - kz * d, oy = iy - ky * d, ox = ix - kx * d;
         if (oz < 0 || oy < 0 || ox < 0 || oz >= So || oy >= So || ox >= So) return make_uint4(0u, 0u, 0u, 0u);
         return *reinterpret_cast<const uint4*>(dz + ((((size_t)b * So + oz) * So + oy) * So + ox) * kC + k % kC);
     }
@@ -145,19 +152,19 @@ struct ConvDx {
     }
 };
 
-// Weight gradient: gw[cout][(kpos,cin)] = sum_{b,p} dz[b][p][cout] x[b][p+kpos][cin]; split-K
+// Weight gradient: gw[cout][(kpos,cin)] = sum_{b,p} dz[b][p][cout] x[b][p + d kpos][cin]; split-K
 // slices add into gw.
 struct ConvDw {
     const bf16* x;
     const bf16* dz;
     float* gw;
-    int S, cin;
+    int S, cin, d;
     __device__ bf16 a(int m, int k) const {
-        const int So = S - 2, n3 = So * So * So, b = k / n3;
+        const int So = S - 2 * d, n3 = So * So * So, b = k / n3;
         int oz, oy, ox, kz, ky, kx;
         decode3(k % n3, So, oz, oy, ox);
         decode3(m / cin, 3, kz, ky, kx);
-        return x[((((size_t)b * S + oz + kz) * S + oy + ky) * S + ox + kx) * cin + m % cin];
+        return x[((((size_t)b * S + oz + kz * d) * S + oy + ky * d) * S + ox + kx * d) * cin + m % cin];
     }
     __device__ bf16 b(int n, int k) const { return dz[(size_t)k * kC + n]; }
     __device__ void store(int m, int n, float v) const { atomicAdd(gw + (size_t)n * 27 * cin + m, v); }
@@ -297,11 +304,12 @@ cudaError_t run_problem(const P& prob, int M, int N, int K, int splits, unsigned
     return cudaGetLastError();
 }
 
-// loss and dy = bf16(2 (y - t) / (B * 2048)); FP64 sum of squared errors into *sse
+// loss and dy = bf16(2 (y - t) / (B * 2048)); FP64 sum of squared errors into *sse.  A negative
+// target marks an output the surrogate field never uses (no loss, no gradient).
 __global__ void loss_kernel(const float* y, const float* t, bf16* dy, size_t n, double* sse) {
     double acc = 0.0;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        const float d = y[i] - t[i];
+        const float d = t[i] < 0.0f ? 0.0f : y[i] - t[i];
         dy[i] = __float2bfloat16_rn(2.0f * d / (float)n);
         acc += (double)d * d;
     }
@@ -424,7 +432,9 @@ int prc_nn_create(int max_batch, prc_net** out) {
         if (e != cudaSuccess) return fail_cleanup(nn_fail(e, "prc_nn_create"));
     }
     const size_t B = (size_t)max_batch;
-    const size_t act_sizes[5] = {B * 729 * kIn, B * 343 * kC, B * 125 * kC, B * 27 * kC, B * kC};
+    auto cube = [](int side) { return (size_t)side * side * side; };
+    const size_t act_sizes[5] = {B * cube(kSide[0]) * kIn, B * cube(kSide[1]) * kC, B * cube(kSide[2]) * kC,
+                                 B * cube(kSide[3]) * kC, B * cube(kSide[4]) * kC};
     cudaError_t e = cudaSuccess;
     for (int i = 0; i < 5 && e == cudaSuccess; ++i) e = net_alloc(n, &n->act[i], act_sizes[i]);
     for (int i = 1; i < 5 && e == cudaSuccess; ++i) e = net_alloc(n, &n->dz[i], act_sizes[i]);
@@ -465,6 +475,8 @@ int prc_nn_set_params(prc_net* n, const float* host) {
     return PRC_OK;
 }
 
+int prc_nn_patch_side(void) { return kSide[0]; }
+
 int64_t prc_nn_param_count(void) {
     return (int64_t)kC * 27 * kIn + kC + 3 * ((int64_t)kC * 27 * kC + kC) + (int64_t)kOut * kC + kOut;
 }
@@ -484,17 +496,18 @@ int prc_nn_get(prc_net* n, int what, float* host) {
     return PRC_OK;
 }
 
-// Forward pass of a batch of patches d_x0 ([batch][9][9][9][4] bf16) into d_y ([batch][2048] fp32;
-// NULL = the network's own buffer), keeping the activations for a backward pass.
+// Forward pass of a batch of patches d_x0 ([batch][21][21][21][8] bf16) into d_y ([batch][2048]
+// fp32; NULL = the network's own buffer), keeping the activations for a backward pass.
 int prc_nn_forward(prc_net* n, const void* d_x0, int batch, float* d_y, void* stream) {
     if (!n || !d_x0 || batch <= 0 || batch > n->max_batch)
         return prc::set_last_error("Invalid argument"), PRC_ERR_ARGUMENT;
     const cudaStream_t s = static_cast<cudaStream_t>(stream);
-    NN_CUDA(cudaMemcpyAsync(n->act[0], d_x0, (size_t)batch * 729 * kIn * sizeof(bf16), cudaMemcpyDeviceToDevice, s),
+    const size_t patch = (size_t)kSide[0] * kSide[0] * kSide[0];
+    NN_CUDA(cudaMemcpyAsync(n->act[0], d_x0, (size_t)batch * patch * kIn * sizeof(bf16), cudaMemcpyDeviceToDevice, s),
             "prc_nn_forward");
     for (int l = 0; l < 4; ++l) {
-        const int S = kSide[l], So = S - 2, cin = l == 0 ? kIn : kC;
-        ConvFwd p{n->act[l], n->wb[l], n->b[l], n->act[l + 1], S, cin};
+        const int S = kSide[l], So = kSide[l + 1], cin = l == 0 ? kIn : kC;
+        ConvFwd p{n->act[l], n->wb[l], n->b[l], n->act[l + 1], S, cin, kDil[l]};
         const int rows = batch * So * So * So;
         if (So == 1) {  // one row per sample: split K, then bias + ReLU
             NN_CUDA(cudaMemsetAsync(n->split_acc, 0, (size_t)rows * kC * sizeof(float), s), "prc_nn_forward");
@@ -531,14 +544,14 @@ int prc_nn_backward(prc_net* n, const float* d_target, int batch, float lr, doub
     relu_grad_epilogue_kernel<<<64, 256, 0, s>>>(n->split_acc, n->act[4], n->dz[4], (size_t)batch * kC);
     // convolutions, last to first
     for (int l = 3; l >= 0; --l) {
-        const int S = kSide[l], So = S - 2, cin = l == 0 ? kIn : kC;
+        const int S = kSide[l], So = kSide[l + 1], cin = l == 0 ? kIn : kC;
         const int rows_out = batch * So * So * So;
-        ConvDw dw{n->act[l], n->dz[l + 1], n->gw[l], S, cin};
+        ConvDw dw{n->act[l], n->dz[l + 1], n->gw[l], S, cin, kDil[l]};
         const int k_tiles = (rows_out + prc::umma::kKT - 1) / prc::umma::kKT;
         NN_CUDA((run_problem<32>(dw, 27 * cin, kC, rows_out, (k_tiles + 7) / 8, n->error, s)), "prc_nn_backward");
         colsum_kernel<<<kC, 256, 0, s>>>(n->dz[l + 1], rows_out, kC, n->gb[l]);
         if (l > 0) {
-            ConvDx dx{n->dz[l + 1], n->wb[l], n->act[l], n->dz[l], S};
+            ConvDx dx{n->dz[l + 1], n->wb[l], n->act[l], n->dz[l], S, kDil[l]};
             NN_CUDA((run_problem<32>(dx, batch * S * S * S, kC, 27 * kC, 1, n->error, s)), "prc_nn_backward");
         }
     }
@@ -573,7 +586,7 @@ int prc_nn_backward(prc_net* n, const float* d_target, int batch, float lr, doub
 // ================================================================================================
 namespace {
 
-constexpr int kPatch = 9, kPatch3 = 729, kHalo = 4;
+constexpr int kPatch = kSide[0], kPatch3 = kPatch * kPatch * kPatch, kHalo = kPatch / 2;
 constexpr int kEllipsoids = 10;  // parameter slots per volume
 constexpr float kAir = 0.0012f;
 
@@ -588,8 +601,9 @@ __device__ __forceinline__ uint32_t hash32(uint64_t x) {
 __device__ __forceinline__ float unit(uint64_t key) { return (hash32(key) >> 8) * (1.0f / 16777216.0f); }
 
 // Volume v: air, then up to 10 ellipsoids (cx, cy, cz, rx, ry, rz [voxels], density, used) painted
-// in order, then 5 % Gaussian multiplicative jitter (Box-Muller on a hash of the voxel).
-__global__ void paint_kernel(float* rho, int n, const float* ell, int n_vol, uint64_t seed) {
+// in order, then Gaussian multiplicative jitter of relative spread `jitter` (Box-Muller on a hash
+// of the voxel).
+__global__ void paint_kernel(float* rho, int n, const float* ell, int n_vol, uint64_t seed, float jitter) {
     const size_t per = (size_t)n * n * n;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < per * n_vol; i += (size_t)gridDim.x * blockDim.x) {
         const int v = (int)(i / per);
@@ -604,7 +618,7 @@ __global__ void paint_kernel(float* rho, int n, const float* ell, int n_vol, uin
         }
         const float u1 = fmaxf(unit(seed * 0x9E3779B97F4A7C15ULL + 2 * i), 1e-7f), u2 = unit(seed * 0x9E3779B97F4A7C15ULL + 2 * i + 1);
         const float g = sqrtf(-2.0f * logf(u1)) * cospif(2.0f * u2);
-        rho[i] = fmaxf(r * (1.0f + 0.05f * g), prc::kMinDensity);
+        rho[i] = fmaxf(r * (1.0f + jitter * g), prc::kMinDensity);
     }
 }
 
@@ -623,7 +637,17 @@ __global__ void pick_kernel(const float* rho, int n, int n_vol, int per_vol, flo
     src[i] = pick;
 }
 
-// Patch of sample i: density / 2 (air beyond the volume) and the one-hot isotope.
+// The input channels of one voxel: density / 2 (air beyond the volume), 1 inside the volume and 0
+// beyond it (a ray stops at the volume's edge but runs on through air inside it), the one-hot
+// isotope, and three zeros (8 channels: one 16-byte row per tap for the tensor-core loader).
+__device__ __forceinline__ void write_input(bf16* o, float r, bool inside, int iso) {
+    o[0] = __float2bfloat16_rn(0.5f * r);
+    o[1] = __float2bfloat16_rn(inside ? 1.0f : 0.0f);
+    for (int c = 0; c < 3; ++c) o[2 + c] = __float2bfloat16_rn(c == iso ? 1.0f : 0.0f);
+    for (int c = 5; c < kIn; ++c) o[c] = __float2bfloat16_rn(0.0f);
+}
+
+// Patch of sample i (channels of write_input).
 __global__ void patch_kernel(const float* rho, int n, int per_vol, const int* src, int n_src, int iso, bf16* out) {
     const size_t total = (size_t)n_src * kPatch3;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
@@ -633,9 +657,7 @@ __global__ void patch_kernel(const float* rho, int n, int per_vol, const int* sr
                   z = s / (n * n) + q / (kPatch * kPatch) - kHalo;
         const bool in = (unsigned)x < (unsigned)n && (unsigned)y < (unsigned)n && (unsigned)z < (unsigned)n;
         const float r = in ? rho[(size_t)v * n * n * n + ((size_t)z * n + y) * n + x] : kAir;
-        bf16* o = out + i * kIn;
-        o[0] = __float2bfloat16_rn(0.5f * r);
-        for (int c = 0; c < 3; ++c) o[1 + c] = __float2bfloat16_rn(c == iso ? 1.0f : 0.0f);
+        write_input(out + i * kIn, r, in, iso);
     }
 }
 
@@ -643,22 +665,40 @@ __global__ void scale_kernel(float* x, size_t n, float s) {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) x[i] *= s;
 }
 
+// Marks (-1) the targets a surrogate field never takes from the network: the bins past the
+// water range, and every bin of a ray with more than `beyond` of its mass past it (the tracer's
+// judge keeps such rays exact).  One thread per (sample, ray) of 16 bins.
+__global__ void mask_targets_kernel(float* t, size_t n_rays_total, int water_bins, float beyond) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n_rays_total; i += (size_t)gridDim.x * blockDim.x) {
+        float* r = t + i * 16;
+        float mass = 0.0f, far = 0.0f;
+        for (int b = 0; b < 16; ++b) {
+            mass += r[b];
+            far += b >= water_bins ? r[b] : 0.0f;
+        }
+        const bool drop = far > beyond * mass;
+        for (int b = 0; b < 16; ++b)
+            if (drop || b >= water_bins) r[b] = -1.0f;
+    }
+}
+
 // Whole-volume inference.  The input lives on the volume padded by kHalo voxels of air on every
-// side; every layer is a 'same' 3x3x3 convolution on that padded grid (zero beyond it), which
-// equals the valid convolutions of training on the 9^3 patch of every voxel of the volume.
+// side; every layer is a 'same' dilated 3x3x3 convolution on that padded grid (zero beyond it),
+// which equals the valid convolutions of training on the 21^3 patch of every voxel of the volume
+// (the halo is the sum of the dilations, so no tap of a volume voxel's cone reaches the zeros).
 struct ConvSame {
     const bf16* x;
     const bf16* w;
     const float* bias;
     bf16* out;
-    int pz, py, px, cin;
+    int pz, py, px, cin, d;
     __device__ bf16 a(int m, int k) const {
         int z, y, x0, kz, ky, kx;
         z = m / (py * px);
         y = (m / px) % py;
         x0 = m % px;
         decode3(k / cin, 3, kz, ky, kx);
-        const int zz = z + kz - 1, yy = y + ky - 1, xx = x0 + kx - 1;
+        const int zz = z + (kz - 1) * d, yy = y + (ky - 1) * d, xx = x0 + (kx - 1) * d;
         if ((unsigned)zz >= (unsigned)pz || (unsigned)yy >= (unsigned)py || (unsigned)xx >= (unsigned)px)
             return __float2bfloat16(0.0f);
         return x[(((size_t)zz * py + yy) * px + xx) * cin + k % cin];
@@ -668,7 +708,7 @@ struct ConvSame {
         const int z = m / (py * px), y = (m / px) % py, x0 = m % px;
         int kz, ky, kx;
         decode3(k / cin, 3, kz, ky, kx);
-        const int zz = z + kz - 1, yy = y + ky - 1, xx = x0 + kx - 1;
+        const int zz = z + (kz - 1) * d, yy = y + (ky - 1) * d, xx = x0 + (kx - 1) * d;
         if ((unsigned)zz >= (unsigned)pz || (unsigned)yy >= (unsigned)py || (unsigned)xx >= (unsigned)px)
             return make_uint4(0u, 0u, 0u, 0u);
         return *reinterpret_cast<const uint4*>(x + (((size_t)zz * py + yy) * px + xx) * cin + k % cin);
@@ -712,9 +752,7 @@ __global__ void padded_input_kernel(const float* rho, int nx, int ny, int nz, in
         const int x = (int)(i % px) - kHalo, y = (int)((i / px) % py) - kHalo, z = (int)(i / ((size_t)px * py)) - kHalo;
         const bool in = (unsigned)x < (unsigned)nx && (unsigned)y < (unsigned)ny && (unsigned)z < (unsigned)nz;
         const float r = in ? rho[((size_t)z * ny + y) * nx + x] : kAir;
-        bf16* o = out + i * kIn;
-        o[0] = __float2bfloat16_rn(0.5f * r);
-        for (int c = 0; c < 3; ++c) o[1 + c] = __float2bfloat16_rn(c == iso ? 1.0f : 0.0f);
+        write_input(out + i * kIn, r, in, iso);
     }
 }
 
@@ -729,25 +767,28 @@ __global__ void judge_kernel(bf16* coef, const float* traced, int n_src, int n_r
     const float* t = traced + (size_t)warp * per_src;
     unsigned char* f = flags + (size_t)(first + warp) * n_rays;
     const int bin = lane & 15;
+    float ray_energy = 0.0f;  // mean over the source's rays of the traced squared norm
+    for (int k = lane; k < n_rays * 16; k += 32) ray_energy += t[k] * t[k];
+    for (int off = 16; off > 0; off >>= 1) ray_energy += __shfl_xor_sync(0xffffffffu, ray_energy, off);
+    ray_energy /= n_rays;
     for (int r0 = 0; r0 < n_rays; r0 += 2) {
         const int r = r0 + (lane >> 4), k = r * 16 + bin;
         const bool ray = r < n_rays;  // the second half-warp idles on an odd last ray
         const float tv = ray ? t[k] : 0.0f;
-        float num = 0.0f;
+        float err = 0.0f;
         if (ray && threshold >= 0.0f) {
-            const float d = __bfloat162float(c[k]) - tv;
-            num = d * d;
+            const float d = bin < water_bins ? __bfloat162float(c[k]) - tv : -tv;  // what the field stores
+            err = d * d;
         } else if (ray) {
             c[k] = __float2bfloat16_rn(tv);
         }
-        float den = tv * tv, mass = tv, far = bin >= water_bins ? tv : 0.0f;
+        float mass = tv, far = bin >= water_bins ? tv : 0.0f;
         for (int off = 8; off > 0; off >>= 1) {  // within the half-warp of this ray
-            num += __shfl_xor_sync(0xffffffffu, num, off);
-            den += __shfl_xor_sync(0xffffffffu, den, off);
+            err += __shfl_xor_sync(0xffffffffu, err, off);
             mass += __shfl_xor_sync(0xffffffffu, mass, off);
             far += __shfl_xor_sync(0xffffffffu, far, off);
         }
-        const bool bad = (threshold >= 0.0f && num > threshold * threshold * den) || far > beyond * mass;
+        const bool bad = (threshold >= 0.0f && err > threshold * threshold * ray_energy) || far > beyond * mass;
         if (ray && bin == 0) f[r] = bad ? 1 : 0;
     }
 }
@@ -783,7 +824,7 @@ int surrogate_infer(prc_net* net, const float* rho, int nx, int ny, int nz, int 
     bf16* out = buf1;
     for (int l = 0; l < 4; ++l) {
         const int cin = l == 0 ? kIn : kC;
-        ConvSame c{in, net->wb[l], net->b[l], out, pz, py, px, cin};
+        ConvSame c{in, net->wb[l], net->b[l], out, pz, py, px, cin, kDil[l]};
         NN_CUDA((run_problem<32>(c, (int)pv, kC, 27 * cin, 1, net->error, s)), "surrogate inference");
         bf16* t = in;
         in = out;
@@ -809,15 +850,16 @@ cudaError_t surrogate_judge(bf16* coef, const float* traced, int n_src, int n_ra
 
 extern "C" int prc_nn_make_samples(const char* isotope, int n_vol, int side, float spacing_mm, const float* ellipsoids,
                                    uint64_t seed, int per_vol, void* d_patches, float* d_targets, float target_scale,
-                                   void* stream) {
+                                   float jitter, void* stream) {
     using namespace prc;
     static const char* kIsos[3] = {"18F", "68Ga", "82Rb"};
     int iso = -1;
     for (int i = 0; i < 3; ++i)
         if (isotope && std::string(isotope) == kIsos[i]) iso = i;
     if (iso < 0 || n_vol <= 0 || side < 8 || per_vol <= 0 || per_vol % kLanes || !ellipsoids || !d_patches ||
-        !d_targets || !(spacing_mm > 0))
-        return set_last_error("Invalid argument: isotope must be 18F, 68Ga or 82Rb; per_vol a multiple of 32"),
+        !d_targets || !(spacing_mm > 0) || !(jitter >= 0.0f && jitter <= 0.5f))
+        return set_last_error("Invalid argument: isotope must be 18F, 68Ga or 82Rb; per_vol a multiple of 32; "
+                              "jitter in [0, 0.5]"),
                PRC_ERR_ARGUMENT;
     const cudaStream_t s = static_cast<cudaStream_t>(stream);
     RangeModel model;
@@ -870,12 +912,15 @@ extern "C" int prc_nn_make_samples(const char* isotope, int n_vol, int side, flo
     for (int b = 0; b < 3; ++b) p.br[b] = model.br[b];
     p.tmpl_len = tmpl_len;
     NN_CUDA(build_radial_tables(p, tab, s), "make_samples");
-    paint_kernel<<<2048, 256, 0, s>>>(rho, side, ell, n_vol, seed);
+    paint_kernel<<<2048, 256, 0, s>>>(rho, side, ell, n_vol, seed, jitter);
     pick_kernel<<<(n_vol * per_vol + 255) / 256, 256, 0, s>>>(rho, side, n_vol, per_vol, g.support_rho, seed, src);
     NN_CUDA(radial_kernels(p, tab, src, n_vol * per_vol, per_vol / kLanes, d_targets, s), "make_samples");
     scale_kernel<<<1024, 256, 0, s>>>(d_targets, (size_t)n_vol * per_vol * kOut, target_scale);
+    mask_targets_kernel<<<1024, 256, 0, s>>>(d_targets, (size_t)n_vol * per_vol * (kOut / 16), radial_water_bins(),
+                                             kBeyondShare);
     patch_kernel<<<2048, 256, 0, s>>>(rho, side, per_vol, src, n_vol * per_vol, iso, static_cast<bf16*>(d_patches));
     NN_CUDA(cudaGetLastError(), "make_samples");
     NN_CUDA(cudaStreamSynchronize(s), "make_samples");
     return PRC_OK;
 }
+
