@@ -116,13 +116,13 @@ int prc_create(const prc_geometry* geometry, const char* isotope, const prc_opti
  * representation without a network) from the density patch around the source.  No
  * counterpart in the reference.  target_scale is the factor the network was trained with.
  * The ray tracer judges every (source, far ray): a ray whose traced mass reaches more than 2%
- * past the water-equivalent range of the bins, or (fallback_nrmse > 0) whose predicted
- * coefficients differ from the traced ones by more than fallback_nrmse times the source's RMS
- * ray norm (L2 over the ray's 16 bins), keeps its exact ray-marched weights, for all 32 sources
- * of its stream group; the
- * other rays store the coefficients of the water range.  *fallbacks (optional) receives the
- * number of (source, far ray) pairs on exact weights (out of n_active x rays).  The near block
- * is traced exactly.  Forward, adjoint and MAP-EM then work as for prc_create.  Synchronises. */
+ * past the water-equivalent range of the bins, with a network every ray the volume's edge cuts
+ * inside that range, and (fallback_nrmse > 0) every ray whose predicted coefficients differ
+ * from the traced ones by more than fallback_nrmse times the source's RMS ray norm (L2 over
+ * the ray's 16 bins) keeps its exact ray-marched weights, for all 32 sources of its stream
+ * group; the other rays store the coefficients of the water range.  *fallbacks (optional)
+ * receives the number of (source, far ray) pairs on exact weights (out of n_active x rays).
+ * The near block is traced exactly.  Forward, adjoint and MAP-EM then work as for prc_create.  Synchronises. */
 typedef struct prc_net prc_net;
 int prc_create_surrogate(const prc_geometry* geometry, const char* isotope, const prc_options* opts,
                          const float* density_host, prc_net* net, float target_scale, float fallback_nrmse,

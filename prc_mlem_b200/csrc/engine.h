@@ -152,13 +152,16 @@ int surrogate_infer(prc_net* net, const float* rho, int nx, int ny, int nz, int 
 // bins exceeds `threshold` times the source's RMS ray norm (the square root of the mean over
 // its rays of the traced squared norm; skipped when threshold < 0), or when more than `beyond`
 // of its traced mass lies past the water-equivalent cutoff distance (a ray through lung or out
-// of the body, where the radial bins are coarse).  The stored prediction is zero past the water
-// bins.  Without a network
-// (threshold < 0) the traced coefficients are copied into coef.  coef and traced hold n_rays x 16
-// bins per source; flags[(first + i) * n_rays + r] is set to 1 for a poorly represented ray r of
-// source first + i, 0 otherwise.
+// of the body, where the radial bins are coarse), or (threshold >= 0) when the volume's edge
+// cuts it inside the water range (the voxel of its last water bin, from the packed offsets
+// bin_xyz of RadialTables::xyz, lies outside the nx x ny x nz volume: a truncated kernel).  The
+// stored prediction is zero past the water bins.  Sources are active[first + i].  Without a
+// network (threshold < 0) the traced coefficients are copied into coef.  coef and traced hold
+// n_rays x 16 bins per source; flags[(first + i) * n_rays + r] is set to 1 for a poorly
+// represented ray r of source first + i, 0 otherwise.
 cudaError_t surrogate_judge(__nv_bfloat16* coef, const float* traced, int n_src, int n_rays, int first,
-                            float threshold, float beyond, int water_bins, unsigned char* flags, cudaStream_t s);
+                            float threshold, float beyond, int water_bins, const int* active, const int* bin_xyz,
+                            int nx, int ny, int nz, unsigned char* flags, cudaStream_t s);
 // Radial bins of the water range (12, a multiple of 4): the coefficients a surrogate field stores
 // for a far ray.
 int radial_water_bins();

@@ -373,7 +373,8 @@ static int build_surrogate_field(prc_handle* h, prc_net* net, float target_scale
             // without the judge (fallback_nrmse == 0) a network's prediction is kept wherever
             // its ray stays within the water range
             PRC_CUDA(surrogate_judge(coef, traced, n, n_rays, first, net ? (fallback_nrmse > 0.0f ? fallback_nrmse : 1e30f) : -1.0f,
-                                     kBeyondShare, radial_water_bins(), flags, h->stream));
+                                     kBeyondShare, radial_water_bins(), h->active, tab.xyz, g.nx, g.ny, g.nz, flags,
+                                     h->stream));
             PRC_CUDA(cudaStreamSynchronize(h->stream));
         }
     }

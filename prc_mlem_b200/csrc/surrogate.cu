@@ -759,9 +759,12 @@ __global__ void padded_input_kernel(const float* rho, int nx, int ny, int nz, in
 // Judge (see surrogate_judge in engine.h); one warp per source, a half-warp per far ray (the 16
 // radial bins of a ray are one lane each).
 __global__ void judge_kernel(bf16* coef, const float* traced, int n_src, int n_rays, int first, float threshold,
-                             float beyond, int water_bins, unsigned char* flags) {
+                             float beyond, int water_bins, const int* active, const int* bin_xyz, int nx, int ny,
+                             int nz, unsigned char* flags) {
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (warp >= n_src) return;
+    const int s = active[first + warp];
+    const int vx = s % nx, vy = (s / nx) % ny, vz = s / (nx * ny);
     const size_t per_src = (size_t)n_rays * 16;
     bf16* c = coef + (size_t)(first + warp) * per_src;
     const float* t = traced + (size_t)warp * per_src;
@@ -788,7 +791,15 @@ __global__ void judge_kernel(bf16* coef, const float* traced, int n_src, int n_r
             mass += __shfl_xor_sync(0xffffffffu, mass, off);
             far += __shfl_xor_sync(0xffffffffu, far, off);
         }
-        const bool bad = (threshold >= 0.0f && err > threshold * threshold * ray_energy) || far > beyond * mass;
+        // a ray cut by the volume's edge inside the water range (the voxel of its last water bin
+        // lies outside; the volume is convex, so the earlier bins lie inside): a truncated kernel
+        bool cut = false;
+        if (ray) {
+            const int xyz = bin_xyz[r * 16 + water_bins - 1];
+            const int x = vx + (xyz & 1023) - 512, y = vy + ((xyz >> 10) & 1023) - 512, z = vz + ((xyz >> 20) & 1023) - 512;
+            cut = (unsigned)x >= (unsigned)nx || (unsigned)y >= (unsigned)ny || (unsigned)z >= (unsigned)nz;
+        }
+        const bool bad = (threshold >= 0.0f && (cut || err > threshold * threshold * ray_energy)) || far > beyond * mass;
         if (ray && bin == 0) f[r] = bad ? 1 : 0;
     }
 }
@@ -840,9 +851,10 @@ int surrogate_infer(prc_net* net, const float* rho, int nx, int ny, int nz, int 
 }
 
 cudaError_t surrogate_judge(bf16* coef, const float* traced, int n_src, int n_rays, int first, float threshold,
-                            float beyond, int water_bins, unsigned char* flags, cudaStream_t s) {
+                            float beyond, int water_bins, const int* active, const int* bin_xyz, int nx, int ny,
+                            int nz, unsigned char* flags, cudaStream_t s) {
     judge_kernel<<<(n_src * 32 + 255) / 256, 256, 0, s>>>(coef, traced, n_src, n_rays, first, threshold, beyond,
-                                                          water_bins, flags);
+                                                          water_bins, active, bin_xyz, nx, ny, nz, flags);
     return cudaGetLastError();
 }
 
