@@ -203,3 +203,22 @@ def test_trained_network_gains_over_the_method_without_it(small):
         with pm.Projector("68Ga", rho, sp, surrogate=n, target_scale=sg.TARGET_SCALE) as Q:
             errs[name] = np.linalg.norm(Q.forward_host(truth) - ref) / np.linalg.norm(ref)
     assert errs["learned"] < errs["blind"], errs
+
+
+def test_judge_keeps_rays_cut_by_the_volume_edge_exact():
+    """With a network, the tracer also keeps exact every far ray that the volume's edge cuts
+    inside the water range (a truncated kernel): on a thin torso slab, whose sources mostly lie
+    near a cut face, more (source, ray) pairs stay exact than with the traced coefficients, which
+    keep exact only the rays that reach past the water range."""
+    from prc_mlem_b200 import phantoms, surrogate as sg
+    net = sg.load_trained()
+    if net is None:
+        pytest.skip("no trained weights committed")
+    rho, truth, sp = phantoms.torso_phantom(seed=2, shape=(24, 128, 128))
+    with pm.Projector("68Ga", rho, sp, surrogate="traced") as Q:
+        beyond_only = Q.fallbacks
+    with pm.Projector("68Ga", rho, sp, surrogate=net, target_scale=sg.TARGET_SCALE) as Q:
+        with_cut = Q.fallbacks
+        total = Q.n_active * 128
+    assert beyond_only < with_cut < total
+    assert with_cut - beyond_only > 0.05 * total  # most rays toward the two faces 12 voxels away
