@@ -637,7 +637,8 @@ def image_quality(truth, measured, corrected):
 
 def projector_forms(pm, sg, net):
     """The projector forms compared with the headline fp32 field: (name, Projector keywords)."""
-    forms = [("bf16_field", dict(cache=pm.PRC_CACHE_FULL, precision=pm.PRC_PRECISION_BF16)),
+    forms = [("fp24_field", dict(cache=pm.PRC_CACHE_FULL, precision=pm.PRC_PRECISION_FP24)),
+             ("bf16_field", dict(cache=pm.PRC_CACHE_FULL, precision=pm.PRC_PRECISION_BF16)),
              ("bf16_volumes", dict(cache=pm.PRC_CACHE_FULL, precision=pm.PRC_PRECISION_BF16_VOLUMES)),
              ("traced", dict(cache=pm.PRC_CACHE_NEAR, precision=pm.PRC_PRECISION_FP32)),
              ("radial_traced_bf16", dict(precision=pm.PRC_PRECISION_BF16, surrogate="traced"))]

@@ -40,8 +40,13 @@ enum {
 enum {
     PRC_PRECISION_FP32 = 0,        /* float weights: the reference's numerics */
     PRC_PRECISION_BF16 = 1,        /* bfloat16 stored weights, float accumulation, FP64 global sums */
-    PRC_PRECISION_BF16_VOLUMES = 2 /* as PRC_PRECISION_BF16, and inside MAP-EM the volumes the
+    PRC_PRECISION_BF16_VOLUMES = 2, /* as PRC_PRECISION_BF16, and inside MAP-EM the volumes the
                                       projections gather (y / W and the EM ratio) in bfloat16 too */
+    PRC_PRECISION_FP24 = 3          /* stored-field weights of 24 bits (the non-negative fp32 weight
+                                      without its sign bit and rounded to 16 mantissa bits: relative
+                                      error <= 2^-17), float near cache,
+                                      accumulation and volumes; 3/4 of the fp32 field's bytes.  Not
+                                      for surrogate fields. */
 };
 
 /* What the projector keeps in device memory between projections.  The reference caches the

@@ -27,6 +27,7 @@ PRC_OK = 0
 PRC_PRECISION_FP32 = 0
 PRC_PRECISION_BF16 = 1
 PRC_PRECISION_BF16_VOLUMES = 2
+PRC_PRECISION_FP24 = 3
 PRC_CACHE_NONE = 0
 PRC_CACHE_NEAR = 1
 PRC_CACHE_FULL = 2

@@ -66,7 +66,10 @@ struct ProjParams {
 struct FarField {
     float* f32 = nullptr;
     __nv_bfloat16* b16 = nullptr;
-    __host__ __device__ bool on() const { return f32 || b16; }
+    // 24-bit weights: bits 30..7 of each (non-negative) fp32 weight rounded to nearest (8 exponent
+    // bits, 16 mantissa bits), little-endian, 3 bytes per entry
+    unsigned char* b24 = nullptr;
+    __host__ __device__ bool on() const { return f32 || b16 || b24; }
 };
 
 // Near-field weight cache, group-interleaved: entry (source src, block offset q) lives at
@@ -177,7 +180,9 @@ enum BatchMode : int {
     kBatchFieldF32 = 3,        // stored field, source-major (adjoint gather / forward scatter)
     kBatchFieldBF16 = 4,
     kBatchFieldF32T = 5,       // stored field, target-major (forward gather of u = f / W)
-    kBatchFieldBF16T = 6
+    kBatchFieldBF16T = 6,
+    kBatchField24 = 7,         // the 24-bit field, source-major and target-major
+    kBatchField24T = 8
 };
 struct BatchItem {
     ProjParams p;

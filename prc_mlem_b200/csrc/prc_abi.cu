@@ -275,8 +275,9 @@ static int build_target_major(prc_handle* h, const std::vector<int>& active, siz
     const size_t desc_count = (size_t)(run / (4 * kLanes));
     // keep room for the MAP-EM volumes and the transient row offsets
     if ((size_t)run * elem + desc_count * 4 + rows * 6 + 16 * h->n * 4 > free_b) return PRC_OK;
-    const bool bf16 = elem == 2;
-    cudaError_t e = bf16 ? h->alloc(&h->far_t.b16, (size_t)run) : h->alloc(&h->far_t.f32, (size_t)run);
+    cudaError_t e = elem == 2   ? h->alloc(&h->far_t.b16, (size_t)run)
+                    : elem == 3 ? h->alloc(&h->far_t.b24, (size_t)run * 3)
+                                : h->alloc(&h->far_t.f32, (size_t)run);
     if (e == cudaSuccess) e = h->alloc(&h->desc_t, desc_count);
     if (e == cudaSuccess) e = h->alloc(&h->len_t, rows);
     if (e == cudaSuccess) e = h->alloc(&h->group_base_t, (size_t)h->n_groups + 1);
@@ -318,6 +319,8 @@ static int build_surrogate_field(prc_handle* h, prc_net* net, float target_scale
                                  int64_t* fallbacks) {
     ProjParams& p = h->params;
     const Grid& g = h->g;
+    if (h->opts.precision == PRC_PRECISION_FP24)
+        return fail(PRC_ERR_ARGUMENT, "surrogate fields hold fp32 or bf16 weights (not PRC_PRECISION_FP24)");
     const bool bf16 = h->opts.precision != PRC_PRECISION_FP32;
     const int n_rays = h->opts.rays;
     const int march_len = (int)(((long long)g.nx + g.ny + g.nz + 6) / 4 * 4);
@@ -533,8 +536,9 @@ static int create_impl(prc_handle* h, const float* density_host, prc_net* net, b
     PRC_CUDA(setup_rays(g, h->opts.rays, h->far, h->near_rays, h->stream));
     PRC_CUDA(order_near_rays(h->near_rays, h->near_order, h->near_start, h->stream));
 
-    const bool bf16 = h->opts.precision != PRC_PRECISION_FP32;
-    const size_t elem = bf16 ? 2 : 4;
+    const bool bf16 = h->opts.precision == PRC_PRECISION_BF16 || h->opts.precision == PRC_PRECISION_BF16_VOLUMES;
+    const bool fp24 = h->opts.precision == PRC_PRECISION_FP24;  // the stored field only
+    const size_t elem = bf16 ? 2 : (fp24 ? 3 : 4);
     h->trace_near = true;
     if (surrogate) {
         int rc = build_surrogate_field(h, net, target_scale, fallback_nrmse, fallbacks);
@@ -581,7 +585,9 @@ static int create_impl(prc_handle* h, const float* density_host, prc_net* net, b
         PRC_CUDA(cudaMemGetInfo(&free_b, &total_b));
         const size_t desc_count = (size_t)(run / (4 * kLanes));
         if ((size_t)run * elem + desc_count * 4 <= free_b / 2) {
-            cudaError_t e = bf16 ? h->alloc(&h->far_field.b16, (size_t)run) : h->alloc(&h->far_field.f32, (size_t)run);
+            cudaError_t e = bf16   ? h->alloc(&h->far_field.b16, (size_t)run)
+                            : fp24 ? h->alloc(&h->far_field.b24, (size_t)run * 3)
+                                   : h->alloc(&h->far_field.f32, (size_t)run);
             if (e == cudaSuccess) e = h->alloc(&h->desc, desc_count);
             if (e == cudaSuccess) {
                 PRC_CUDA(cudaMemcpyAsync(h->group_base, totals.data(), totals.size() * sizeof(long long),
@@ -606,7 +612,7 @@ static int create_impl(prc_handle* h, const float* density_host, prc_net* net, b
         // a batch member keeps a near cache whenever it fits: retracing 2048 near rays per
         // source every pass would dominate the whole batch
         const size_t limit = batch_member ? (free_b > ((size_t)1 << 30) ? free_b - ((size_t)1 << 30) : 0) : free_b / 4;
-        if (entries * elem <= limit) {
+        if (entries * (bf16 ? 2 : 4) <= limit) {  // the near cache is fp32 unless bf16
             cudaError_t e = bf16 ? h->alloc(&h->cache.b16, entries) : h->alloc(&h->cache.f32, entries);
             if (e == cudaSuccess) h->trace_near = false, h->cache_mode = PRC_CACHE_NEAR;
             else cudaGetLastError();  // optional: fall back to retracing
@@ -636,7 +642,7 @@ static int create_handle(const prc_geometry* geo, const char* isotope, const prc
         !std::isfinite(geo->dx) || !std::isfinite(geo->dy) || !std::isfinite(geo->dz) || o.rays < 2 ||
         (o.rays & 1) || o.rays > INT_MAX - 31 || !(o.support_rho >= 0) || !(o.air_cap_mm > 0) ||
         !std::isfinite(o.support_rho) || !std::isfinite(o.air_cap_mm) ||
-        o.precision < PRC_PRECISION_FP32 || o.precision > PRC_PRECISION_BF16_VOLUMES || o.cache < PRC_CACHE_NONE ||
+        o.precision < PRC_PRECISION_FP32 || o.precision > PRC_PRECISION_FP24 || o.cache < PRC_CACHE_NONE ||
         o.cache > PRC_CACHE_SOURCE_MAJOR || o.tile < PRC_TILE_AUTO || o.tile > PRC_TILE_16x1x2 ||
         !(target_scale > 0) || !(fallback_nrmse >= 0))
         return fail(PRC_ERR_ARGUMENT, "Invalid geometry or solver parameters");
@@ -1183,8 +1189,9 @@ struct prc_batch {
 namespace {
 
 int batch_mode(const prc_handle* h, Op op) {
-    if (op == Op::Forward && h->far_t.on()) return h->far_t.b16 ? kBatchFieldBF16T : kBatchFieldF32T;
-    if (h->far_field.on()) return h->far_field.b16 ? kBatchFieldBF16 : kBatchFieldF32;
+    if (op == Op::Forward && h->far_t.on())
+        return h->far_t.b16 ? kBatchFieldBF16T : (h->far_t.b24 ? kBatchField24T : kBatchFieldF32T);
+    if (h->far_field.on()) return h->far_field.b16 ? kBatchFieldBF16 : (h->far_field.b24 ? kBatchField24 : kBatchFieldF32);
     if (!h->trace_near && h->cache.on()) return h->cache.b16 ? kBatchCacheBF16March : kBatchCacheF32March;
     return kBatchTraceMarch;
 }
@@ -1493,11 +1500,12 @@ int prc_batch_create(int n_frames, const prc_frame* frames, const prc_options* o
             if (cudaMemGetInfo(&free_b2, &total_b2) != cudaSuccess) break;
             size_t caller = (size_t)8 << 30;
             for (prc_handle* o : b->frames) caller += 3 * o->n * sizeof(float);
-            const size_t need = (size_t)((double)h->far_entries * (h->far_field.b16 ? 2 : 4) * 1.05) + caller;
+            const size_t elem_b = h->far_field.b16 ? 2 : (h->far_field.b24 ? 3 : 4);
+            const size_t need = (size_t)((double)h->far_entries * elem_b * 1.05) + caller;
             if (free_b2 < need) continue;
             std::vector<int> act(h->n_active);
             if (cudaMemcpy(act.data(), h->active, act.size() * sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) break;
-            const int rc = build_target_major(h, act, h->far_field.b16 ? 2 : 4);
+            const int rc = build_target_major(h, act, elem_b);
             if (rc != PRC_OK) {
                 prc_batch_destroy(b);
                 return rc;

@@ -37,7 +37,7 @@ struct Settings {
     int rays = 128, iterations = 20, save_every = 0;
     float beta = 0.2f, gamma = 20.0f, support_rho = 0.05f, air_cap_mm = 50.0f;
     bool reproject = false, trace_near_every_pass = false, exact_range = false, plain = false, bf16 = false;
-    bool bf16_volumes = false;
+    bool bf16_volumes = false, fp24 = false;
     int cache = PRC_CACHE_FULL;
     int tile = PRC_TILE_AUTO;
 };
@@ -64,6 +64,7 @@ void print_usage(const char* prog, FILE* stream = stderr) {  // the usage text o
             "  --cache MODE      none|near|source|full: weights kept on the GPU between passes (default full)\n"
             "  --bf16-weights    store the projector weights in bfloat16 (mixed precision)\n"
             "  --bf16-volumes    bfloat16 weights, and bfloat16 volumes gathered inside MAP-EM\n"
+            "  --fp24-weights    store the stored-field weights in 24 bits (fp32 rounded to 16 mantissa bits)\n"
             "  --tile SHAPE      auto|tune|8x2x2|16x2x1|32x1x1|4x4x2|16x1x2: source tile of the stored field\n"
             "                    (default auto; tune: time the candidates on a slab first)\n"
             "Isotopes:",
@@ -124,6 +125,7 @@ const Spec kSpecs[] = {
     {"--no-accel", false, [](Settings& s, const char*, const char*) { s.plain = true; }},
     {"--bf16-weights", false, [](Settings& s, const char*, const char*) { s.bf16 = true; }},
     {"--bf16-volumes", false, [](Settings& s, const char*, const char*) { s.bf16 = s.bf16_volumes = true; }},
+    {"--fp24-weights", false, [](Settings& s, const char*, const char*) { s.fp24 = true; }},
     {"--cache", true,
      [](Settings& s, const char* v, const char*) {
          static const std::pair<const char*, int> modes[] = {{"none", PRC_CACHE_NONE},
@@ -347,7 +349,10 @@ int main(int argc, char** argv) {
     opts.air_cap_mm = o.air_cap_mm;
     opts.exact_range = o.exact_range;
     opts.cache = o.trace_near_every_pass ? PRC_CACHE_NONE : o.cache;
-    opts.precision = o.bf16_volumes ? PRC_PRECISION_BF16_VOLUMES : o.bf16 ? PRC_PRECISION_BF16 : PRC_PRECISION_FP32;
+    opts.precision = o.bf16_volumes ? PRC_PRECISION_BF16_VOLUMES
+                     : o.bf16       ? PRC_PRECISION_BF16
+                     : o.fp24       ? PRC_PRECISION_FP24
+                                    : PRC_PRECISION_FP32;
     opts.tile = o.tile;
     struct Build {
         prc_handle* h = nullptr;

@@ -151,11 +151,16 @@ enum NearMode : int { kTraceNear = 0, kCacheF32 = 1, kCacheBF16 = 2 };
 // kFieldBF16H / kFieldBF16TH: the bf16 field gathering a bf16 volume (a.in16) -- inside
 // MAP-EM the mixed-precision form keeps the gathered volumes (u = y / W and the EM ratio) in
 // bf16, and its forward epilogue writes the ratio as bf16 (a.out16).
+// kField24 / kField24T: the 24-bit field (FarField::b24) of PRC_PRECISION_FP24.
 enum FarMode : int { kMarch = 0, kFieldF32 = 1, kFieldBF16 = 2, kFieldF32T = 3, kFieldBF16T = 4, kFieldBF16H = 5,
-                     kFieldBF16TH = 6 };
-__host__ __device__ constexpr bool target_major(int m) { return m == kFieldF32T || m == kFieldBF16T || m == kFieldBF16TH; }
+                     kFieldBF16TH = 6, kField24 = 7, kField24T = 8 };
+__host__ __device__ constexpr bool target_major(int m) {
+    return m == kFieldF32T || m == kFieldBF16T || m == kFieldBF16TH || m == kField24T;
+}
 __host__ __device__ constexpr bool half_volume(int m) { return m == kFieldBF16H || m == kFieldBF16TH; }
-__host__ __device__ constexpr int field_base(int m) { return m == kFieldF32 || m == kFieldF32T ? kFieldF32 : kFieldBF16; }
+__host__ __device__ constexpr int field_base(int m) {
+    return m == kFieldF32 || m == kFieldF32T ? kFieldF32 : (m == kField24 || m == kField24T ? kField24 : kFieldBF16);
+}
 
 // ---- stored coefficient field ----------------------------------------------------------------
 // Stream of one group: template row 0 is the near block (125 offsets, padded to kNearRow
@@ -167,7 +172,7 @@ __host__ __device__ constexpr int field_base(int m) { return m == kFieldF32 || m
 // walking the stream.
 constexpr int kPack = 4;
 constexpr int kNearRow = 128;  // 125 block offsets rounded up to whole packs
-// TMA ring of the fp32 field stream: kStages chunks of kChunk bytes per warp.  The bf16 form
+// TMA ring of the fp32 and 24-bit field streams: kStages chunks of kChunk bytes per warp.  The bf16 form
 // loads its vectors directly and keeps the reservation only for the L1 / shared-memory split it
 // gives (launched without it, with the largest L1, it measured 1.7-2x slower).
 constexpr int kStages = 2;
@@ -220,6 +225,7 @@ __device__ __forceinline__ uint2 ld_stream(const uint2* q) {
     return x;
 }
 
+
 __device__ __forceinline__ int near_offset(const ProjParams& p, int q) {
     const int dx = q % kNearSide - kNearR, dy = q / kNearSide % kNearSide - kNearR,
               dz = q / (kNearSide * kNearSide) - kNearR;
@@ -231,9 +237,42 @@ __device__ __forceinline__ long long pack_slot(long long row_base, int m, int la
     return row_base + (long long)(m / kPack) * (kPack * kLanes) + lane * kPack + m % kPack;
 }
 
+// The 24-bit weight of a non-negative finite w: bits 30..7 of its fp32 pattern (the sign is
+// always 0; 8 exponent and 16 mantissa bits) rounded to nearest, ties to even (a carry into the
+// exponent gives the next binade's value, as it should).  Relative error at most 2^-17.
+// Stream layout: every pack (4 steps x 32 lanes, 128 entries) is 384 bytes, the upper 16 bits of
+// its 128 values (256 bytes, entry order: lane L's four at 8 L) and then their low bytes (128
+// bytes, lane L's four at 256 + 4 L), so a lane loads one 8-byte and one 4-byte vector per pack.
+__device__ __forceinline__ unsigned bits24(float w) {
+    const unsigned u = __float_as_uint(w);
+    return (u + 0x3Fu + ((u >> 7) & 1u)) >> 7;
+}
+__device__ __forceinline__ float round24(float w) { return __uint_as_float(bits24(w) << 7); }
+__device__ __forceinline__ float load24(const unsigned char* b, long long e) {
+    const unsigned char* pack = b + (e >> 7) * 384;
+    const int i = (int)(e & 127);
+    const unsigned hi = *reinterpret_cast<const unsigned short*>(pack + 2 * i), lo = pack[256 + i];
+    return __uint_as_float(((hi << 8) | lo) << 7);
+}
+__device__ __forceinline__ void store24(unsigned char* b, long long e, unsigned v) {
+    unsigned char* pack = b + (e >> 7) * 384;
+    const int i = (int)(e & 127);
+    *reinterpret_cast<unsigned short*>(pack + 2 * i) = (unsigned short)(v >> 8);
+    pack[256 + i] = (unsigned char)v;
+}
+// The four weights of one lane's pack: hi = their upper 16-bit halves (two per word), lo = their
+// low bytes.  Each weight's three bytes go to the top of a word, then one bit down (bits 30..7).
+__device__ __forceinline__ void decode24(uint2 hi, unsigned lo, float* w) {
+    w[0] = __uint_as_float((__byte_perm(hi.x, lo, 0x1044) & 0xFFFFFF00u) >> 1);
+    w[1] = __uint_as_float((__byte_perm(hi.x, lo, 0x3255) & 0xFFFFFF00u) >> 1);
+    w[2] = __uint_as_float((__byte_perm(hi.y, lo, 0x1066) & 0xFFFFFF00u) >> 1);
+    w[3] = __uint_as_float((__byte_perm(hi.y, lo, 0x3277) & 0xFFFFFF00u) >> 1);
+}
+
 template <int FAR_MODE>
 __device__ __forceinline__ void store_weight(const FarField& f, long long e, float w) {
     if constexpr (FAR_MODE == kFieldF32) f.f32[e] = w;
+    else if constexpr (FAR_MODE == kField24) store24(f.b24, e, bits24(w));
     else f.b16[e] = __float2bfloat16_rn(w);
 }
 
@@ -327,6 +366,7 @@ __device__ __forceinline__ void project_group(const ProjParams& p, const OpArgs&
         // are rounded before they are accumulated.
         const bool near_round = OP == Op::Norm && (a.near.b16 || a.far.b16);
         const bool far_round = OP == Op::Norm && a.far.b16;
+        const bool round_24 = OP == Op::Norm && a.far.b24;  // W sums the weights as stored
 
         // Near block (prc.cu:193-218).
         if constexpr (OP != Op::Layout) {
@@ -359,10 +399,12 @@ __device__ __forceinline__ void project_group(const ProjParams& p, const OpArgs&
                     w = in ? near_sum[q * kLanes] * near_scale : 0.0f;
                     if constexpr (OP == Op::Norm) {
                         if (near_round) w = __bfloat162float(__float2bfloat16_rn(w));
+                        if (round_24) w = round24(w);
                         if (valid && a.near.b16) a.near.b16[cache_base + (size_t)q * kLanes] = __float2bfloat16_rn(w);
                         if (valid && a.near.f32) a.near.f32[cache_base + (size_t)q * kLanes] = w;
                         if (field && valid) {
                             if (a.far.f32) store_weight<kFieldF32>(a.far, pack_slot(gbase, q, lane), w);
+                            else if (a.far.b24) store_weight<kField24>(a.far, pack_slot(gbase, q, lane), w);
                             else store_weight<kFieldBF16>(a.far, pack_slot(gbase, q, lane), w);
                         }
                     }
@@ -392,9 +434,11 @@ __device__ __forceinline__ void project_group(const ProjParams& p, const OpArgs&
             } else if constexpr (OP == Op::Norm) {
                 march<false, EXACT>(p, R, live, s, vx, vy, vz, [&](int, float w, int, int m) {
                     if (far_round) w = __bfloat162float(__float2bfloat16_rn(w));
+                    if (round_24) w = round24(w);
                     acc += w;
                     if (field) {
                         if (a.far.f32) store_weight<kFieldF32>(a.far, pack_slot(rbase, m, lane), w);
+                        else if (a.far.b24) store_weight<kField24>(a.far, pack_slot(rbase, m, lane), w);
                         else store_weight<kFieldBF16>(a.far, pack_slot(rbase, m, lane), w);
                     }
                 });
@@ -404,7 +448,7 @@ __device__ __forceinline__ void project_group(const ProjParams& p, const OpArgs&
             }
         }
     } else {
-        // Stored field.  fp32: streamed by TMA -- lane 0 keeps kStages bulk copies of kChunk bytes in
+        // Stored field.  fp32 and 24-bit: streamed by TMA -- lane 0 keeps kStages bulk copies of kChunk bytes in
         // flight into this warp's shared-memory ring (cp.async.bulk, completion counted by an
         // mbarrier), so the weights arrive as contiguous DRAM bursts without holding
         // registers.  A chunk is consumed in batches of kBatch packs: the packs' template
@@ -417,13 +461,16 @@ __device__ __forceinline__ void project_group(const ProjParams& p, const OpArgs&
         // batch instead of three.
         constexpr bool kGatherT = OP == Op::Forward && target_major(FAR_MODE);
         constexpr int kBase = field_base(FAR_MODE);  // kFieldF32 / kFieldBF16
-        constexpr int kElem = kBase == kFieldF32 ? 4 : 2;
+        constexpr int kElem = kBase == kFieldF32 ? 4 : (kBase == kField24 ? 3 : 2);
         constexpr int kPackBytes = kPack * kLanes * kElem;
-        constexpr int kPacksPerChunk = kChunk / kPackBytes;
 #ifndef PRC_FIELD_BATCH
 #define PRC_FIELD_BATCH 4
 #endif
         constexpr int kBatch = PRC_FIELD_BATCH;  // packs per batch: 16 steps in flight per lane
+        // whole batches per ring chunk (24-bit packs of 384 bytes: 4 per 1536-byte chunk)
+        constexpr int kPacksPerChunk = kChunk / kPackBytes / kBatch * kBatch;
+        constexpr int kChunkBytes = kPacksPerChunk * kPackBytes;
+        static_assert(kPacksPerChunk > 0 && kChunkBytes % 16 == 0, "bulk copies of whole 16-byte units");
         const StreamLayout& lay = kGatherT ? p.tgt : p.src;
         const FarField& fld = kGatherT ? a.farT : a.far;
         const int* tmpl = kGatherT ? p.tmpl_neg : p.tmpl;
@@ -443,7 +490,9 @@ __device__ __forceinline__ void project_group(const ProjParams& p, const OpArgs&
             // bf16 form: each lane loads its own 8-byte vectors straight from HBM (a warp's loads
             // of one pack coalesce into 256 contiguous bytes) one batch ahead of their use.  This
             // form is bound by L1 wavefronts, not bytes, and skipping the shared-memory ring
-            // (its copies in and its reads out) measured 5 % faster than the TMA stream.
+            // (its copies in and its reads out) measured 5 % faster than the TMA stream.  (The
+            // 24-bit form loaded the same way, with a second 4-byte vector per pack, measured
+            // within 1.5 % of its TMA stream and is streamed like fp32.)
             const uint2* vec = reinterpret_cast<const uint2*>(fld.b16) + e0 / kPack + lane;
             auto load_vec = [&](int P) {
                 uint2 x = make_uint2(0u, 0u);
@@ -493,15 +542,17 @@ __device__ __forceinline__ void project_group(const ProjParams& p, const OpArgs&
             }
         } else {
             unsigned char* ring = dyn_smem + (size_t)warp * kStages * kChunk;
+            // a group's stream starts at a multiple of 128 entries: 16-byte aligned in every format
             const char* src_bytes = (kBase == kFieldF32 ? reinterpret_cast<const char*>(fld.f32)
-                                                        : reinterpret_cast<const char*>(fld.b16)) + e0 * kElem;
+                                     : kBase == kField24 ? reinterpret_cast<const char*>(fld.b24)
+                                                         : reinterpret_cast<const char*>(fld.b16)) + e0 * kElem;
             const long long total = (e1 - e0) * kElem;
             const int n_chunks = (n_packs + kPacksPerChunk - 1) / kPacksPerChunk;
             auto issue = [&](int c) {  // lane 0 only
                 const int stage = c % kStages;
-                const unsigned bytes = (unsigned)min((long long)kChunk, total - (long long)c * kChunk);
+                const unsigned bytes = (unsigned)min((long long)kChunkBytes, total - (long long)c * kChunkBytes);
                 mbar_expect_tx(&bars[stage], bytes);
-                bulk_copy_g2s(ring + stage * kChunk, src_bytes + (long long)c * kChunk, bytes, &bars[stage]);
+                bulk_copy_g2s(ring + stage * kChunk, src_bytes + (long long)c * kChunkBytes, bytes, &bars[stage]);
             };
             if (lane == 0) {
                 for (int k = 0; k < kStages; ++k) mbar_init(&bars[k], 1);
@@ -546,6 +597,10 @@ __device__ __forceinline__ void project_group(const ProjParams& p, const OpArgs&
                             const float4 x = here ? reinterpret_cast<const float4*>(chunk + (b + k) * kPackBytes)[lane]
                                                   : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
                             w[k * kPack] = x.x, w[k * kPack + 1] = x.y, w[k * kPack + 2] = x.z, w[k * kPack + 3] = x.w;
+                        } else if constexpr (kBase == kField24) {
+                            const unsigned char* q = chunk + (b + k) * kPackBytes;
+                            decode24(here ? reinterpret_cast<const uint2*>(q)[lane] : make_uint2(0u, 0u),
+                                     here ? reinterpret_cast<const unsigned*>(q + 256)[lane] : 0u, w + k * kPack);
                         } else {
                             const uint2 x = here ? reinterpret_cast<const uint2*>(chunk + (b + k) * kPackBytes)[lane]
                                                  : make_uint2(0u, 0u);
@@ -644,6 +699,8 @@ __global__ void __launch_bounds__(kMaxBlock) project_batch_kernel(const BatchIte
         case kBatchFieldBF16: project_group<OP, false, kTraceNear, kFieldBF16>(p, a, group, warp, dyn_smem, bars); break;
         case kBatchFieldF32T: project_group<OP, false, kTraceNear, kFieldF32T>(p, a, group, warp, dyn_smem, bars); break;
         case kBatchFieldBF16T: project_group<OP, false, kTraceNear, kFieldBF16T>(p, a, group, warp, dyn_smem, bars); break;
+        case kBatchField24: project_group<OP, false, kTraceNear, kField24>(p, a, group, warp, dyn_smem, bars); break;
+        case kBatchField24T: project_group<OP, false, kTraceNear, kField24T>(p, a, group, warp, dyn_smem, bars); break;
         default: break;
     }
 }
@@ -698,7 +755,11 @@ __global__ void __launch_bounds__(kBlock) transpose_kernel(const ProjParams p, c
         for (int m = 0; m < L; ++m) {
             const long long e = pack_slot(row_base, m, lane);
             float w = 0.0f;
-            if (valid) w = FAR_MODE == kFieldF32 ? far.f32[e] : __bfloat162float(far.b16[e]);
+            if (valid) {
+                if constexpr (FAR_MODE == kFieldF32) w = far.f32[e];
+                else if constexpr (FAR_MODE == kField24) w = load24(far.b24, e);
+                else w = __bfloat162float(far.b16[e]);
+            }
             const bool dep = valid && w > 0.0f;
             int tsrc = -1;
             if (dep) tsrc = p.vox2src[s + p.tmpl[(size_t)k * p.tmpl_len + m]];
@@ -711,6 +772,7 @@ __global__ void __launch_bounds__(kBlock) transpose_kernel(const ProjParams p, c
                     const int tg = tsrc >> 5, tl = tsrc & 31;
                     const long long et = pack_slot(p.tgt.group_base[tg] + row_base_t[(size_t)tg * p.n_rows + k], m, tl);
                     if constexpr (FAR_MODE == kFieldF32) farT.f32[et] = far.f32[e];
+                    else if constexpr (FAR_MODE == kField24) store24(farT.b24, et, bits24(w));  // w is exact in 24 bits
                     else farT.b16[et] = far.b16[e];
                 }
             }
@@ -1041,8 +1103,10 @@ cudaError_t launch_modes(const ProjParams& p, const OpArgs& a, bool trace_near, 
             }
         }
         if (OP == Op::Forward && a.farT.f32) return launch<OP, EXACT, kTraceNear, kFieldF32T>(p, a, s);
+        if (OP == Op::Forward && a.farT.b24) return launch<OP, EXACT, kTraceNear, kField24T>(p, a, s);
         if (OP == Op::Forward && a.farT.b16) return launch<OP, EXACT, kTraceNear, kFieldBF16T>(p, a, s);
         if (a.far.f32) return launch<OP, EXACT, kTraceNear, kFieldF32>(p, a, s);
+        if (a.far.b24) return launch<OP, EXACT, kTraceNear, kField24>(p, a, s);
         if (a.far.b16) return launch<OP, EXACT, kTraceNear, kFieldBF16>(p, a, s);
         if (trace_near || !a.near.on()) return launch<OP, EXACT, kTraceNear, kMarch>(p, a, s);
         if (a.near.b16) return launch<OP, EXACT, kCacheBF16, kMarch>(p, a, s);
@@ -1090,6 +1154,7 @@ cudaError_t transpose_lengths(const ProjParams& p, const FarField& far, int* len
     const int groups = (p.n_active + kLanes - 1) / kLanes;
     if (groups == 0) return cudaSuccess;
     if (far.f32) transpose_kernel<false, kFieldF32><<<(groups + kWarps - 1) / kWarps, kBlock, 0, s>>>(p, far, FarField{}, len_t32, nullptr);
+    else if (far.b24) transpose_kernel<false, kField24><<<(groups + kWarps - 1) / kWarps, kBlock, 0, s>>>(p, far, FarField{}, len_t32, nullptr);
     else transpose_kernel<false, kFieldBF16><<<(groups + kWarps - 1) / kWarps, kBlock, 0, s>>>(p, far, FarField{}, len_t32, nullptr);
     return cudaGetLastError();
 }
@@ -1099,6 +1164,7 @@ cudaError_t transpose_fill(const ProjParams& p, const FarField& far, const FarFi
     const int groups = (p.n_active + kLanes - 1) / kLanes;
     if (groups == 0) return cudaSuccess;
     if (far.f32) transpose_kernel<true, kFieldF32><<<(groups + kWarps - 1) / kWarps, kBlock, 0, s>>>(p, far, farT, nullptr, row_base_t);
+    else if (far.b24) transpose_kernel<true, kField24><<<(groups + kWarps - 1) / kWarps, kBlock, 0, s>>>(p, far, farT, nullptr, row_base_t);
     else transpose_kernel<true, kFieldBF16><<<(groups + kWarps - 1) / kWarps, kBlock, 0, s>>>(p, far, farT, nullptr, row_base_t);
     return cudaGetLastError();
 }
@@ -1190,6 +1256,7 @@ cudaError_t radial_kernels(const ProjParams& p, const RadialTables& t, const int
 cudaError_t surrogate_fill(const ProjParams& p, const OpArgs& a, const RadialTables& t, const __nv_bfloat16* coef,
                            const unsigned char* support, const unsigned char* fallback_rays, int water_bins,
                            cudaStream_t s) {
+    if (a.far.b24) return cudaErrorInvalidValue;  // surrogate fields hold fp32 or bf16 weights
     const int groups = (p.n_active + kLanes - 1) / kLanes;
     if (groups == 0) return cudaSuccess;
     const int blocks = (groups + kWarps - 1) / kWarps;

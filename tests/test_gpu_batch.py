@@ -21,14 +21,15 @@ def frame_set():
     return out
 
 
-@pytest.mark.parametrize("cache", [pm.PRC_CACHE_FULL, pm.PRC_CACHE_NEAR], ids=["field", "traced"])
-def test_batched_correction_matches_each_frame_alone(cache):
+@pytest.mark.parametrize("cache,prec", [(pm.PRC_CACHE_FULL, pm.PRC_PRECISION_FP32), (pm.PRC_CACHE_NEAR, pm.PRC_PRECISION_FP32),
+                                        (pm.PRC_CACHE_FULL, pm.PRC_PRECISION_FP24)], ids=["field", "traced", "field-fp24"])
+def test_batched_correction_matches_each_frame_alone(cache, prec):
     frames = frame_set()
-    batch = pm.Batch([(iso, rho, sp) for iso, rho, sp, _ in frames], rays=32, cache=cache)
+    batch = pm.Batch([(iso, rho, sp) for iso, rho, sp, _ in frames], rays=32, cache=cache, precision=prec)
     assert batch.warps in (2, 4, 8)
     gs, outs, refs = [], [], []
     for iso, rho, sp, truth in frames:
-        with pm.Projector(iso, rho, sp, rays=32, cache=cache) as P:
+        with pm.Projector(iso, rho, sp, rays=32, cache=cache, precision=prec) as P:
             g = phantoms.poisson_counts(P.forward_host(truth), 1e5, seed=3)
             refs.append(P.correct_host(g, 5, 0.03, 20.0, True))
         gs.append(torch.from_numpy(g).cuda())
@@ -42,7 +43,7 @@ def test_batched_correction_matches_each_frame_alone(cache):
     batch.correct(gs, outs, 3, 0.0, 20.0, False)
     batch.synchronize()
     for (iso, rho, sp, truth), g, out in zip(frames, gs, outs):
-        with pm.Projector(iso, rho, sp, rays=32, cache=cache) as P:
+        with pm.Projector(iso, rho, sp, rays=32, cache=cache, precision=prec) as P:
             ref = P.correct_host(g.cpu().numpy(), 3, 0.0, 20.0, False)
         assert rel_l2(out.cpu().numpy(), ref) < 1e-5
     batch.close()

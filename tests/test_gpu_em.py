@@ -1,6 +1,7 @@
 """MAP-EM parity and behaviour on a B200 (prc.cu:659-711; tests/test_solver.py:245-348): the
-corrected images match the reference executable within 1e-5 relative L2 in every fp32 form, the
-bf16-weight form stays within 1 % NRMSE of the FP64 oracle, and the solver's invariants hold."""
+corrected images match the reference executable within 1e-5 relative L2 in every fp32 form and
+in the 24-bit-weight form, the bf16-weight form stays within 1 % NRMSE of the FP64 oracle, and
+the solver's invariants hold."""
 import numpy as np
 import pytest
 import torch
@@ -29,6 +30,18 @@ def test_correction_matches_reference_binary(fixture72, ref_golden, oracle_mod, 
     rho, x, y, shape, sp = fixture72
     it, beta, gamma, accel = EM_CASES[case]
     out = projector(fixture72, cache).correct_host(x, it, beta, gamma, accel)
+    assert rel_l2(out, ref_golden[f"fixture_{case}"]) < 1e-5
+
+
+@pytest.mark.parametrize("cache", [pm.PRC_CACHE_FULL, pm.PRC_CACHE_SOURCE_MAJOR], ids=["full", "source"])
+@pytest.mark.parametrize("case", sorted(EM_CASES))
+def test_fp24_correction_matches_reference_binary(fixture72, ref_golden, case, cache):
+    """The 24-bit stored field (weights rounded to 16 mantissa bits) keeps the reference's 1e-5."""
+    rho, x, y, shape, sp = fixture72
+    it, beta, gamma, accel = EM_CASES[case]
+    P = projector(fixture72, cache, pm.PRC_PRECISION_FP24)
+    assert P.cache_mode[0] == cache
+    out = P.correct_host(x, it, beta, gamma, accel)
     assert rel_l2(out, ref_golden[f"fixture_{case}"]) < 1e-5
 
 

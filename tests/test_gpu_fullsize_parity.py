@@ -7,8 +7,9 @@ the measured data itself -- its forward blur of the truth with 128 rays, Poisson
 counts -- and then projects and corrects that data (--mode forward / adjoint / correct with 6
 MAP-EM iterations, beta 0.03, gamma 20, acceleration on, support density 0.05).  The engine runs
 the same inputs through the C ABI.  Tolerances: every fp32 form within 1e-5 relative L2 of the
-reference (its forward scatters with atomics, so the summation order differs); the bf16 stored
-field within 2e-3 relative L2 per projection and 1 % NRMSE for the corrected image.
+reference (its forward scatters with atomics, so the summation order differs), the 24-bit stored
+field (fp32 weights rounded to 16 mantissa bits) too; the bf16 stored field within 2e-3 relative
+L2 per projection and 1 % NRMSE for the corrected image.
 """
 import numpy as np
 import pytest
@@ -26,7 +27,8 @@ EM_OPTS = ("--rays", str(RAYS), "--iterations", str(ITERS), "--beta", str(BETA),
            "--support-rho", "0.05")
 FORMS = {"fp32_field": dict(cache=pm.PRC_CACHE_FULL),
          "traced": dict(cache=pm.PRC_CACHE_NEAR),
-         "bf16_field": dict(cache=pm.PRC_CACHE_FULL, precision=pm.PRC_PRECISION_BF16)}
+         "bf16_field": dict(cache=pm.PRC_CACHE_FULL, precision=pm.PRC_PRECISION_BF16),
+         "fp24_field": dict(cache=pm.PRC_CACHE_FULL, precision=pm.PRC_PRECISION_FP24)}
 _cases = {}
 
 

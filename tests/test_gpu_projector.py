@@ -1,7 +1,7 @@
 """Projector parity on a B200: the CUDA engine against the reference executable's own outputs
 (tests/golden/ref_outputs.npz, prc.cu built for sm_100a) and the FP64 CPU oracle, in every
-cache mode and weight precision.  fp32 forms must match the reference within 1e-5 relative L2;
-bf16-stored weights within 2e-3.  The adjoint identity and count conservation hold to 3e-6
+cache mode and weight precision.  fp32 and 24-bit-weight forms must match the reference within
+1e-5 relative L2; bf16-stored weights within 2e-3.  The adjoint identity and count conservation hold to 3e-6
 (tests/test_solver.py:180-214)."""
 import numpy as np
 import pytest
@@ -15,12 +15,15 @@ ISOTOPES = ("11C", "13N", "15O", "18F", "64Cu", "68Ga", "82Rb", "124I")
 MODES = [(pm.PRC_CACHE_FULL, pm.PRC_PRECISION_FP32), (pm.PRC_CACHE_SOURCE_MAJOR, pm.PRC_PRECISION_FP32),
          (pm.PRC_CACHE_NEAR, pm.PRC_PRECISION_FP32), (pm.PRC_CACHE_NONE, pm.PRC_PRECISION_FP32),
          (pm.PRC_CACHE_FULL, pm.PRC_PRECISION_BF16), (pm.PRC_CACHE_SOURCE_MAJOR, pm.PRC_PRECISION_BF16),
-         (pm.PRC_CACHE_NEAR, pm.PRC_PRECISION_BF16)]
-MODE_IDS = ["full-fp32", "source-fp32", "near-fp32", "none-fp32", "full-bf16", "source-bf16", "near-bf16"]
+         (pm.PRC_CACHE_NEAR, pm.PRC_PRECISION_BF16), (pm.PRC_CACHE_FULL, pm.PRC_PRECISION_FP24),
+         (pm.PRC_CACHE_SOURCE_MAJOR, pm.PRC_PRECISION_FP24)]
+MODE_IDS = ["full-fp32", "source-fp32", "near-fp32", "none-fp32", "full-bf16", "source-bf16", "near-bf16",
+            "full-fp24", "source-fp24"]
 
 
 def tol(prec):
-    return 1e-5 if prec == pm.PRC_PRECISION_FP32 else 2e-3
+    """fp32 and the 24-bit field (weights within 2^-17 relative) at the reference's 1e-5."""
+    return 1e-5 if prec in (pm.PRC_PRECISION_FP32, pm.PRC_PRECISION_FP24) else 2e-3
 
 
 _cache = {}
