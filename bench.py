@@ -63,7 +63,7 @@ def parse():
                     help="skip the FP64-oracle NRMSE of every form on a crop of the workload")
     ap.add_argument("--ops", type=int, default=0,
                     help="only run this many forward+adjoint pairs of the headline form (profiling)")
-    ap.add_argument("--form", choices=("fp32", "bf16", "traced"), default="fp32",
+    ap.add_argument("--form", choices=("fp32", "fp24", "bf16", "traced"), default="fp32",
                     help="projector form of the headline number (default: plain fp32 stored field)")
     ap.add_argument("--workload", choices=("torso", "batch", "surrogate", "tiles"), default="torso",
                     help="batch: 32 dynamic-PET frames of mixed grids and isotopes, 10 iterations each; "
@@ -196,7 +196,8 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-FORMS = {"fp32": (2, 0), "bf16": (2, 1), "traced": (1, 0)}  # (PRC_CACHE_*, PRC_PRECISION_*)
+FORMS = {"fp32": (2, 0), "fp24": (2, 3), "bf16": (2, 1), "traced": (1, 0)}  # (PRC_CACHE_*, PRC_PRECISION_*)
+WEIGHT_BYTES = {"fp32": 4, "fp24": 3, "bf16": 2, "traced": 4}
 
 
 def ncu_traffic(kernel_key: str, stored_bytes: float):
@@ -338,7 +339,7 @@ def run_ours(args):
     top = max(region_ms, key=region_ms.get)
     nz, ny, nx = args.grid
     n_vox = nx * ny * nz
-    acct = algorithmic_bytes(n_vox, n_active, deposits, weight_bytes=2 if args.form == "bf16" else 4)
+    acct = algorithmic_bytes(n_vox, n_active, deposits, weight_bytes=WEIGHT_BYTES[args.form])
     alg_bytes = acct["projection"]
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / (region_ms[top] / 1e3) / 1e9
@@ -350,7 +351,7 @@ def run_ours(args):
                  "compulsory_gbs": round(acct["compulsory"] / iter_s / 1e9, 1)}
     projection_share = (in_region["forward_ms"] + in_region["adjoint_ms"]) / sum(times)
     mode, far_entries, far_t_entries = P.cache_mode
-    elem = 2 if args.form == "bf16" else 4
+    elem = WEIGHT_BYTES[args.form]
     stored_bytes = (far_t_entries if top == "forward" else far_entries) * elem
     traffic = ncu_traffic(f"{top}_{args.form}", stored_bytes) if mode == 2 else None
 
@@ -395,7 +396,8 @@ def run_ours(args):
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f32" if args.form != "bf16" else "bf16 (stored weights; f32 accumulation, f64 sums)",
+        "dtype": {"bf16": "bf16 (stored weights; f32 accumulation, f64 sums)",
+                  "fp24": "f32 (24-bit stored weights; f32 accumulation, f64 sums)"}.get(args.form, "f32"),
         "data": data_how,
         "data_sha256": data_sha,
         "config": workload_config(args.grid, args.iterations, world),
