@@ -65,10 +65,11 @@ def parse():
                     help="only run this many forward+adjoint pairs of the headline form (profiling)")
     ap.add_argument("--form", choices=("fp32", "fp24", "bf16", "traced"), default="fp32",
                     help="projector form of the headline number (default: plain fp32 stored field)")
-    ap.add_argument("--workload", choices=("torso", "batch", "surrogate", "tiles"), default="torso",
+    ap.add_argument("--workload", choices=("torso", "batch", "surrogate", "tiles", "frames"), default="torso",
                     help="batch: 32 dynamic-PET frames of mixed grids and isotopes, 10 iterations each; "
                          "surrogate: the learned surrogate's evaluation on the small phantom at 128x128x159; "
-                         "tiles: projection and MAP-EM times of every source tile shape in both precisions")
+                         "tiles: projection and MAP-EM times of every source tile shape in both precisions; "
+                         "frames: projections and MAP-EM of --frames frames sharing the torso's density map")
     ap.add_argument("--no-parity", action="store_true",
                     help="skip the comparison with the reference executable and the time-to-image leg")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-frames sub-record")
@@ -371,6 +372,9 @@ def run_ours(args):
     batch = None
     if single and not args.no_batch:
         batch = batch_record(frames=8, iterations=10, steps=2, warmup=1)
+    shared = None
+    if single and not args.no_batch and args.form != "traced":
+        shared = shared_frames_record(P, truth, g_host, stream, l2_flush, args.iterations, value, corrected)
 
     if world > 1:
         torch.distributed.barrier()
@@ -451,6 +455,8 @@ def run_ours(args):
         line["fp64_oracle_check"] = check
     if batch:
         line["batch"] = batch
+    if shared:
+        line["shared_density_frames"] = shared
     print(json.dumps(line))
     if world > 1:
         torch.distributed.destroy_process_group()
@@ -947,6 +953,57 @@ def measured_data(rho, truth, spacing, P=None, use_reference=True):
     return g, how, hashlib.sha256(g.tobytes()).hexdigest()[:16]
 
 
+# ------------------------------------------------------------------ frames sharing one density map
+def shared_frames_record(P, truth, g_host, stream, l2_flush, iterations, single_value, corrected,
+                         n_frames: int = 4, steps: int = 3, warmup: int = 1) -> dict:
+    """The frames of one dynamic study share the density map (one CT), so they share the
+    projector: frame 0 is the headline data, frames 1.. further Poisson draws (seeds 101..) of
+    the same blur, all corrected by one prc_em_run_frames call per step (each projection one
+    pass over the stored field for up to four frames).  Reports frame-iterations/s, the
+    projection passes' mean device time against the single-volume launches, and frame 0's
+    difference from the single-volume correction of the same data (bit-identical by design)."""
+    import torch
+    import prc_mlem_b200 as pm
+    from prc_mlem_b200 import phantoms
+    blur = torch.empty(g_host.size, dtype=torch.float32, device="cuda")
+    d_truth = torch.from_numpy(np.ascontiguousarray(truth, np.float32)).cuda().reshape(-1)
+    P.forward(d_truth, blur)
+    P.synchronize()
+    d_gs = [torch.from_numpy(g_host).cuda().reshape(-1)]
+    d_gs += [phantoms.poisson_counts_device(blur, COUNTS, seed=100 + k).reshape(-1) for k in range(1, n_frames)]
+    d_outs = [torch.empty_like(d_gs[0]) for _ in range(n_frames)]
+    torch.cuda.synchronize()
+    for _ in range(warmup):
+        P.correct_frames(d_gs, d_outs, iterations, BETA, GAMMA, True)
+    P.synchronize()
+    times = []
+    P.timing(True)
+    for _ in range(steps):
+        l2_flush()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        P.correct_frames(d_gs, d_outs, iterations, BETA, GAMMA, True)
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    P.timing(False)
+    passes = P.timing_read()
+    total_s = sum(times) / 1e3
+    value = n_frames * iterations * steps / total_s
+    diff = float(np.max(np.abs(d_outs[0].cpu().numpy().reshape(corrected.shape) - corrected)))
+    return {"value": round(value, 3), "unit": "EM frame-iterations/s",
+            "frames_per_s": round(n_frames * steps / total_s, 3),
+            "x_single_volume": round(value / single_value, 3),
+            "steps": steps, "warmup": warmup, "ms_per_step": round(sum(times) / steps, 3),
+            "config": {"workload": f"{n_frames} frames of the 128x128x159 68Ga torso sharing its density map, "
+                                   f"{iterations} MAP-EM iterations each per step (beta {BETA}, gamma {GAMMA}, "
+                                   "accel), fp32 stored field", "l2": "flushed before every step"},
+            "pass_ms": {"forward": round(passes["forward_ms"] / max(passes["forward_launches"], 1), 4),
+                        "adjoint": round(passes["adjoint_ms"] / max(passes["adjoint_launches"], 1), 4),
+                        "frames_per_pass": min(n_frames, 4)},
+            "frame0_max_abs_diff_vs_single_volume": diff}
+
+
 # ------------------------------------------------------------------------------- batched frames
 BATCH_GRIDS = ((64, 64, 64), (80, 96, 96), (159, 128, 128), (200, 192, 192))
 BATCH_ISOTOPES = ("11C", "15O", "18F", "68Ga")
@@ -1162,6 +1219,62 @@ def run_tiles(args):
     print(json.dumps({"workload": f"torso {nx}x{ny}x{nz}, {ISOTOPE}, rays {RAYS}", "tiles": out}))
 
 
+def run_frames(args):
+    """Frames sharing one density map on the torso (--grid, --form): the mean device time of ten
+    forward and ten adjoint projections of 1, 2 and 4 frames per call (after two warm-up calls),
+    per frame and against the single-volume launch, and one MAP-EM run of --frames frames
+    (--iterations each) against as many single-volume runs."""
+    import torch
+    import prc_mlem_b200 as pm
+    torch.cuda.set_device(0)
+    rho, truth, spacing = make_workload(args.grid)
+    cache, prec = FORMS[args.form]
+    P = pm.Projector(ISOTOPE, rho, spacing, rays=RAYS, support_rho=SUPPORT_RHO, cache=cache, precision=prec)
+    s = torch.cuda.ExternalStream(P.stream)
+    d = torch.from_numpy(truth).cuda()
+    n = max(1, args.frames)
+    ins = [d * (1.0 + 0.1 * k) for k in range(max(n, 4))]
+    outs = [torch.empty_like(d) for _ in ins]
+    torch.cuda.synchronize()
+
+    def timed(fn, reps=10, warm=2):
+        for _ in range(warm):
+            fn()
+        P.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        for _ in range(reps):
+            fn()
+        e1.record(s)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    single = {"forward_ms": round(timed(lambda: P.forward(ins[0], outs[0])), 4),
+              "adjoint_ms": round(timed(lambda: P.adjoint(ins[0], outs[0])), 4)}
+    per_call = {}
+    for k in (1, 2, 4):
+        f = timed(lambda: P.forward_frames(ins[:k], outs[:k]))
+        a = timed(lambda: P.adjoint_frames(ins[:k], outs[:k]))
+        per_call[str(k)] = {"forward_ms": round(f, 4), "adjoint_ms": round(a, 4),
+                            "forward_ms_per_frame": round(f / k, 4), "adjoint_ms_per_frame": round(a / k, 4)}
+    gs = [torch.empty_like(d) for _ in range(n)]
+    for k in range(n):
+        P.forward(ins[k], gs[k])
+    em_outs = [torch.empty_like(d) for _ in range(n)]
+    shared = timed(lambda: P.correct_frames(gs, em_outs, args.iterations, BETA, GAMMA, True), reps=2, warm=1)
+
+    def one_by_one():
+        for k in range(n):
+            P.correct(gs[k], em_outs[k], args.iterations, BETA, GAMMA, True)
+    alone = timed(one_by_one, reps=2, warm=1)
+    nz, ny, nx = args.grid
+    print(json.dumps({"workload": f"torso {nx}x{ny}x{nz}, {ISOTOPE}, rays {RAYS}, {args.form} stored field",
+                      "single_volume": single, "frames_per_call": per_call,
+                      "map_em": {"frames": n, "iterations": args.iterations,
+                                 "shared_ms": round(shared, 3), "one_by_one_ms": round(alone, 3),
+                                 "speedup": round(alone / shared, 3)}}))
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -1172,6 +1285,8 @@ def main():
         run_surrogate_eval(args)
     elif args.workload == "tiles":
         run_tiles(args)
+    elif args.workload == "frames":
+        run_frames(args)
     else:
         run_ours(args)
 

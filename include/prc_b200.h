@@ -189,6 +189,21 @@ int prc_em_run(prc_handle* h, const float* d_g, float* d_out, int iterations, fl
 int prc_em_run_host(prc_handle* h, const float* g_host, float* out_host, int iterations, float beta,
                     float gamma, int accelerate);
 
+/* Frames of one dynamic study: n_frames volumes that share this handle's density map, isotope
+ * and grid, hence its operator.  Each is the reference's single-volume computation run once per
+ * frame (prc.cu:430-436 for the projections, prc.cu:659-711 for MAP-EM: main() corrects one
+ * volume per process).  With the stored field (PRC_CACHE_FULL in both majors) every projection
+ * reads the field once for up to four frames, and each frame's result is bit-identical to the
+ * single-volume entry point's on the same input; other forms (and the bf16-volume precision in
+ * MAP-EM) run the frames one after another through the single-volume entry points.  d_in / d_g and d_out are arrays of
+ * n_frames device pointers to distinct volumes; enqueued on `stream` like the single-volume
+ * forms.  The handle keeps n_frames sets of MAP-EM volumes (7 volumes each) after the first call;
+ * the single-volume MAP-EM state is separate and untouched. */
+int prc_forward_frames(prc_handle* h, int n_frames, const float* const* d_in, float* const* d_out, void* stream);
+int prc_adjoint_frames(prc_handle* h, int n_frames, const float* const* d_in, float* const* d_out, void* stream);
+int prc_em_run_frames(prc_handle* h, int n_frames, const float* const* d_g, float* const* d_out, int iterations,
+                      float beta, float gamma, int accelerate, void* stream);
+
 /* prc_em_begin from host memory, and the current estimate copied back to host memory (the
  * checkpoint path of --save-every, prc.cu:705-709).  Synchronise. */
 int prc_em_begin_host(prc_handle* h, const float* g_host);

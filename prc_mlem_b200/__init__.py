@@ -24,6 +24,7 @@ CLI_PATH = PKG_DIR / "bin" / "prc"
 HEADER_PATH = PKG_DIR.parent / "include" / "prc_b200.h"
 
 PRC_OK = 0
+PRC_ERR_ARGUMENT = 1
 PRC_PRECISION_FP32 = 0
 PRC_PRECISION_BF16 = 1
 PRC_PRECISION_BF16_VOLUMES = 2
@@ -80,6 +81,10 @@ _SIGNATURES = {
     "prc_em_estimate": (ctypes.c_int, [_P, _P, _P]),
     "prc_em_run": (ctypes.c_int, [_P, _P, _P, ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_int, _P]),
     "prc_em_run_host": (ctypes.c_int, [_P, _P, _P, ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_int]),
+    "prc_forward_frames": (ctypes.c_int, [_P, ctypes.c_int, _P, _P, _P]),
+    "prc_adjoint_frames": (ctypes.c_int, [_P, ctypes.c_int, _P, _P, _P]),
+    "prc_em_run_frames": (ctypes.c_int, [_P, ctypes.c_int, _P, _P, ctypes.c_int, ctypes.c_float, ctypes.c_float,
+                                         ctypes.c_int, _P]),
     "prc_em_begin_host": (ctypes.c_int, [_P, _P]),
     "prc_em_estimate_host": (ctypes.c_int, [_P, _P]),
     "prc_forward_host": (ctypes.c_int, [_P, _P, _P]),
@@ -330,6 +335,27 @@ class Projector:
         Enqueued on ``stream`` (default: the engine's own stream) and asynchronous to the host
         and to torch's current stream: call ``synchronize()`` before reading d_out elsewhere."""
         _check(lib().prc_em_run(self._h, _ptr(d_g), _ptr(d_out), iterations, beta, gamma, int(accelerate), stream))
+
+    # frames sharing this projector (one density map, many activity volumes) ---------------
+    @staticmethod
+    def _pointers(vols):
+        return (ctypes.c_void_p * len(vols))(*[_ptr(x) for x in vols])
+
+    def forward_frames(self, d_ins, d_outs, stream=None) -> None:
+        """d_outs[i] = A d_ins[i] for every frame; the stored field is read once per pass of up to
+        four frames.  Each result equals ``forward(d_ins[i], d_outs[i])`` bit for bit."""
+        _check(lib().prc_forward_frames(self._h, len(d_ins), self._pointers(d_ins), self._pointers(d_outs), stream))
+
+    def adjoint_frames(self, d_ins, d_outs, stream=None) -> None:
+        """d_outs[i][s] = (A^T d_ins[i])[s] on tissue voxels for every frame."""
+        _check(lib().prc_adjoint_frames(self._h, len(d_ins), self._pointers(d_ins), self._pointers(d_outs), stream))
+
+    def correct_frames(self, d_gs, d_outs, iterations: int, beta: float = 0.2, gamma: float = 20.0,
+                       accelerate: bool = True, stream=None) -> None:
+        """MAP-EM correction of every frame (one ``correct`` per frame, prc.cu:659-711) with the
+        projections of all frames done together.  Asynchronous like ``correct``."""
+        _check(lib().prc_em_run_frames(self._h, len(d_gs), self._pointers(d_gs), self._pointers(d_outs), iterations,
+                                       beta, gamma, int(accelerate), stream))
 
     def synchronize(self) -> None:
         _check(lib().prc_synchronize(self._h))

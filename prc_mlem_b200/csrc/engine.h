@@ -210,6 +210,24 @@ struct PrepItem {
 };
 cudaError_t forward_prep_batch(const PrepItem* d_items, int n_items, cudaStream_t s);
 
+// ---- frames that share one stored field (dynamic PET: one density, many activity volumes) ----
+// One pass over the stored field projects up to kMaxFrames volumes: every stored weight, its
+// template offsets and its predicate are loaded once and used for every frame's gather and
+// accumulation.  Per frame the accumulation order is the single-volume kernel's, so each
+// frame's result is bit-identical to projecting it alone.
+constexpr int kMaxFrames = 4;
+struct FrameArgs {
+    const float* in[kMaxFrames] = {};        // gathered volume of each frame (u = f / W, or the EM ratio)
+    float* out[kMaxFrames] = {};             // each frame's result
+    const float* ratio_g[kMaxFrames] = {};   // forward inside MAP-EM: write g / max(Af, *eps) (prc.cu:270-274)
+    const float* ratio_eps[kMaxFrames] = {};
+    int n = 0;                               // frames in this pass, 1..kMaxFrames
+};
+// Forward (target-major field, a gather of each frame's u) or Adjoint (source-major field) of
+// fr.n frames through the stored field of a (fp32, 24-bit or bf16 weights; not the bf16-volume
+// form).  cudaErrorInvalidValue when the handle has no such field.
+cudaError_t project_frames(Op op, const ProjParams& p, const OpArgs& a, const FrameArgs& fr, cudaStream_t s);
+
 // Self-test of the bounded mbarrier wait: a wait that nothing completes, `rounds` rounds.
 cudaError_t wait_selftest(int rounds, unsigned int* error, cudaStream_t s);
 

@@ -97,6 +97,16 @@ struct prc_handle {
     EmScalars* scalars = nullptr;
     Reduction red{};
     bool em_started = false;
+    // Frames sharing this projector (prc_*_frames): each frame's MAP-EM volumes, its u = f / W
+    // volume for the forward gather, its FP64 scalars and reduction scratch.  Grown on demand.
+    struct Frame {
+        float* g = nullptr;
+        float* vol[5] = {};  // f, prev, y, h_prev, est (rotated by pointer swaps)
+        float* u = nullptr;
+        EmScalars* scalars = nullptr;
+        Reduction red{};
+    };
+    std::vector<Frame> frames;
     int64_t bytes = 0;
     int64_t launches = 0;  // kernels this handle's entry points have enqueued (prc_launch_count)
     int tile = PRC_TILE_AUTO;  // source tile in effect (PRC_TILE_*)
@@ -1112,6 +1122,158 @@ int prc_adjoint_host(prc_handle* h, const float* in_host, float* out_host) {
     if (rc != PRC_OK) return rc;
     PRC_CUDA(cudaMemcpyAsync(out_host, out, h->n * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
     return check_device_error(h);
+}
+
+// ---- frames that share this projector --------------------------------------------------------
+// The frames of one dynamic study share the density map, isotope and grid, hence the operator:
+// with the stored field every projection pass reads the field once for up to kMaxFrames frames.
+static int ensure_frames(prc_handle* h, int n_frames) {
+    while ((int)h->frames.size() < n_frames) {
+        prc_handle::Frame fr;
+        PRC_CUDA(h->alloc(&fr.g, h->n));
+        for (float*& v : fr.vol) PRC_CUDA(h->alloc(&v, h->n));
+        PRC_CUDA(h->alloc(&fr.u, h->n));
+        PRC_CUDA(h->alloc(&fr.scalars, 1));
+        PRC_CUDA(h->alloc(&fr.red.partials, (size_t)kReduceBlocks * 4));
+        PRC_CUDA(h->alloc(&fr.red.counter, 1));
+        h->frames.push_back(fr);
+    }
+    return PRC_OK;
+}
+
+static int check_frames(int n_frames, const float* const* in, const void* out) {
+    if (n_frames < 1 || !in || !out) return fail(PRC_ERR_ARGUMENT, "Invalid argument");
+    for (int i = 0; i < n_frames; ++i)
+        if (!in[i] || !static_cast<float* const*>(out)[i]) return fail(PRC_ERR_ARGUMENT, "Invalid argument: null frame volume");
+    return PRC_OK;
+}
+
+// op over frames [0, n) in passes of kMaxFrames, then 2, then 1 frame(s).
+static int project_frame_passes(prc_handle* h, Op op, int n, const float* const* in, float* const* out,
+                                const float* const* ratio_g, const float* const* ratio_eps, cudaStream_t s) {
+    const OpArgs a = h->op_args();
+    const int kind = op == Op::Forward ? 0 : 1;
+    for (int first = 0; first < n;) {
+        const int left = n - first;
+        const int k = left >= kMaxFrames ? kMaxFrames : (left >= 2 ? 2 : 1);
+        FrameArgs fr;
+        fr.n = k;
+        for (int f = 0; f < k; ++f) {
+            fr.in[f] = in[first + f];
+            fr.out[f] = out[first + f];
+            fr.ratio_g[f] = ratio_g ? ratio_g[first + f] : nullptr;
+            fr.ratio_eps[f] = ratio_eps ? ratio_eps[first + f] : nullptr;
+        }
+        PRC_CUDA(timing_mark(h, kind, s));
+        PRC_CUDA(project_frames(op, h->params, a, fr, s));
+        PRC_CUDA(timing_mark(h, kind, s));
+        ++h->launches;
+        first += k;
+    }
+    return PRC_OK;
+}
+
+int prc_forward_frames(prc_handle* h, int n_frames, const float* const* d_in, float* const* d_out, void* stream) {
+    if (!h) return fail(PRC_ERR_ARGUMENT, "Invalid argument");
+    if (const int rc = check_frames(n_frames, d_in, d_out); rc != PRC_OK) return rc;
+    const cudaStream_t s = h->pick(stream);
+    if (!h->far_t.on()) {  // no target-major field: one projection per frame
+        for (int i = 0; i < n_frames; ++i)
+            if (const int rc = prc_forward(h, d_in[i], d_out[i], s); rc != PRC_OK) return rc;
+        return PRC_OK;
+    }
+    if (const int rc = ensure_frames(h, n_frames); rc != PRC_OK) return rc;
+    std::vector<const float*> u(n_frames);
+    for (int i = 0; i < n_frames; ++i) {  // u = f / W on the support, out = 0 off it
+        PRC_CUDA(forward_prep(h->params, h->W, d_in[i], h->frames[i].u, d_out[i], s));
+        ++h->launches;
+        u[i] = h->frames[i].u;
+    }
+    return project_frame_passes(h, Op::Forward, n_frames, u.data(), d_out, nullptr, nullptr, s);
+}
+
+int prc_adjoint_frames(prc_handle* h, int n_frames, const float* const* d_in, float* const* d_out, void* stream) {
+    if (!h) return fail(PRC_ERR_ARGUMENT, "Invalid argument");
+    if (const int rc = check_frames(n_frames, d_in, d_out); rc != PRC_OK) return rc;
+    const cudaStream_t s = h->pick(stream);
+    if (!h->far_field.on()) {
+        for (int i = 0; i < n_frames; ++i)
+            if (const int rc = prc_adjoint(h, d_in[i], d_out[i], s); rc != PRC_OK) return rc;
+        return PRC_OK;
+    }
+    return project_frame_passes(h, Op::Adjoint, n_frames, d_in, d_out, nullptr, nullptr, s);
+}
+
+int prc_em_run_frames(prc_handle* h, int n_frames, const float* const* d_g, float* const* d_out, int iterations,
+                      float beta, float gamma, int accelerate, void* stream) {
+    if (!h) return fail(PRC_ERR_ARGUMENT, "Invalid argument");
+    if (const int rc = check_frames(n_frames, d_g, d_out); rc != PRC_OK) return rc;
+    if (iterations < 0 || !(beta >= 0) || !(gamma >= 0) || !std::isfinite(beta) || !std::isfinite(gamma))
+        return fail(PRC_ERR_ARGUMENT, "Invalid geometry or solver parameters");
+    const cudaStream_t s = h->pick(stream);
+    if (!h->far_t.on() || !h->far_field.on() || half_volumes(h)) {  // one correction per frame
+        for (int i = 0; i < n_frames; ++i)
+            if (const int rc = prc_em_run(h, d_g[i], d_out[i], iterations, beta, gamma, accelerate, s); rc != PRC_OK)
+                return rc;
+        return PRC_OK;
+    }
+    if (h->n_active == 0) return fail(PRC_ERR_NO_ACTIVITY, "No tissue voxels: nothing to do");
+    if (const int rc = ensure_em(h); rc != PRC_OK) return rc;  // the RDP's distance weights
+    if (const int rc = ensure_frames(h, n_frames); rc != PRC_OK) return rc;
+    const int n = n_frames;
+    // Every frame runs prc_em_iterate's five-launch iteration (prc.cu:675-700) with its own
+    // volumes and FP64 scalars; only the two projections are shared passes over the field.
+    std::vector<float*> f(n), prev(n), y(n), hp(n), est(n);
+    std::vector<const float*> u(n), start(n), est_in(n), g(n), eps(n);
+    std::vector<EmVolumes> v(n);
+    auto scalar = [](const EmScalars* sc, size_t off) {
+        return reinterpret_cast<const float*>(reinterpret_cast<const char*>(sc) + off);
+    };
+    for (int i = 0; i < n; ++i) {
+        const prc_handle::Frame& fr = h->frames[i];
+        f[i] = fr.vol[0], prev[i] = fr.vol[1], y[i] = fr.vol[2], hp[i] = fr.vol[3], est[i] = fr.vol[4];
+        v[i] = EmVolumes{h->n, h->support, fr.scalars, fr.red};
+        g[i] = fr.g;
+        u[i] = fr.u;
+        eps[i] = scalar(fr.scalars, offsetof(EmScalars, eps));
+        for (float* p : {prev[i], y[i], hp[i]}) PRC_CUDA(cudaMemsetAsync(p, 0, h->n * sizeof(float), s));
+        PRC_CUDA(em_begin(v[i], d_g[i], fr.g, f[i], h->n_active, iterations > 0, s));
+        h->launches += iterations > 0 ? 3 : 1;
+    }
+    for (int it = 0; it < iterations; ++it) {
+        for (int i = 0; i < n; ++i) {
+            if (accelerate) {
+                PRC_CUDA(forward_prep_extrapolate(h->params, h->W, f[i], prev[i],
+                                                  scalar(h->frames[i].scalars, offsetof(EmScalars, lambda)), y[i],
+                                                  h->frames[i].u, est[i], s));
+            } else {
+                PRC_CUDA(forward_prep(h->params, h->W, f[i], h->frames[i].u, est[i], s));
+            }
+            ++h->launches;
+            start[i] = accelerate ? y[i] : f[i];
+            est_in[i] = est[i];
+        }
+        int rc = project_frame_passes(h, Op::Forward, n, u.data(), est.data(), g.data(), eps.data(), s);
+        if (rc == PRC_OK) rc = project_frame_passes(h, Op::Adjoint, n, est_in.data(), prev.data(), nullptr, nullptr, s);
+        if (rc != PRC_OK) return rc;
+        for (int i = 0; i < n; ++i) {
+            PRC_CUDA(em_update_active(v[i], h->g, h->active, h->n_active, h->geo_w, start[i], prev[i], est[i], beta,
+                                      gamma, s));
+            ++h->launches;
+            if (beta > 0.0f || accelerate) {
+                PRC_CUDA(em_finish(v[i], est[i], accelerate ? y[i] : nullptr, hp[i], beta > 0.0f, s));
+                ++h->launches;
+            }
+            if (accelerate) {
+                std::swap(y[i], hp[i]);
+                std::swap(prev[i], f[i]);
+            }
+            std::swap(f[i], est[i]);
+        }
+    }
+    for (int i = 0; i < n; ++i)
+        PRC_CUDA(cudaMemcpyAsync(d_out[i], f[i], h->n * sizeof(float), cudaMemcpyDeviceToDevice, s));
+    return PRC_OK;
 }
 
 int prc_sum(prc_handle* h, const float* d_x, double* sum, void* stream) {

@@ -705,6 +705,210 @@ __global__ void __launch_bounds__(kMaxBlock) project_batch_kernel(const BatchIte
     }
 }
 
+// NF frames through one stored field (fr.n == NF): the gather forms only -- the adjoint over the
+// source-major field and the forward over the target-major one (lanes are targets, fr.in holds
+// each frame's u = f / W).  The stream is consumed exactly as project_group consumes it (the
+// bf16 vectors loaded by the lanes, the fp32 and 24-bit packs through the per-warp TMA ring), but
+// each pack's weights, template offsets and w > 0 predicates serve NF gathers and NF
+// accumulators.  Fewer packs per batch as NF grows keep the gathers in flight per lane (and the
+// registers) where the single-volume kernel has them.  Each frame accumulates its terms in stream
+// order with fmaf, as project_group does, so every frame equals its single-volume projection bit
+// for bit.
+template <Op OP, int FAR_MODE, int NF>
+__device__ __forceinline__ void project_frames_group(const ProjParams& p, const OpArgs& a, const FrameArgs& fr,
+                                                     int group, int warp, unsigned char* dyn_smem, uint64_t* bars) {
+    static_assert(OP == Op::Adjoint ? !target_major(FAR_MODE) : (OP == Op::Forward && target_major(FAR_MODE)),
+                  "gather forms only");
+    static_assert(!half_volume(FAR_MODE) && FAR_MODE != kMarch, "fp32 volumes through a stored field");
+    const int lane = threadIdx.x & 31;
+    if (group * kLanes >= p.n_active) return;  // the whole warp leaves together
+    const int src = group * kLanes + lane;
+    const bool valid = src < p.n_active;
+    const int s = valid ? __ldg(p.active + src) : 0;
+    bool live = valid;
+    if constexpr (OP == Op::Adjoint) {  // prc.cu:260-264
+        const float ws = valid ? __ldg(a.W + src) : 0.0f;
+        live = valid && ws > 0.0f;
+        if (valid && !live)
+#pragma unroll
+            for (int f = 0; f < NF; ++f) fr.out[f][s] = 0.0f;
+    }
+    if (!__any_sync(kFull, live)) return;
+
+    constexpr bool kT = target_major(FAR_MODE);
+    constexpr int kBase = field_base(FAR_MODE);
+    constexpr int kElem = kBase == kFieldF32 ? 4 : (kBase == kField24 ? 3 : 2);
+    constexpr int kPackBytes = kPack * kLanes * kElem;
+    constexpr int kB = NF == 1 ? 4 : (NF == 2 ? 2 : 1);  // packs per batch: kB * 4 * NF gathers in flight
+    constexpr int kPacksPerChunk = kChunk / kPackBytes / kB * kB;
+    constexpr int kChunkBytes = kPacksPerChunk * kPackBytes;
+    static_assert(kPacksPerChunk > 0 && kChunkBytes % 16 == 0, "bulk copies of whole 16-byte units");
+    const StreamLayout& lay = kT ? p.tgt : p.src;
+    const FarField& fld = kT ? a.farT : a.far;
+    const int* tmpl = kT ? p.tmpl_neg : p.tmpl;
+    const long long e0 = lay.group_base[group], e1 = lay.group_base[group + 1];
+    const int* desc = lay.desc + e0 / (kPack * kLanes);
+    const int n_packs = (int)((e1 - e0) / (kPack * kLanes));
+    auto desc_at = [&](int P) { return P < n_packs ? __ldg(desc + P) : 0; };
+    float acc[NF];
+#pragma unroll
+    for (int f = 0; f < NF; ++f) acc[f] = 0.0f;
+    // One batch: kB packs of template offsets tc and weights w (a zero weight is padding: no load).
+    auto consume = [&](const int4* tc, const float* w) {
+        int idx[kB * kPack];
+#pragma unroll
+        for (int k = 0; k < kB; ++k) {
+            idx[k * kPack] = (int)((unsigned)s + (unsigned)tc[k].x), idx[k * kPack + 1] = (int)((unsigned)s + (unsigned)tc[k].y);
+            idx[k * kPack + 2] = (int)((unsigned)s + (unsigned)tc[k].z), idx[k * kPack + 3] = (int)((unsigned)s + (unsigned)tc[k].w);
+        }
+        float v[NF][kB * kPack];
+#pragma unroll
+        for (int u = 0; u < kB * kPack; ++u)
+#pragma unroll
+            for (int f = 0; f < NF; ++f) v[f][u] = w[u] > 0.0f ? __ldg(fr.in[f] + idx[u]) : 0.0f;
+#pragma unroll
+        for (int u = 0; u < kB * kPack; ++u)
+#pragma unroll
+            for (int f = 0; f < NF; ++f) acc[f] = fmaf(w[u], v[f][u], acc[f]);
+    };
+
+    if constexpr (kBase == kFieldBF16) {
+        const uint2* vec = reinterpret_cast<const uint2*>(fld.b16) + e0 / kPack + lane;
+        auto load_vec = [&](int P) {
+            uint2 x = make_uint2(0u, 0u);
+            if (P < n_packs) x = ld_stream(vec + (size_t)P * kLanes);
+            return x;
+        };
+        int4 tn[kB];
+        uint2 wn[kB];
+        int dq[kB];
+#pragma unroll
+        for (int k = 0; k < kB; ++k) wn[k] = load_vec(k);
+#pragma unroll
+        for (int k = 0; k < kB; ++k) tn[k] = __ldg(reinterpret_cast<const int4*>(tmpl + desc_at(k)));
+#pragma unroll
+        for (int k = 0; k < kB; ++k) dq[k] = desc_at(kB + k);
+        for (int P0 = 0; P0 < n_packs; P0 += kB) {
+            float w[kB * kPack];
+            int4 tc[kB];
+#pragma unroll
+            for (int k = 0; k < kB; ++k) {
+                tc[k] = tn[k];
+                w[k * kPack] = __uint_as_float(wn[k].x << 16), w[k * kPack + 1] = __uint_as_float(wn[k].x & 0xffff0000u);
+                w[k * kPack + 2] = __uint_as_float(wn[k].y << 16), w[k * kPack + 3] = __uint_as_float(wn[k].y & 0xffff0000u);
+            }
+#pragma unroll
+            for (int k = 0; k < kB; ++k) tn[k] = __ldg(reinterpret_cast<const int4*>(tmpl + dq[k]));
+#pragma unroll
+            for (int k = 0; k < kB; ++k) wn[k] = load_vec(P0 + kB + k);
+#pragma unroll
+            for (int k = 0; k < kB; ++k) dq[k] = desc_at(P0 + 2 * kB + k);
+            consume(tc, w);
+        }
+    } else {
+        unsigned char* ring = dyn_smem + (size_t)warp * kStages * kChunk;
+        // a group's stream starts at a multiple of 128 entries: 16-byte aligned in every format
+        const char* src_bytes = (kBase == kFieldF32 ? reinterpret_cast<const char*>(fld.f32)
+                                                    : reinterpret_cast<const char*>(fld.b24)) + e0 * kElem;
+        const long long total = (e1 - e0) * kElem;
+        const int n_chunks = (n_packs + kPacksPerChunk - 1) / kPacksPerChunk;
+        auto issue = [&](int c) {  // lane 0 only
+            const int stage = c % kStages;
+            const unsigned bytes = (unsigned)min((long long)kChunkBytes, total - (long long)c * kChunkBytes);
+            mbar_expect_tx(&bars[stage], bytes);
+            bulk_copy_g2s(ring + stage * kChunk, src_bytes + (long long)c * kChunkBytes, bytes, &bars[stage]);
+        };
+        if (lane == 0) {
+            for (int k = 0; k < kStages; ++k) mbar_init(&bars[k], 1);
+            fence_mbarrier_init();
+            for (int c = 0; c < n_chunks && c < kStages; ++c) issue(c);
+        }
+        __syncwarp();
+        int4 tn[kB];
+        int dq[kB];
+#pragma unroll
+        for (int k = 0; k < kB; ++k) tn[k] = __ldg(reinterpret_cast<const int4*>(tmpl + desc_at(k)));
+#pragma unroll
+        for (int k = 0; k < kB; ++k) dq[k] = desc_at(kB + k);
+        bool ok = true;
+        for (int c = 0; c < n_chunks; ++c) {
+            const int packs = min(kPacksPerChunk, n_packs - c * kPacksPerChunk);
+            const int stage = c % kStages;
+            if (!mbar_wait_bounded(&bars[stage], (c / kStages) & 1)) {
+                ok = false;
+                break;
+            }
+            const unsigned char* chunk = ring + stage * kChunk;
+            for (int b = 0; b < packs; b += kB) {
+                const int P0 = c * kPacksPerChunk + b;
+                float w[kB * kPack];
+                int4 tc[kB];
+#pragma unroll
+                for (int k = 0; k < kB; ++k) tc[k] = tn[k];
+#pragma unroll
+                for (int k = 0; k < kB; ++k) tn[k] = __ldg(reinterpret_cast<const int4*>(tmpl + dq[k]));
+#pragma unroll
+                for (int k = 0; k < kB; ++k) dq[k] = desc_at(P0 + 2 * kB + k);
+#pragma unroll
+                for (int k = 0; k < kB; ++k) {
+                    const bool here = b + k < packs;
+                    if constexpr (kBase == kFieldF32) {
+                        const float4 x = here ? reinterpret_cast<const float4*>(chunk + (b + k) * kPackBytes)[lane]
+                                              : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                        w[k * kPack] = x.x, w[k * kPack + 1] = x.y, w[k * kPack + 2] = x.z, w[k * kPack + 3] = x.w;
+                    } else {
+                        const unsigned char* q = chunk + (b + k) * kPackBytes;
+                        decode24(here ? reinterpret_cast<const uint2*>(q)[lane] : make_uint2(0u, 0u),
+                                 here ? reinterpret_cast<const unsigned*>(q + 256)[lane] : 0u, w + k * kPack);
+                    }
+                }
+                consume(tc, w);
+            }
+            __syncwarp();
+            if (lane == 0 && c + kStages < n_chunks) {
+                fence_proxy_async();  // this stage's reads precede the copy that overwrites it
+                issue(c + kStages);
+            }
+        }
+        if (!ok) {
+            // A copy did not complete in time: report it, and give the copies still in flight
+            // a bounded chance to land before this warp's shared memory is released.
+            if (lane == 0) {
+                atomicOr(a.error, 1u);
+                for (int k = 0; k < kStages; ++k) {
+                    mbar_wait_bounded(&bars[k], 0);
+                    mbar_wait_bounded(&bars[k], 1);
+                }
+            }
+            __syncwarp();
+        }
+    }
+
+    if constexpr (OP == Op::Adjoint) {
+        if (live) {
+            const float ws = __ldg(a.W + src);
+#pragma unroll
+            for (int f = 0; f < NF; ++f) fr.out[f][s] = acc[f] / ws;  // prc.cu:266
+        }
+    } else {
+        if (valid)
+#pragma unroll
+            for (int f = 0; f < NF; ++f)
+                fr.out[f][s] = fr.ratio_g[f] ? __ldg(fr.ratio_g[f] + s) / fmaxf(acc[f], __ldg(fr.ratio_eps[f])) : acc[f];
+    }
+}
+
+// 64 registers at most (four 256-thread blocks per SM), as the single-volume stream kernel.
+template <Op OP, int FAR_MODE, int NF>
+__global__ void __launch_bounds__(kMaxBlock, 4) project_frames_kernel(const ProjParams p, const OpArgs a,
+                                                                      const FrameArgs fr) {
+    extern __shared__ __align__(128) unsigned char dyn_smem[];
+    __shared__ uint64_t field_bars[kMaxWarps][kStages];
+    const int warp = threadIdx.x >> 5;
+    project_frames_group<OP, FAR_MODE, NF>(p, a, fr, blockIdx.x * (blockDim.x >> 5) + warp, warp, dyn_smem,
+                                           field_bars[warp]);
+}
+
 // Template rows: row 0 the near block's 125 offsets (then zeros), rows 1..n_rays the offsets of
 // the post-block steps of each far ray, from the same uniform DDA the march performs.
 __global__ void template_kernel(const ProjParams p, int* tmpl) {
@@ -1229,6 +1433,55 @@ cudaError_t project_batch(Op op, const BatchItem* d_items, int n_items, int tota
     };
     if (op == Op::Forward) return go(project_batch_kernel<Op::Forward>);
     if (op == Op::Adjoint) return go(project_batch_kernel<Op::Adjoint>);
+    return cudaErrorInvalidValue;
+}
+
+namespace {
+template <Op OP, int FAR_MODE>
+cudaError_t launch_frames(const ProjParams& p, const OpArgs& a, const FrameArgs& fr, cudaStream_t s) {
+    const int groups = (p.n_active + kLanes - 1) / kLanes;
+    const int blocks = (groups + kWarps - 1) / kWarps;
+    if (blocks == 0) return cudaSuccess;
+    auto go = [&](auto kernel) {
+        if (kFieldSmemBytes > 48 * 1024) {
+            const cudaError_t e =
+                cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFieldSmemBytes);
+            if (e != cudaSuccess) return e;
+        }
+        kernel<<<blocks, kBlock, kFieldSmemBytes, s>>>(p, a, fr);
+        return cudaGetLastError();
+    };
+    switch (fr.n) {
+        case 2: return go(project_frames_kernel<OP, FAR_MODE, 2>);
+        case 4: return go(project_frames_kernel<OP, FAR_MODE, 4>);
+        default: return cudaErrorInvalidValue;
+    }
+}
+}  // namespace
+
+cudaError_t project_frames(Op op, const ProjParams& p, const OpArgs& a, const FrameArgs& fr, cudaStream_t s) {
+    for (int f = 0; f < fr.n && f < kMaxFrames; ++f)
+        if (!fr.in[f] || !fr.out[f] || (fr.ratio_g[f] && !fr.ratio_eps[f])) return cudaErrorInvalidValue;
+    if (fr.n == 1) {  // one frame: the single-volume kernel (same stream, same accumulation order)
+        if (op == Op::Forward ? !a.farT.on() : !a.far.on()) return cudaErrorInvalidValue;
+        OpArgs b = a;
+        b.in = fr.in[0];
+        b.out = fr.out[0];
+        b.ratio_g = fr.ratio_g[0];
+        b.ratio_eps = fr.ratio_eps[0];
+        b.in16 = nullptr;
+        b.out16 = nullptr;
+        return project(op, p, b, false, s);
+    }
+    if (op == Op::Forward) {
+        if (a.farT.f32) return launch_frames<Op::Forward, kFieldF32T>(p, a, fr, s);
+        if (a.farT.b24) return launch_frames<Op::Forward, kField24T>(p, a, fr, s);
+        if (a.farT.b16) return launch_frames<Op::Forward, kFieldBF16T>(p, a, fr, s);
+    } else if (op == Op::Adjoint) {
+        if (a.far.f32) return launch_frames<Op::Adjoint, kFieldF32>(p, a, fr, s);
+        if (a.far.b24) return launch_frames<Op::Adjoint, kField24>(p, a, fr, s);
+        if (a.far.b16) return launch_frames<Op::Adjoint, kFieldBF16>(p, a, fr, s);
+    }
     return cudaErrorInvalidValue;
 }
 
