@@ -212,13 +212,17 @@ cudaError_t forward_prep_batch(const PrepItem* d_items, int n_items, cudaStream_
 
 // ---- frames that share one stored field (dynamic PET: one density, many activity volumes) ----
 // One pass over the stored field projects up to kMaxFrames volumes: every stored weight, its
-// template offsets and its predicate are loaded once and used for every frame's gather and
-// accumulation.  Per frame the accumulation order is the single-volume kernel's, so each
-// frame's result is bit-identical to projecting it alone.
+// template offsets and its predicate are loaded once, and one 16-byte gather of the interleaved
+// volume (four frames per voxel) feeds every frame's accumulation.  Per frame the accumulation
+// order is the single-volume kernel's, so each frame's result is bit-identical to projecting it
+// alone.
 constexpr int kMaxFrames = 4;
 struct FrameArgs {
-    const float* in[kMaxFrames] = {};        // gathered volume of each frame (u = f / W, or the EM ratio)
+    const float* in[kMaxFrames] = {};        // n == 1: the gathered volume (single-volume kernel)
+    const float4* in4 = nullptr;             // n >= 2: in4[t] = the frames' gathered values of voxel t
+                                             // (u = f / W, or the EM ratio); slots n..3 zero
     float* out[kMaxFrames] = {};             // each frame's result
+    float4* out4 = nullptr;                  // forward, n >= 2: results interleaved here instead of out
     const float* ratio_g[kMaxFrames] = {};   // forward inside MAP-EM: write g / max(Af, *eps) (prc.cu:270-274)
     const float* ratio_eps[kMaxFrames] = {};
     int n = 0;                               // frames in this pass, 1..kMaxFrames
@@ -227,6 +231,22 @@ struct FrameArgs {
 // fr.n frames through the stored field of a (fp32, 24-bit or bf16 weights; not the bf16-volume
 // form).  cudaErrorInvalidValue when the handle has no such field.
 cudaError_t project_frames(Op op, const ProjParams& p, const OpArgs& a, const FrameArgs& fr, cudaStream_t s);
+// Interleaving for the frame passes (n frames, 2..4; slots n..3 of every voxel are zero):
+// frame_prep: u4 = each frame's y / W (PREDICT: y = the Biggs-Andrews prediction
+// max(f + lambda (f - prev), f / 2), written to y[k]; else y = f) on the support, and out[k] = 0
+// off it -- per voxel and frame the expressions of forward_prep / forward_prep_extrapolate.
+// frame_pack: v4 = the frames' volumes in[k] side by side.
+struct FramePrep {
+    const float* f[kMaxFrames] = {};
+    const float* prev[kMaxFrames] = {};
+    const float* lambda[kMaxFrames] = {};
+    float* y[kMaxFrames] = {};
+    float* out[kMaxFrames] = {};
+    int n = 0;
+};
+cudaError_t frame_prep(const ProjParams& p, const float* W, const FramePrep& fp, bool predict, float4* u4,
+                       cudaStream_t s);
+cudaError_t frame_pack(const float* const* in, int n, size_t voxels, float4* v4, cudaStream_t s);
 
 // Self-test of the bounded mbarrier wait: a wait that nothing completes, `rounds` rounds.
 cudaError_t wait_selftest(int rounds, unsigned int* error, cudaStream_t s);

@@ -107,6 +107,7 @@ struct prc_handle {
         Reduction red{};
     };
     std::vector<Frame> frames;
+    std::vector<float4*> frame_u4, frame_r4;  // per group of four frames: interleaved u and EM ratio
     int64_t bytes = 0;
     int64_t launches = 0;  // kernels this handle's entry points have enqueued (prc_launch_count)
     int tile = PRC_TILE_AUTO;  // source tile in effect (PRC_TILE_*)
@@ -1126,7 +1127,9 @@ int prc_adjoint_host(prc_handle* h, const float* in_host, float* out_host) {
 
 // ---- frames that share this projector --------------------------------------------------------
 // The frames of one dynamic study share the density map, isotope and grid, hence the operator:
-// with the stored field every projection pass reads the field once for up to kMaxFrames frames.
+// with the stored field the frames go through the projections in groups of up to kMaxFrames,
+// each group one pass over the field gathering an interleaved volume (four frames per voxel).
+// A group of one frame takes the single-volume kernels.
 static int ensure_frames(prc_handle* h, int n_frames) {
     while ((int)h->frames.size() < n_frames) {
         prc_handle::Frame fr;
@@ -1138,6 +1141,13 @@ static int ensure_frames(prc_handle* h, int n_frames) {
         PRC_CUDA(h->alloc(&fr.red.counter, 1));
         h->frames.push_back(fr);
     }
+    while ((int)h->frame_u4.size() < (n_frames + kMaxFrames - 1) / kMaxFrames) {
+        float4 *u4 = nullptr, *r4 = nullptr;
+        PRC_CUDA(h->alloc(&u4, h->n));
+        PRC_CUDA(h->alloc(&r4, h->n));
+        h->frame_u4.push_back(u4);
+        h->frame_r4.push_back(r4);
+    }
     return PRC_OK;
 }
 
@@ -1148,28 +1158,13 @@ static int check_frames(int n_frames, const float* const* in, const void* out) {
     return PRC_OK;
 }
 
-// op over frames [0, n) in passes of kMaxFrames, then 2, then 1 frame(s).
-static int project_frame_passes(prc_handle* h, Op op, int n, const float* const* in, float* const* out,
-                                const float* const* ratio_g, const float* const* ratio_eps, cudaStream_t s) {
-    const OpArgs a = h->op_args();
+// One projection pass of frames [first, first + k).
+static int frame_pass(prc_handle* h, Op op, const FrameArgs& fr, cudaStream_t s) {
     const int kind = op == Op::Forward ? 0 : 1;
-    for (int first = 0; first < n;) {
-        const int left = n - first;
-        const int k = left >= kMaxFrames ? kMaxFrames : (left >= 2 ? 2 : 1);
-        FrameArgs fr;
-        fr.n = k;
-        for (int f = 0; f < k; ++f) {
-            fr.in[f] = in[first + f];
-            fr.out[f] = out[first + f];
-            fr.ratio_g[f] = ratio_g ? ratio_g[first + f] : nullptr;
-            fr.ratio_eps[f] = ratio_eps ? ratio_eps[first + f] : nullptr;
-        }
-        PRC_CUDA(timing_mark(h, kind, s));
-        PRC_CUDA(project_frames(op, h->params, a, fr, s));
-        PRC_CUDA(timing_mark(h, kind, s));
-        ++h->launches;
-        first += k;
-    }
+    PRC_CUDA(timing_mark(h, kind, s));
+    PRC_CUDA(project_frames(op, h->params, h->op_args(), fr, s));
+    PRC_CUDA(timing_mark(h, kind, s));
+    ++h->launches;
     return PRC_OK;
 }
 
@@ -1183,13 +1178,23 @@ int prc_forward_frames(prc_handle* h, int n_frames, const float* const* d_in, fl
         return PRC_OK;
     }
     if (const int rc = ensure_frames(h, n_frames); rc != PRC_OK) return rc;
-    std::vector<const float*> u(n_frames);
-    for (int i = 0; i < n_frames; ++i) {  // u = f / W on the support, out = 0 off it
-        PRC_CUDA(forward_prep(h->params, h->W, d_in[i], h->frames[i].u, d_out[i], s));
+    for (int first = 0; first < n_frames; first += kMaxFrames) {
+        const int k = std::min(kMaxFrames, n_frames - first);
+        if (k == 1) {
+            if (const int rc = prc_forward(h, d_in[first], d_out[first], s); rc != PRC_OK) return rc;
+            continue;
+        }
+        float4* u4 = h->frame_u4[first / kMaxFrames];
+        FramePrep fp;  // u = f / W interleaved, out = 0 off the support
+        FrameArgs fr;
+        fp.n = fr.n = k;
+        for (int f = 0; f < k; ++f) fp.f[f] = d_in[first + f], fp.out[f] = d_out[first + f], fr.out[f] = d_out[first + f];
+        PRC_CUDA(frame_prep(h->params, h->W, fp, false, u4, s));
         ++h->launches;
-        u[i] = h->frames[i].u;
+        fr.in4 = u4;
+        if (const int rc = frame_pass(h, Op::Forward, fr, s); rc != PRC_OK) return rc;
     }
-    return project_frame_passes(h, Op::Forward, n_frames, u.data(), d_out, nullptr, nullptr, s);
+    return PRC_OK;
 }
 
 int prc_adjoint_frames(prc_handle* h, int n_frames, const float* const* d_in, float* const* d_out, void* stream) {
@@ -1201,7 +1206,23 @@ int prc_adjoint_frames(prc_handle* h, int n_frames, const float* const* d_in, fl
             if (const int rc = prc_adjoint(h, d_in[i], d_out[i], s); rc != PRC_OK) return rc;
         return PRC_OK;
     }
-    return project_frame_passes(h, Op::Adjoint, n_frames, d_in, d_out, nullptr, nullptr, s);
+    if (const int rc = ensure_frames(h, n_frames); rc != PRC_OK) return rc;
+    for (int first = 0; first < n_frames; first += kMaxFrames) {
+        const int k = std::min(kMaxFrames, n_frames - first);
+        if (k == 1) {
+            if (const int rc = prc_adjoint(h, d_in[first], d_out[first], s); rc != PRC_OK) return rc;
+            continue;
+        }
+        float4* v4 = h->frame_r4[first / kMaxFrames];
+        PRC_CUDA(frame_pack(d_in + first, k, h->n, v4, s));
+        ++h->launches;
+        FrameArgs fr;
+        fr.n = k;
+        fr.in4 = v4;
+        for (int f = 0; f < k; ++f) fr.out[f] = d_out[first + f];
+        if (const int rc = frame_pass(h, Op::Adjoint, fr, s); rc != PRC_OK) return rc;
+    }
+    return PRC_OK;
 }
 
 int prc_em_run_frames(prc_handle* h, int n_frames, const float* const* d_g, float* const* d_out, int iterations,
@@ -1222,9 +1243,9 @@ int prc_em_run_frames(prc_handle* h, int n_frames, const float* const* d_g, floa
     if (const int rc = ensure_frames(h, n_frames); rc != PRC_OK) return rc;
     const int n = n_frames;
     // Every frame runs prc_em_iterate's five-launch iteration (prc.cu:675-700) with its own
-    // volumes and FP64 scalars; only the two projections are shared passes over the field.
+    // volumes and FP64 scalars; the preparation and the two projections are shared per group.
     std::vector<float*> f(n), prev(n), y(n), hp(n), est(n);
-    std::vector<const float*> u(n), start(n), est_in(n), g(n), eps(n);
+    std::vector<const float*> start(n);
     std::vector<EmVolumes> v(n);
     auto scalar = [](const EmScalars* sc, size_t off) {
         return reinterpret_cast<const float*>(reinterpret_cast<const char*>(sc) + off);
@@ -1233,29 +1254,53 @@ int prc_em_run_frames(prc_handle* h, int n_frames, const float* const* d_g, floa
         const prc_handle::Frame& fr = h->frames[i];
         f[i] = fr.vol[0], prev[i] = fr.vol[1], y[i] = fr.vol[2], hp[i] = fr.vol[3], est[i] = fr.vol[4];
         v[i] = EmVolumes{h->n, h->support, fr.scalars, fr.red};
-        g[i] = fr.g;
-        u[i] = fr.u;
-        eps[i] = scalar(fr.scalars, offsetof(EmScalars, eps));
         for (float* p : {prev[i], y[i], hp[i]}) PRC_CUDA(cudaMemsetAsync(p, 0, h->n * sizeof(float), s));
         PRC_CUDA(em_begin(v[i], d_g[i], fr.g, f[i], h->n_active, iterations > 0, s));
         h->launches += iterations > 0 ? 3 : 1;
     }
     for (int it = 0; it < iterations; ++it) {
-        for (int i = 0; i < n; ++i) {
-            if (accelerate) {
-                PRC_CUDA(forward_prep_extrapolate(h->params, h->W, f[i], prev[i],
-                                                  scalar(h->frames[i].scalars, offsetof(EmScalars, lambda)), y[i],
-                                                  h->frames[i].u, est[i], s));
+        // forward preparation (with the prediction), forward gather with the ratio, adjoint gather
+        for (int first = 0; first < n; first += kMaxFrames) {
+            const int k = std::min(kMaxFrames, n - first);
+            const prc_handle::Frame* fr0 = &h->frames[first];
+            FrameArgs fwd, adj;
+            fwd.n = adj.n = k;
+            if (k == 1) {  // the single-volume kernels: u and the ratio in the frame's own volumes
+                const int i = first;
+                if (accelerate) {
+                    PRC_CUDA(forward_prep_extrapolate(h->params, h->W, f[i], prev[i],
+                                                      scalar(fr0->scalars, offsetof(EmScalars, lambda)), y[i], fr0->u,
+                                                      est[i], s));
+                } else {
+                    PRC_CUDA(forward_prep(h->params, h->W, f[i], fr0->u, est[i], s));
+                }
+                fwd.in[0] = fr0->u, fwd.out[0] = est[i];
+                adj.in[0] = est[i], adj.out[0] = prev[i];
             } else {
-                PRC_CUDA(forward_prep(h->params, h->W, f[i], h->frames[i].u, est[i], s));
+                float4 *u4 = h->frame_u4[first / kMaxFrames], *r4 = h->frame_r4[first / kMaxFrames];
+                FramePrep fp;
+                fp.n = k;
+                for (int j = 0; j < k; ++j) {
+                    const int i = first + j;
+                    fp.f[j] = f[i], fp.prev[j] = prev[i], fp.y[j] = y[i], fp.out[j] = est[i];
+                    fp.lambda[j] = scalar(h->frames[i].scalars, offsetof(EmScalars, lambda));
+                    adj.out[j] = prev[i];
+                }
+                PRC_CUDA(frame_prep(h->params, h->W, fp, accelerate != 0, u4, s));
+                fwd.in4 = u4, fwd.out4 = r4;  // the ratio, interleaved for the adjoint's gather
+                adj.in4 = r4;
             }
             ++h->launches;
-            start[i] = accelerate ? y[i] : f[i];
-            est_in[i] = est[i];
+            for (int j = 0; j < k; ++j) {
+                const int i = first + j;
+                fwd.ratio_g[j] = h->frames[i].g;
+                fwd.ratio_eps[j] = scalar(h->frames[i].scalars, offsetof(EmScalars, eps));
+                start[i] = accelerate ? y[i] : f[i];
+            }
+            if (const int rc = frame_pass(h, Op::Forward, fwd, s); rc != PRC_OK) return rc;
+            if (const int rc = frame_pass(h, Op::Adjoint, adj, s); rc != PRC_OK) return rc;
         }
-        int rc = project_frame_passes(h, Op::Forward, n, u.data(), est.data(), g.data(), eps.data(), s);
-        if (rc == PRC_OK) rc = project_frame_passes(h, Op::Adjoint, n, est_in.data(), prev.data(), nullptr, nullptr, s);
-        if (rc != PRC_OK) return rc;
+        // est is 0 off the support (the preparation wrote it), which the update leaves there
         for (int i = 0; i < n; ++i) {
             PRC_CUDA(em_update_active(v[i], h->g, h->active, h->n_active, h->geo_w, start[i], prev[i], est[i], beta,
                                       gamma, s));

@@ -705,21 +705,26 @@ __global__ void __launch_bounds__(kMaxBlock) project_batch_kernel(const BatchIte
     }
 }
 
-// NF frames through one stored field (fr.n == NF): the gather forms only -- the adjoint over the
-// source-major field and the forward over the target-major one (lanes are targets, fr.in holds
-// each frame's u = f / W).  The stream is consumed exactly as project_group consumes it (the
-// bf16 vectors loaded by the lanes, the fp32 and 24-bit packs through the per-warp TMA ring), but
-// each pack's weights, template offsets and w > 0 predicates serve NF gathers and NF
-// accumulators.  Fewer packs per batch as NF grows keep the gathers in flight per lane (and the
-// registers) where the single-volume kernel has them.  Each frame accumulates its terms in stream
-// order with fmaf, as project_group does, so every frame equals its single-volume projection bit
-// for bit.
-template <Op OP, int FAR_MODE, int NF>
+// Up to four frames through one stored field: the gather forms only -- the adjoint over the
+// source-major field and the forward over the target-major one (lanes are targets, the gathered
+// volume holds each frame's u = f / W).  The gathered volumes are interleaved, fr.in4[t] = the
+// four frames' values of voxel t, so ONE 16-byte gather per lane and step fetches every frame:
+// the same cache lines, hence the same L1 wavefronts, as one frame's 4-byte gather (the L1 data
+// pipe is what bounds these kernels).  The stream is consumed exactly as project_group consumes
+// it (the bf16 vectors loaded by the lanes, the fp32 and 24-bit packs through the per-warp TMA
+// ring); each pack's weights, template offsets and w > 0 predicates serve all four frames.  One
+// pack per batch keeps 16 gathered values in flight per lane, as the single-volume kernel.  Each
+// frame accumulates its terms in stream order with fmaf, as project_group does, so every frame
+// equals its single-volume projection bit for bit.  Slots fr.n..3 are padding (gathered zeros,
+// nothing written).
+template <Op OP, int FAR_MODE>
 __device__ __forceinline__ void project_frames_group(const ProjParams& p, const OpArgs& a, const FrameArgs& fr,
                                                      int group, int warp, unsigned char* dyn_smem, uint64_t* bars) {
     static_assert(OP == Op::Adjoint ? !target_major(FAR_MODE) : (OP == Op::Forward && target_major(FAR_MODE)),
                   "gather forms only");
     static_assert(!half_volume(FAR_MODE) && FAR_MODE != kMarch, "fp32 volumes through a stored field");
+    constexpr int NF = kMaxFrames;  // the interleaved width: one float4 per voxel
+    static_assert(NF == 4, "frames are interleaved four to a 16-byte vector");
     const int lane = threadIdx.x & 31;
     if (group * kLanes >= p.n_active) return;  // the whole warp leaves together
     const int src = group * kLanes + lane;
@@ -731,7 +736,8 @@ __device__ __forceinline__ void project_frames_group(const ProjParams& p, const 
         live = valid && ws > 0.0f;
         if (valid && !live)
 #pragma unroll
-            for (int f = 0; f < NF; ++f) fr.out[f][s] = 0.0f;
+            for (int f = 0; f < NF; ++f)
+                if (f < fr.n) fr.out[f][s] = 0.0f;
     }
     if (!__any_sync(kFull, live)) return;
 
@@ -739,7 +745,7 @@ __device__ __forceinline__ void project_frames_group(const ProjParams& p, const 
     constexpr int kBase = field_base(FAR_MODE);
     constexpr int kElem = kBase == kFieldF32 ? 4 : (kBase == kField24 ? 3 : 2);
     constexpr int kPackBytes = kPack * kLanes * kElem;
-    constexpr int kB = NF == 1 ? 4 : (NF == 2 ? 2 : 1);  // packs per batch: kB * 4 * NF gathers in flight
+    constexpr int kB = 1;  // packs per batch: 4 steps x 4 frames of gathered values in flight
     constexpr int kPacksPerChunk = kChunk / kPackBytes / kB * kB;
     constexpr int kChunkBytes = kPacksPerChunk * kPackBytes;
     static_assert(kPacksPerChunk > 0 && kChunkBytes % 16 == 0, "bulk copies of whole 16-byte units");
@@ -761,15 +767,17 @@ __device__ __forceinline__ void project_frames_group(const ProjParams& p, const 
             idx[k * kPack] = (int)((unsigned)s + (unsigned)tc[k].x), idx[k * kPack + 1] = (int)((unsigned)s + (unsigned)tc[k].y);
             idx[k * kPack + 2] = (int)((unsigned)s + (unsigned)tc[k].z), idx[k * kPack + 3] = (int)((unsigned)s + (unsigned)tc[k].w);
         }
-        float v[NF][kB * kPack];
+        float4 v[kB * kPack];
 #pragma unroll
         for (int u = 0; u < kB * kPack; ++u)
+            v[u] = w[u] > 0.0f ? __ldg(fr.in4 + idx[u]) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
 #pragma unroll
-            for (int f = 0; f < NF; ++f) v[f][u] = w[u] > 0.0f ? __ldg(fr.in[f] + idx[u]) : 0.0f;
-#pragma unroll
-        for (int u = 0; u < kB * kPack; ++u)
-#pragma unroll
-            for (int f = 0; f < NF; ++f) acc[f] = fmaf(w[u], v[f][u], acc[f]);
+        for (int u = 0; u < kB * kPack; ++u) {
+            acc[0] = fmaf(w[u], v[u].x, acc[0]);
+            acc[1] = fmaf(w[u], v[u].y, acc[1]);
+            acc[2] = fmaf(w[u], v[u].z, acc[2]);
+            acc[3] = fmaf(w[u], v[u].w, acc[3]);
+        }
     };
 
     if constexpr (kBase == kFieldBF16) {
@@ -888,25 +896,34 @@ __device__ __forceinline__ void project_frames_group(const ProjParams& p, const 
         if (live) {
             const float ws = __ldg(a.W + src);
 #pragma unroll
-            for (int f = 0; f < NF; ++f) fr.out[f][s] = acc[f] / ws;  // prc.cu:266
+            for (int f = 0; f < NF; ++f)
+                if (f < fr.n) fr.out[f][s] = acc[f] / ws;  // prc.cu:266
         }
-    } else {
-        if (valid)
+    } else if (valid) {
+        float r[NF];
+#pragma unroll
+        for (int f = 0; f < NF; ++f)  // inside MAP-EM the EM ratio (prc.cu:270-274)
+            r[f] = f >= fr.n ? 0.0f
+                             : (fr.ratio_g[f] ? __ldg(fr.ratio_g[f] + s) / fmaxf(acc[f], __ldg(fr.ratio_eps[f])) : acc[f]);
+        if (fr.out4) {
+            fr.out4[s] = make_float4(r[0], r[1], r[2], r[3]);
+        } else {
 #pragma unroll
             for (int f = 0; f < NF; ++f)
-                fr.out[f][s] = fr.ratio_g[f] ? __ldg(fr.ratio_g[f] + s) / fmaxf(acc[f], __ldg(fr.ratio_eps[f])) : acc[f];
+                if (f < fr.n) fr.out[f][s] = r[f];
+        }
     }
 }
 
 // 64 registers at most (four 256-thread blocks per SM), as the single-volume stream kernel.
-template <Op OP, int FAR_MODE, int NF>
+template <Op OP, int FAR_MODE>
 __global__ void __launch_bounds__(kMaxBlock, 4) project_frames_kernel(const ProjParams p, const OpArgs a,
                                                                       const FrameArgs fr) {
     extern __shared__ __align__(128) unsigned char dyn_smem[];
     __shared__ uint64_t field_bars[kMaxWarps][kStages];
     const int warp = threadIdx.x >> 5;
-    project_frames_group<OP, FAR_MODE, NF>(p, a, fr, blockIdx.x * (blockDim.x >> 5) + warp, warp, dyn_smem,
-                                           field_bars[warp]);
+    project_frames_group<OP, FAR_MODE>(p, a, fr, blockIdx.x * (blockDim.x >> 5) + warp, warp, dyn_smem,
+                                       field_bars[warp]);
 }
 
 // Template rows: row 0 the near block's 125 offsets (then zeros), rows 1..n_rays the offsets of
@@ -1254,6 +1271,46 @@ __global__ void surrogate_template_kernel(const ProjParams p, const int* offset,
         tmpl[(size_t)(1 + p.n_rays + r) * p.tmpl_len + j] = j < kRadialBins ? offset[r * kRadialBins + j] : 0;
 }
 
+// The interleaved input of a frame pass: per voxel and frame the expressions of
+// forward_prep_kernel (PREDICT false: y = f) or forward_prep_extrapolate_kernel (PREDICT true),
+// the frames' u = y / W stored side by side in one 16-byte vector (zeros in the unused slots).
+template <bool PREDICT>
+__global__ void frame_prep_kernel(const int* __restrict__ vox2src, const float* __restrict__ W, const FramePrep fp,
+                                  float4* __restrict__ u4, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const int src = vox2src[i];
+        const float ws = src >= 0 ? __ldg(W + src) : 0.0f;
+        float u[kMaxFrames];
+#pragma unroll
+        for (int k = 0; k < kMaxFrames; ++k) {
+            u[k] = 0.0f;
+            if (k >= fp.n) continue;
+            const float fi = fp.f[k][i];
+            float yi = fi;
+            if constexpr (PREDICT) {
+                const float lambda = __ldg(fp.lambda[k]), pi = fp.prev[k][i];
+                yi = fmaxf(fi + lambda * (fi - pi), 0.5f * fi);  // prc.cu:320
+                fp.y[k][i] = yi;
+            }
+            float scale = 0.0f;
+            if (src >= 0) scale = ws > 0.0f ? yi / ws : 0.0f;  // prc.cu:246
+            else fp.out[k][i] = 0.0f;
+            u[k] = scale > 0.0f ? scale : 0.0f;
+        }
+        u4[i] = make_float4(u[0], u[1], u[2], u[3]);
+    }
+}
+
+// The frames' volumes fp.f[k] side by side, one 16-byte vector per voxel.
+__global__ void frame_pack_kernel(const FramePrep fp, float4* __restrict__ v4, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        float v[kMaxFrames];
+#pragma unroll
+        for (int k = 0; k < kMaxFrames; ++k) v[k] = k < fp.n ? __ldg(fp.f[k] + i) : 0.0f;
+        v4[i] = make_float4(v[0], v[1], v[2], v[3]);
+    }
+}
+
 __global__ void forward_prep_batch_kernel(const PrepItem* items) {
     const PrepItem it = items[blockIdx.y];
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < it.n; i += (long long)gridDim.x * blockDim.x) {
@@ -1436,6 +1493,24 @@ cudaError_t project_batch(Op op, const BatchItem* d_items, int n_items, int tota
     return cudaErrorInvalidValue;
 }
 
+cudaError_t frame_prep(const ProjParams& p, const float* W, const FramePrep& fp, bool predict, float4* u4,
+                       cudaStream_t s) {
+    if (fp.n < 2 || fp.n > kMaxFrames) return cudaErrorInvalidValue;
+    const size_t n = (size_t)p.nxy * p.g.nz;
+    if (predict) frame_prep_kernel<true><<<592, 256, 0, s>>>(p.vox2src, W, fp, u4, n);
+    else frame_prep_kernel<false><<<592, 256, 0, s>>>(p.vox2src, W, fp, u4, n);
+    return cudaGetLastError();
+}
+
+cudaError_t frame_pack(const float* const* in, int n_frames, size_t voxels, float4* v4, cudaStream_t s) {
+    if (n_frames < 2 || n_frames > kMaxFrames) return cudaErrorInvalidValue;
+    FramePrep fp;
+    fp.n = n_frames;
+    for (int k = 0; k < n_frames; ++k) fp.f[k] = in[k];
+    frame_pack_kernel<<<592, 256, 0, s>>>(fp, v4, voxels);
+    return cudaGetLastError();
+}
+
 namespace {
 template <Op OP, int FAR_MODE>
 cudaError_t launch_frames(const ProjParams& p, const OpArgs& a, const FrameArgs& fr, cudaStream_t s) {
@@ -1451,17 +1526,17 @@ cudaError_t launch_frames(const ProjParams& p, const OpArgs& a, const FrameArgs&
         kernel<<<blocks, kBlock, kFieldSmemBytes, s>>>(p, a, fr);
         return cudaGetLastError();
     };
-    switch (fr.n) {
-        case 2: return go(project_frames_kernel<OP, FAR_MODE, 2>);
-        case 4: return go(project_frames_kernel<OP, FAR_MODE, 4>);
-        default: return cudaErrorInvalidValue;
-    }
+    if (fr.n < 2 || fr.n > kMaxFrames || !fr.in4) return cudaErrorInvalidValue;
+    return go(project_frames_kernel<OP, FAR_MODE>);
 }
 }  // namespace
 
 cudaError_t project_frames(Op op, const ProjParams& p, const OpArgs& a, const FrameArgs& fr, cudaStream_t s) {
-    for (int f = 0; f < fr.n && f < kMaxFrames; ++f)
-        if (!fr.in[f] || !fr.out[f] || (fr.ratio_g[f] && !fr.ratio_eps[f])) return cudaErrorInvalidValue;
+    if (fr.n < 1 || fr.n > kMaxFrames) return cudaErrorInvalidValue;
+    for (int f = 0; f < fr.n; ++f) {
+        const bool out_ok = fr.out[f] || (fr.n > 1 && op == Op::Forward && fr.out4);
+        if (!out_ok || (fr.ratio_g[f] && !fr.ratio_eps[f]) || (fr.n == 1 && !fr.in[0])) return cudaErrorInvalidValue;
+    }
     if (fr.n == 1) {  // one frame: the single-volume kernel (same stream, same accumulation order)
         if (op == Op::Forward ? !a.farT.on() : !a.far.on()) return cudaErrorInvalidValue;
         OpArgs b = a;

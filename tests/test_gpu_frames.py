@@ -6,7 +6,8 @@ the stored field one pass projects up to four frames: the stream of weights, the
 offsets and predicates are read once and serve every frame's gather.  Each frame keeps the
 single-volume accumulation order and the single-volume MAP-EM kernels, so its result must equal
 the single-volume entry point's on the same input BIT FOR BIT in every stored-weight format and
-for frame counts that use the 4-, 2- and 1-frame passes.  The forms without both majors of the
+for frame counts that make groups of four, three and two interleaved frames and of one frame
+(which takes the single-volume kernels).  The forms without both majors of the
 field run the frames one by one (their forward scatters with atomics, so they agree to rounding).
 One case is also pinned to the reference executable's own MAP-EM output."""
 import ctypes
@@ -60,7 +61,7 @@ def assert_identical(got, expect, what):
 def test_projections_equal_single_volume(torso, form):
     P = projector(torso, FORMS[form])
     assert P.cache_mode[0] == pm.PRC_CACHE_FULL
-    ins = frames(P.shape, 7, seed=1)  # passes of 4, 2 and 1 frames
+    ins = frames(P.shape, 9, seed=1)  # two interleaved groups of four, then one frame alone
     fwd = [torch.full_like(x, -7.0) for x in ins]
     P.forward_frames(ins, fwd)
     adj = [torch.full_like(x, -7.0) for x in ins]  # the adjoint leaves off-tissue voxels untouched
