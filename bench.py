@@ -372,9 +372,11 @@ def run_ours(args):
     batch = None
     if single and not args.no_batch:
         batch = batch_record(frames=8, iterations=10, steps=2, warmup=1)
-    shared = None
+    shared = study = None
     if single and not args.no_batch and args.form != "traced":
         shared = shared_frames_record(P, truth, g_host, stream, l2_flush, args.iterations, value, corrected)
+        if args.form == "fp32":
+            study = study_batch_record(rho, truth, spacing, args.iterations, value)
 
     if world > 1:
         torch.distributed.barrier()
@@ -457,6 +459,8 @@ def run_ours(args):
         line["batch"] = batch
     if shared:
         line["shared_density_frames"] = shared
+    if study:
+        line["study_batch"] = study
     print(json.dumps(line))
     if world > 1:
         torch.distributed.destroy_process_group()
@@ -1002,6 +1006,48 @@ def shared_frames_record(P, truth, g_host, stream, l2_flush, iterations, single_
                         "adjoint": round(passes["adjoint_ms"] / max(passes["adjoint_launches"], 1), 4),
                         "frames_per_pass": min(n_frames, 4)},
             "frame0_max_abs_diff_vs_single_volume": diff}
+
+
+def study_batch_record(rho, truth, spacing, iterations, single_value, n_frames: int = 8, steps: int = 3,
+                       warmup: int = 1) -> dict:
+    """A dynamic study through the batch API: n_frames frames of the torso passing the same density
+    array (prc_batch_create shares one projector among them and the batched projections take them
+    four at a time), the data n_frames Poisson draws of the same blur; one graph replay of
+    `iterations` MAP-EM iterations of every frame per step."""
+    import torch
+    import prc_mlem_b200 as pm
+    from prc_mlem_b200 import phantoms
+    batch = pm.Batch([(ISOTOPE, rho, spacing)] * n_frames, rays=RAYS, support_rho=SUPPORT_RHO)
+    stream = torch.cuda.ExternalStream(batch.stream)
+    with pm.Projector(ISOTOPE, rho, spacing, rays=RAYS, support_rho=SUPPORT_RHO) as P:
+        blur = torch.empty(truth.size, dtype=torch.float32, device="cuda")
+        P.forward(torch.from_numpy(np.ascontiguousarray(truth, np.float32)).cuda().reshape(-1), blur)
+        P.synchronize()
+    gs = [phantoms.poisson_counts_device(blur, COUNTS, seed=300 + k) for k in range(n_frames)]
+    outs = [torch.empty_like(g) for g in gs]
+    torch.cuda.synchronize()
+    for _ in range(warmup):
+        batch.correct(gs, outs, iterations, BETA, GAMMA, True)
+    batch.synchronize()
+    times = []
+    for _ in range(steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        batch.correct(gs, outs, iterations, BETA, GAMMA, True)
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    total_s = sum(times) / 1e3
+    value = n_frames * iterations * steps / total_s
+    device_gb = [round(batch.device_bytes(i) / 1e9, 3) for i in (0, 1)]
+    batch.close()
+    return {"value": round(value, 3), "unit": "EM frame-iterations/s",
+            "frames_per_s": round(n_frames * steps / total_s, 3), "x_single_volume": round(value / single_value, 3),
+            "steps": steps, "warmup": warmup, "ms_per_step": round(sum(times) / steps, 3),
+            "device_gb_owner_and_sharer": device_gb,
+            "config": {"workload": f"{n_frames} frames of the 128x128x159 68Ga torso passing one density array to "
+                                   f"prc_batch_create, {iterations} MAP-EM iterations each per step (beta {BETA}, "
+                                   f"gamma {GAMMA}, accel), fp32 stored field, one graph replay per step"}}
 
 
 # ------------------------------------------------------------------------------- batched frames

@@ -243,8 +243,11 @@ int prc_sum_static(const float* d_x, int64_t n, double* d_sum, void* stream);
  * reductions), and the whole schedule of a run is captured once into a CUDA graph and replayed.
  * Each frame chooses its projector form as prc_create does (stored field while memory lasts,
  * then the near cache); with `net`, frames of 18F, 68Ga and 82Rb use the learned surrogate
- * (prc_create_surrogate with target_scale and fallback_nrmse).  The first run autotunes the
- * projector's warps per block (2, 4 or 8) on one forward projection of every frame. */
+ * (prc_create_surrogate with target_scale and fallback_nrmse).  Frames that pass the same
+ * density_host pointer with the same geometry and isotope (the frames of one study) share one
+ * projector: it is built once, and the later frames hold only their own MAP-EM volumes.  The
+ * first run autotunes the projector's warps per block (2, 4 or 8) on one forward projection of
+ * every frame. */
 typedef struct prc_frame {
     prc_geometry geometry;
     const char* isotope;

@@ -410,7 +410,9 @@ class Batch:
     """Many frames (density maps of any grid, isotope) corrected together: one launch per MAP-EM
     phase for all frames, the schedule captured into a CUDA graph (prc_batch_*).
 
-    frames: list of (isotope, density (nz, ny, nx), spacing (dx, dy, dz)).
+    frames: list of (isotope, density (nz, ny, nx), spacing (dx, dy, dz)).  Frames that pass the
+    same density array object with the same isotope and spacing (the frames of one study) share
+    one projector.
     """
 
     def __init__(self, frames, rays: int = 128, support_rho: float = 0.05, cache: int = PRC_CACHE_FULL,
@@ -419,8 +421,9 @@ class Batch:
         self._keep = []
         arr = (Frame * len(frames))()
         self.shapes = []
+        converted = {}  # one host array per distinct density object, so shared maps stay shared
         for i, (iso, rho, spacing) in enumerate(frames):
-            rho = _host(rho)
+            rho = converted.setdefault(id(rho), _host(rho))
             nz, ny, nx = rho.shape
             self._keep.append(rho)
             self.shapes.append(rho.shape)
@@ -482,6 +485,13 @@ class Batch:
         h = _P()
         _check(lib().prc_batch_frame(self._h, i, ctypes.byref(h)))
         return h.value
+
+    def device_bytes(self, i: int) -> int:
+        """Device memory frame i's handle allocated itself (a frame sharing another frame's
+        projector counts only its own MAP-EM volumes and scratch)."""
+        v = ctypes.c_int64()
+        _check(lib().prc_device_bytes(self.frame_handle(i), ctypes.byref(v)))
+        return v.value
 
     def forward(self, i: int, d_in, d_out) -> None:
         """Forward projection of frame i with its own projector (its handle's stream)."""

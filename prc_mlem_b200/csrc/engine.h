@@ -172,44 +172,6 @@ int radial_water_bins();
 // weights in a surrogate field (and trains no network output).
 constexpr float kBeyondShare = 0.02f;
 
-// ---- batched projection over many volumes (one launch for all) --------------------------------
-enum BatchMode : int {
-    kBatchTraceMarch = 0,      // near block and far rays traced every pass
-    kBatchCacheF32March = 1,   // near cache (fp32 / bf16), far rays traced
-    kBatchCacheBF16March = 2,
-    kBatchFieldF32 = 3,        // stored field, source-major (adjoint gather / forward scatter)
-    kBatchFieldBF16 = 4,
-    kBatchFieldF32T = 5,       // stored field, target-major (forward gather of u = f / W)
-    kBatchFieldBF16T = 6,
-    kBatchField24 = 7,         // the 24-bit field, source-major and target-major
-    kBatchField24T = 8
-};
-struct BatchItem {
-    ProjParams p;
-    OpArgs a;
-    int mode;
-    int first_block;  // blocks [first_block, first_block + blocks) of the launch belong to this item
-    int blocks;
-    int pad;
-};
-// Dynamic shared memory per warp a mode needs.
-size_t batch_smem_per_warp(int mode);
-cudaError_t project_batch(Op op, const BatchItem* d_items, int n_items, int total_blocks, int warps, size_t smem,
-                          cudaStream_t s);
-// Batched forward preparation: gather items get u = f / W (and 0 off the support of out),
-// scatter items get out = 0.
-struct PrepItem {
-    const int* vox2src;
-    const float* W;
-    const float* f;
-    float* u;
-    float* out;
-    long long n;
-    int gather;
-    int pad;
-};
-cudaError_t forward_prep_batch(const PrepItem* d_items, int n_items, cudaStream_t s);
-
 // ---- frames that share one stored field (dynamic PET: one density, many activity volumes) ----
 // One pass over the stored field projects up to kMaxFrames volumes: every stored weight, its
 // template offsets and its predicate are loaded once, and one 16-byte gather of the interleaved
@@ -247,6 +209,61 @@ struct FramePrep {
 cudaError_t frame_prep(const ProjParams& p, const float* W, const FramePrep& fp, bool predict, float4* u4,
                        cudaStream_t s);
 cudaError_t frame_pack(const float* const* in, int n, size_t voxels, float4* v4, cudaStream_t s);
+
+// ---- batched projection over many volumes (one launch for all) --------------------------------
+enum BatchMode : int {
+    kBatchTraceMarch = 0,      // near block and far rays traced every pass
+    kBatchCacheF32March = 1,   // near cache (fp32 / bf16), far rays traced
+    kBatchCacheBF16March = 2,
+    kBatchFieldF32 = 3,        // stored field, source-major (adjoint gather / forward scatter)
+    kBatchFieldBF16 = 4,
+    kBatchFieldF32T = 5,       // stored field, target-major (forward gather of u = f / W)
+    kBatchFieldBF16T = 6,
+    kBatchField24 = 7,         // the 24-bit field, source-major and target-major
+    kBatchField24T = 8,
+    // frames sharing one projector, up to four per item (BatchItem::fr, interleaved volumes)
+    kBatchFramesF32 = 9,
+    kBatchFramesBF16 = 10,
+    kBatchFrames24 = 11,
+    kBatchFramesF32T = 12,
+    kBatchFramesBF16T = 13,
+    kBatchFrames24T = 14
+};
+struct BatchItem {
+    ProjParams p;
+    OpArgs a;
+    FrameArgs fr;  // kBatchFrames* modes: the frames of this item (fr.in4, fr.out[0..fr.n))
+    int mode;
+    int first_block;  // blocks [first_block, first_block + blocks) of the launch belong to this item
+    int blocks;
+    int pad;
+};
+// Dynamic shared memory per warp a mode needs.
+size_t batch_smem_per_warp(int mode);
+cudaError_t project_batch(Op op, const BatchItem* d_items, int n_items, int total_blocks, int warps, size_t smem,
+                          cudaStream_t s);
+// Batched forward preparation: gather items get u = f / W (and 0 off the support of out),
+// scatter items get out = 0.  With u4 set, u goes to component `slot` of the interleaved u4
+// instead of u (a frame of a shared pass).
+struct PrepItem {
+    const int* vox2src;
+    const float* W;
+    const float* f;
+    float* u;
+    float* out;
+    long long n;
+    int gather;
+    int slot;
+    float4* u4;
+};
+cudaError_t forward_prep_batch(const PrepItem* d_items, int n_items, cudaStream_t s);
+// Batched interleaving: item i writes v4 = its frames' volumes fp.f[0..fp.n) side by side.
+struct PackItem {
+    FramePrep fp;
+    float4* v4;
+    long long n;
+};
+cudaError_t frame_pack_batch(const PackItem* d_items, int n_items, cudaStream_t s);
 
 // Self-test of the bounded mbarrier wait: a wait that nothing completes, `rounds` rounds.
 cudaError_t wait_selftest(int rounds, unsigned int* error, cudaStream_t s);

@@ -1391,6 +1391,12 @@ struct prc_batch {
     int key_iters = -1, key_accel = -1;
     float key_beta = -1.0f, key_gamma = -1.0f;
     static constexpr int kWarpsDefault = 4;
+    // Frames sharing one projector with its stored field in both majors go through the
+    // projections in chunks of 2..4 (one item of the batched launch each, gathering the
+    // interleaved u4 / r4 of the chunk); chunk_of / slot_of place a frame (-1: its own item).
+    std::vector<std::vector<int>> chunks;
+    std::vector<float4*> chunk_u4, chunk_r4;
+    std::vector<int> chunk_of, slot_of;
 };
 
 namespace {
@@ -1401,6 +1407,11 @@ int batch_mode(const prc_handle* h, Op op) {
     if (h->far_field.on()) return h->far_field.b16 ? kBatchFieldBF16 : (h->far_field.b24 ? kBatchField24 : kBatchFieldF32);
     if (!h->trace_near && h->cache.on()) return h->cache.b16 ? kBatchCacheBF16March : kBatchCacheF32March;
     return kBatchTraceMarch;
+}
+
+int frames_mode(const prc_handle* h, Op op) {
+    if (op == Op::Forward) return h->far_t.b16 ? kBatchFramesBF16T : (h->far_t.b24 ? kBatchFrames24T : kBatchFramesF32T);
+    return h->far_field.b16 ? kBatchFramesBF16 : (h->far_field.b24 ? kBatchFrames24 : kBatchFramesF32);
 }
 
 void release_graph(prc_batch* b) {
@@ -1414,7 +1425,8 @@ void release_graph(prc_batch* b) {
 struct BatchPlan {
     std::vector<unsigned char> host;  // all tables, uploaded at once
     struct Launch {
-        int kind;  // 0 EM phase, 1 projector, 2 forward prep, 3 memset (frame, buffer), 4 copy-out (frame)
+        int kind;  // 0 EM phase, 1 projector, 2 forward prep, 3 memset (frame, buffer), 4 copy-out (frame),
+                   // 5 interleaving of the chunks' EM ratios
         EmPhase phase;
         Op op;
         size_t offset;  // of its table in `host`
@@ -1467,25 +1479,36 @@ BatchPlan plan_batch(prc_batch* b, const float* const* d_g, float* const* d_out,
         plan.launches.push_back(l);
     };
     auto projector_launch = [&](Op op, const std::vector<const float*>& in, const std::vector<float*>& out) {
-        std::vector<BatchItem> items(n);
+        std::vector<BatchItem> items;
         int blocks = 0;
         size_t smem = 0;
         for (int i = 0; i < n; ++i) {
+            const int c = b->chunk_of[i];
+            if (c >= 0 && b->slot_of[i] != 0) continue;  // the chunk's item is made at its first frame
             prc_handle* h = b->frames[i];
-            BatchItem& it = items[i];
+            BatchItem it{};
             it.p = h->params;
             it.a = h->op_args();
             it.a.in = in[i];
             it.a.out = out[i];
             it.mode = batch_mode(h, op);
+            if (c >= 0) {  // one pass for the chunk's frames
+                const std::vector<int>& fr = b->chunks[c];
+                it.mode = frames_mode(h, op);
+                it.fr.n = (int)fr.size();
+                it.fr.in4 = op == Op::Forward ? b->chunk_u4[c] : b->chunk_r4[c];
+                for (size_t j = 0; j < fr.size(); ++j) it.fr.out[j] = out[fr[j]];
+            }
             const int groups = (h->n_active + kLanes - 1) / kLanes;
             it.blocks = (groups + warps - 1) / warps;
             it.first_block = blocks;
             blocks += it.blocks;
             smem = std::max(smem, batch_smem_per_warp(it.mode) * warps);
+            items.push_back(it);
         }
         BatchPlan::Launch l{};
-        l.kind = 1, l.op = op, l.offset = plan.add(items), l.n_items = n, l.total_blocks = blocks, l.smem = smem;
+        l.kind = 1, l.op = op, l.offset = plan.add(items), l.n_items = (int)items.size(), l.total_blocks = blocks,
+        l.smem = smem;
         plan.launches.push_back(l);
     };
     auto forward = [&](const std::vector<const float*>& in, const std::vector<float*>& out) {
@@ -1494,7 +1517,8 @@ BatchPlan plan_batch(prc_batch* b, const float* const* d_g, float* const* d_out,
         for (int i = 0; i < n; ++i) {
             prc_handle* h = b->frames[i];
             const bool gather = h->far_t.on();
-            prep[i] = PrepItem{h->vox2src, h->W, in[i], h->u, out[i], (long long)h->n, gather ? 1 : 0, 0};
+            prep[i] = PrepItem{h->vox2src, h->W, in[i], h->u, out[i], (long long)h->n, gather ? 1 : 0, 0, nullptr};
+            if (b->chunk_of[i] >= 0) prep[i].u4 = b->chunk_u4[b->chunk_of[i]], prep[i].slot = b->slot_of[i];
             pin[i] = gather ? h->u : in[i];
         }
         BatchPlan::Launch l{};
@@ -1530,6 +1554,18 @@ BatchPlan plan_batch(prc_batch* b, const float* const* d_g, float* const* d_out,
         if (accel) em_launch(EmPhase::Extrapolate, items);
         forward(start, est);
         em_launch(EmPhase::Ratio, items);
+        if (!b->chunks.empty()) {  // the chunks' EM ratios, interleaved for their adjoint passes
+            std::vector<PackItem> pack(b->chunks.size());
+            for (size_t c = 0; c < b->chunks.size(); ++c) {
+                pack[c].fp.n = (int)b->chunks[c].size();
+                for (size_t j = 0; j < b->chunks[c].size(); ++j) pack[c].fp.f[j] = est_in[b->chunks[c][j]];
+                pack[c].v4 = b->chunk_r4[c];
+                pack[c].n = (long long)b->frames[b->chunks[c][0]]->n;
+            }
+            BatchPlan::Launch l{};
+            l.kind = 5, l.offset = plan.add(pack), l.n_items = (int)pack.size();
+            plan.launches.push_back(l);
+        }
         projector_launch(Op::Adjoint, est_in, prev);
         em_launch(EmPhase::Update, items);
         if (beta > 0.0f || accel) em_launch(EmPhase::Finish, items);
@@ -1559,7 +1595,7 @@ int enqueue_plan(prc_batch* b, const BatchPlan& plan, float* const* d_out, float
     const int em_blocks = std::max(1, std::min(kReduceBlocks, 4096 / std::max(1, (int)b->frames.size())));
     for (const BatchPlan::Launch& l : plan.launches) {
         cudaError_t e = cudaSuccess;
-        const bool kernel = l.kind <= 2;
+        const bool kernel = l.kind <= 2 || l.kind == 5;
         if (timed && kernel) {
             std::pair<cudaEvent_t, cudaEvent_t> ev{nullptr, nullptr};
             PRC_CUDA(cudaEventCreate(&ev.first));
@@ -1586,11 +1622,58 @@ int enqueue_plan(prc_batch* b, const BatchPlan& plan, float* const* d_out, float
                 e = cudaMemcpyAsync(d_out[l.frame], l.ptr, b->frames[l.frame]->n * sizeof(float),
                                     cudaMemcpyDeviceToDevice, b->stream);
                 break;
+            case 5:
+                e = frame_pack_batch(reinterpret_cast<const PackItem*>(base + l.offset), l.n_items, b->stream);
+                break;
         }
         if (e != cudaSuccess) return fail(PRC_ERR_CUDA, std::string("CUDA error '") + cudaGetErrorString(e) +
                                                             "' in the batched MAP-EM schedule");
         if (timed && kernel) PRC_CUDA(cudaEventRecord(timed->back().second, b->stream));
     }
+    return PRC_OK;
+}
+
+// Frames that repeat an earlier frame's geometry, isotope and density array share its projector.
+bool same_projector(const prc_frame& a, const prc_frame& b) {
+    const prc_geometry &x = a.geometry, &y = b.geometry;
+    return a.density_host && a.density_host == b.density_host && a.isotope && b.isotope &&
+           std::strcmp(a.isotope, b.isotope) == 0 && x.nx == y.nx && x.ny == y.ny && x.nz == y.nz && x.dx == y.dx &&
+           x.dy == y.dy && x.dz == y.dz;
+}
+
+// A handle on another handle's projector: every projector array (density, support, W, stored
+// field in both majors, templates, rays) is the owner's, read only; the borrower owns its stream,
+// its forward-gather scratch u and, once allocated, its MAP-EM state, and frees only those.
+int borrow_projector(const prc_handle* o, prc_handle** out) {
+    prc_handle* h = new prc_handle(*o);
+    h->allocations.clear();
+    h->bytes = 0;
+    h->launches = 0;
+    h->stream = nullptr;
+    h->u = nullptr;
+    h->scratch = h->scratch_out = nullptr;
+    h->g_em = h->geo_w = nullptr;
+    h->u16 = h->ratio16 = nullptr;
+    for (float*& v : h->vol) v = nullptr;
+    h->f = h->prev = h->y = h->h_prev = h->est = nullptr;
+    h->scalars = nullptr;
+    h->red = Reduction{};
+    h->em_started = false;
+    h->frames.clear();
+    h->frame_u4.clear();
+    h->frame_r4.clear();
+    h->timing = false;
+    for (auto& pool : h->events) pool.clear();
+    h->events_used[0] = h->events_used[1] = 0;
+    cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess && o->u) e = h->alloc(&h->u, h->n);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) {
+        prc_destroy(h);
+        return fail(e == cudaErrorMemoryAllocation ? PRC_ERR_MEMORY : PRC_ERR_CUDA,
+                    std::string("CUDA error '") + cudaGetErrorString(e) + "' while sharing a projector");
+    }
+    *out = h;
     return PRC_OK;
 }
 
@@ -1615,6 +1698,8 @@ void prc_batch_destroy(prc_batch* b) {
     if (b->stream) cudaStreamSynchronize(b->stream);
     release_graph(b);
     if (b->d_tables) cudaFree(b->d_tables);
+    for (float4* p : b->chunk_u4) cudaFree(p);
+    for (float4* p : b->chunk_r4) cudaFree(p);
     for (prc_handle* h : b->frames) prc_destroy(h);
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
@@ -1665,9 +1750,19 @@ int prc_batch_create(int n_frames, const prc_frame* frames, const prc_options* o
     if (opts) member = *opts;
     const bool want_full = member.cache == PRC_CACHE_FULL;
     if (want_full) member.cache = PRC_CACHE_SOURCE_MAJOR;
+    // the frames of one study (the same geometry, isotope and density array) share one projector:
+    // frame i borrows frame owner[i]'s once every projector is built
+    std::vector<int> owner(n_frames, -1);
+    for (int i = 0; i < n_frames; ++i)
+        for (int j = 0; j < i && owner[i] < 0; ++j)
+            if (owner[j] < 0 && same_projector(frames[i], frames[j])) owner[i] = j;
     for (int i = 0; i < n_frames; ++i) {
         const prc_frame& f = frames[i];
         if (near_hold[i]) cudaFree(near_hold[i]), near_hold[i] = nullptr;
+        if (owner[i] >= 0) {
+            b->frames.push_back(nullptr);
+            continue;
+        }
         bool learned = false;
         for (const char* iso : kNet) learned = learned || (net && f.isotope && std::strcmp(f.isotope, iso) == 0);
         prc_handle* h = nullptr;
@@ -1686,6 +1781,7 @@ int prc_batch_create(int n_frames, const prc_frame* frames, const prc_options* o
     }
     if (held) cudaFree(held);
     for (int i = 0; i < n_frames; ++i) {
+        if (!b->frames[i]) continue;
         const int em = ensure_em(b->frames[i]);
         if (em != PRC_OK) {
             const std::string msg = g_last_error;
@@ -1695,8 +1791,9 @@ int prc_batch_create(int n_frames, const prc_frame* frames, const prc_options* o
         }
     }
     if (want_full) {  // target-major copies (forward as a gather), smallest fields first, while they fit
-        std::vector<int> order(n_frames);
-        for (int i = 0; i < n_frames; ++i) order[i] = i;
+        std::vector<int> order;
+        for (int i = 0; i < n_frames; ++i)
+            if (b->frames[i]) order.push_back(i);
         std::sort(order.begin(), order.end(),
                   [&](int x, int y) { return b->frames[x]->far_entries < b->frames[y]->far_entries; });
         for (int i : order) {
@@ -1706,7 +1803,8 @@ int prc_batch_create(int n_frames, const prc_frame* frames, const prc_options* o
             size_t free_b2 = 0, total_b2 = 0;
             if (cudaMemGetInfo(&free_b2, &total_b2) != cudaSuccess) break;
             size_t caller = (size_t)8 << 30;
-            for (prc_handle* o : b->frames) caller += 3 * o->n * sizeof(float);
+            for (int k = 0; k < n_frames; ++k)
+                caller += 3 * (size_t)frames[k].geometry.nx * frames[k].geometry.ny * frames[k].geometry.nz * sizeof(float);
             const size_t elem_b = h->far_field.b16 ? 2 : (h->far_field.b24 ? 3 : 4);
             const size_t need = (size_t)((double)h->far_entries * elem_b * 1.05) + caller;
             if (free_b2 < need) continue;
@@ -1719,6 +1817,49 @@ int prc_batch_create(int n_frames, const prc_frame* frames, const prc_options* o
             }
             if (h->far_t.on()) h->cache_mode = PRC_CACHE_FULL;
         }
+    }
+    for (int i = 0; i < n_frames; ++i) {
+        if (owner[i] < 0) continue;
+        int rc = borrow_projector(b->frames[owner[i]], &b->frames[i]);
+        if (rc == PRC_OK) rc = ensure_em(b->frames[i]);
+        if (rc != PRC_OK) {
+            const std::string msg = g_last_error;
+            prc_batch_destroy(b);
+            g_last_error = "frame " + std::to_string(i) + ": " + msg;
+            return rc;
+        }
+    }
+    // chunks of 2..4 frames on one projector with the stored field in both majors
+    b->chunk_of.assign(n_frames, -1);
+    b->slot_of.assign(n_frames, -1);
+    for (int o = 0; o < n_frames; ++o) {
+        if (owner[o] >= 0) continue;
+        const prc_handle* h = b->frames[o];
+        if (!h->far_t.on() || !h->far_field.on()) continue;
+        std::vector<int> list{o};
+        for (int i = o + 1; i < n_frames; ++i)
+            if (owner[i] == o) list.push_back(i);
+        for (size_t k = 0; k + 1 < list.size(); k += kMaxFrames) {
+            const size_t m = std::min(list.size() - k, (size_t)kMaxFrames);
+            if (m < 2) break;
+            float4 *u4 = nullptr, *r4 = nullptr;
+            cudaError_t e = cudaMalloc(&u4, h->n * sizeof(float4));
+            if (e == cudaSuccess) b->chunk_u4.push_back(u4), e = cudaMalloc(&r4, h->n * sizeof(float4));
+            if (e == cudaSuccess) b->chunk_r4.push_back(r4);
+            if (e == cudaSuccess) e = cudaMemsetAsync(u4, 0, h->n * sizeof(float4), b->stream);
+            if (e == cudaSuccess) e = cudaMemsetAsync(r4, 0, h->n * sizeof(float4), b->stream);
+            if (e != cudaSuccess) {
+                prc_batch_destroy(b);
+                return fail(e == cudaErrorMemoryAllocation ? PRC_ERR_MEMORY : PRC_ERR_CUDA,
+                            std::string("CUDA error '") + cudaGetErrorString(e) + "' for shared frame passes");
+            }
+            for (size_t j = 0; j < m; ++j) b->chunk_of[list[k + j]] = (int)b->chunks.size(), b->slot_of[list[k + j]] = (int)j;
+            b->chunks.emplace_back(list.begin() + k, list.begin() + k + m);
+        }
+    }
+    if (const cudaError_t e = cudaStreamSynchronize(b->stream); e != cudaSuccess) {
+        prc_batch_destroy(b);
+        return fail(PRC_ERR_CUDA, std::string("CUDA error '") + cudaGetErrorString(e) + "' in prc_batch_create");
     }
     *out = b;
     return PRC_OK;

@@ -673,6 +673,10 @@ __global__ void __launch_bounds__(kMaxBlock) project_kernel(const ProjParams p, 
                                                   field_bars[warp]);
 }
 
+template <Op OP, int FAR_MODE>
+__device__ __forceinline__ void project_frames_group(const ProjParams& p, const OpArgs& a, const FrameArgs& fr,
+                                                     int group, int warp, unsigned char* dyn_smem, uint64_t* bars);
+
 // Batched launch over many volumes: block b belongs to the item (volume) whose first_block is
 // the largest one <= b; every item carries its own parameters and projector form.
 template <Op OP>
@@ -701,7 +705,17 @@ __global__ void __launch_bounds__(kMaxBlock) project_batch_kernel(const BatchIte
         case kBatchFieldBF16T: project_group<OP, false, kTraceNear, kFieldBF16T>(p, a, group, warp, dyn_smem, bars); break;
         case kBatchField24: project_group<OP, false, kTraceNear, kField24>(p, a, group, warp, dyn_smem, bars); break;
         case kBatchField24T: project_group<OP, false, kTraceNear, kField24T>(p, a, group, warp, dyn_smem, bars); break;
-        default: break;
+        default:
+            if constexpr (OP == Op::Forward) {
+                if (mode == kBatchFramesF32T) project_frames_group<OP, kFieldF32T>(p, a, items[lo].fr, group, warp, dyn_smem, bars);
+                else if (mode == kBatchFramesBF16T) project_frames_group<OP, kFieldBF16T>(p, a, items[lo].fr, group, warp, dyn_smem, bars);
+                else if (mode == kBatchFrames24T) project_frames_group<OP, kField24T>(p, a, items[lo].fr, group, warp, dyn_smem, bars);
+            } else if constexpr (OP == Op::Adjoint) {
+                if (mode == kBatchFramesF32) project_frames_group<OP, kFieldF32>(p, a, items[lo].fr, group, warp, dyn_smem, bars);
+                else if (mode == kBatchFramesBF16) project_frames_group<OP, kFieldBF16>(p, a, items[lo].fr, group, warp, dyn_smem, bars);
+                else if (mode == kBatchFrames24) project_frames_group<OP, kField24>(p, a, items[lo].fr, group, warp, dyn_smem, bars);
+            }
+            break;
     }
 }
 
@@ -1326,7 +1340,19 @@ __global__ void forward_prep_batch_kernel(const PrepItem* items) {
         } else {
             it.out[i] = 0.0f;
         }
-        it.u[i] = scale > 0.0f ? scale : 0.0f;
+        const float u = scale > 0.0f ? scale : 0.0f;
+        if (it.u4) reinterpret_cast<float*>(it.u4)[4 * i + it.slot] = u;
+        else it.u[i] = u;
+    }
+}
+
+__global__ void frame_pack_batch_kernel(const PackItem* items) {
+    const PackItem it = items[blockIdx.y];
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < it.n; i += (long long)gridDim.x * blockDim.x) {
+        float v[kMaxFrames];
+#pragma unroll
+        for (int k = 0; k < kMaxFrames; ++k) v[k] = k < it.fp.n ? __ldg(it.fp.f[k] + i) : 0.0f;
+        it.v4[i] = make_float4(v[0], v[1], v[2], v[3]);
     }
 }
 
@@ -1455,7 +1481,7 @@ int near_row_steps() { return kNearRow; }
 
 size_t batch_smem_per_warp(int mode) {
     if (mode == kBatchTraceMarch) return (size_t)kNear * kLanes * sizeof(float);
-    if (mode >= kBatchFieldF32) return kFieldSmemPerWarp;
+    if (mode >= kBatchFieldF32) return kFieldSmemPerWarp;  // the field and frames modes
     return 0;
 }
 
@@ -1558,6 +1584,12 @@ cudaError_t project_frames(Op op, const ProjParams& p, const OpArgs& a, const Fr
         if (a.far.b16) return launch_frames<Op::Adjoint, kFieldBF16>(p, a, fr, s);
     }
     return cudaErrorInvalidValue;
+}
+
+cudaError_t frame_pack_batch(const PackItem* d_items, int n_items, cudaStream_t s) {
+    if (n_items == 0) return cudaSuccess;
+    frame_pack_batch_kernel<<<dim3(128, n_items), 256, 0, s>>>(d_items);
+    return cudaGetLastError();
 }
 
 cudaError_t forward_prep_batch(const PrepItem* d_items, int n_items, cudaStream_t s) {

@@ -131,6 +131,44 @@ def test_forms_without_shared_passes_run_frame_by_frame(torso, cache, prec, exac
         check(fwd[i], f1, f"forward frame {i}")
 
 
+def test_full_size_torso_frames_equal_single_volume():
+    """The 128x128x159 68Ga torso at 128 rays (the headline configuration), five frames (a group
+    of four and one alone), 6 accelerated MAP-EM iterations: bit-identical to one by one."""
+    rho, truth, spacing = phantoms.torso_phantom(seed=2)
+    with pm.Projector("68Ga", rho, spacing, rays=128, cache=pm.PRC_CACHE_FULL) as P:
+        d_truth = torch.from_numpy(truth).cuda()
+        blur = torch.empty_like(d_truth)
+        P.forward(d_truth, blur)
+        P.synchronize()
+        gs = [phantoms.poisson_counts_device(blur, 5e7 * (k + 1), seed=200 + k) for k in range(5)]
+        torch.cuda.synchronize()
+        outs = [torch.empty_like(d_truth) for _ in gs]
+        P.correct_frames(gs, outs, 6, 0.03, 20.0, True)
+        P.synchronize()
+        for i, g in enumerate(gs):
+            one = torch.empty_like(g)
+            P.correct(g, one, 6, 0.03, 20.0, True)
+            P.synchronize()
+            assert_identical(outs[i], one, f"torso frame {i}")
+
+
+def test_surrogate_field_frames_equal_single_volume():
+    """Frames through a surrogate coefficient field (the traced radial bins with exact fallback
+    rays): the same shared passes over another template, bit-identical per frame."""
+    rho, truth, sp = phantoms.small_phantom(seed=1)
+    with pm.Projector("68Ga", rho, sp, surrogate="traced", precision=pm.PRC_PRECISION_BF16) as Q:
+        assert Q.cache_mode[0] == pm.PRC_CACHE_FULL
+        gs = frames(Q.shape, 4, seed=4)
+        outs = [torch.empty_like(g) for g in gs]
+        Q.correct_frames(gs, outs, 4, 0.03, 20.0, True)
+        Q.synchronize()
+        for i, g in enumerate(gs):
+            one = torch.empty_like(g)
+            Q.correct(g, one, 4, 0.03, 20.0, True)
+            Q.synchronize()
+            assert_identical(outs[i], one, f"surrogate frame {i}")
+
+
 def test_fixture_frames_match_reference_binary(fixture72, ref_golden):
     """The seed-72 fixture as frame 1 of 3: its MAP-EM result is prc.cu's within 1e-5."""
     rho, x, y, shape, sp = fixture72
