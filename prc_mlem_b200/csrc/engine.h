@@ -257,13 +257,6 @@ struct PrepItem {
     float4* u4;
 };
 cudaError_t forward_prep_batch(const PrepItem* d_items, int n_items, cudaStream_t s);
-// Batched interleaving: item i writes v4 = its frames' volumes fp.f[0..fp.n) side by side.
-struct PackItem {
-    FramePrep fp;
-    float4* v4;
-    long long n;
-};
-cudaError_t frame_pack_batch(const PackItem* d_items, int n_items, cudaStream_t s);
 
 // Self-test of the bounded mbarrier wait: a wait that nothing completes, `rounds` rounds.
 cudaError_t wait_selftest(int rounds, unsigned int* error, cudaStream_t s);

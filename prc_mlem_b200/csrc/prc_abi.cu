@@ -1393,7 +1393,8 @@ struct prc_batch {
     static constexpr int kWarpsDefault = 4;
     // Frames sharing one projector with its stored field in both majors go through the
     // projections in chunks of 2..4 (one item of the batched launch each, gathering the
-    // interleaved u4 / r4 of the chunk); chunk_of / slot_of place a frame (-1: its own item).
+    // interleaved u4 / r4 of the chunk: the forward preparation writes u4, the forward's
+    // epilogue the EM ratios r4); chunk_of / slot_of place a frame (-1: its own item).
     std::vector<std::vector<int>> chunks;
     std::vector<float4*> chunk_u4, chunk_r4;
     std::vector<int> chunk_of, slot_of;
@@ -1425,8 +1426,7 @@ void release_graph(prc_batch* b) {
 struct BatchPlan {
     std::vector<unsigned char> host;  // all tables, uploaded at once
     struct Launch {
-        int kind;  // 0 EM phase, 1 projector, 2 forward prep, 3 memset (frame, buffer), 4 copy-out (frame),
-                   // 5 interleaving of the chunks' EM ratios
+        int kind;  // 0 EM phase, 1 projector, 2 forward prep, 3 memset (frame, buffer), 4 copy-out (frame)
         EmPhase phase;
         Op op;
         size_t offset;  // of its table in `host`
@@ -1473,12 +1473,15 @@ BatchPlan plan_batch(prc_batch* b, const float* const* d_g, float* const* d_out,
         }
         return items;
     };
-    auto em_launch = [&](EmPhase ph, size_t off) {
+    auto em_launch = [&](EmPhase ph, size_t off, int n_items) {
         BatchPlan::Launch l{};
-        l.kind = 0, l.phase = ph, l.offset = off, l.n_items = n;
+        l.kind = 0, l.phase = ph, l.offset = off, l.n_items = n_items;
         plan.launches.push_back(l);
     };
-    auto projector_launch = [&](Op op, const std::vector<const float*>& in, const std::vector<float*>& out) {
+    // ratio: inside MAP-EM a chunk's forward pass takes its frames' EM ratios in its epilogue,
+    // interleaved into the chunk's r4 for the adjoint (those frames skip the Ratio phase)
+    auto projector_launch = [&](Op op, const std::vector<const float*>& in, const std::vector<float*>& out,
+                                bool ratio) {
         std::vector<BatchItem> items;
         int blocks = 0;
         size_t smem = 0;
@@ -1498,6 +1501,15 @@ BatchPlan plan_batch(prc_batch* b, const float* const* d_g, float* const* d_out,
                 it.fr.n = (int)fr.size();
                 it.fr.in4 = op == Op::Forward ? b->chunk_u4[c] : b->chunk_r4[c];
                 for (size_t j = 0; j < fr.size(); ++j) it.fr.out[j] = out[fr[j]];
+                if (op == Op::Forward && ratio) {
+                    it.fr.out4 = b->chunk_r4[c];
+                    for (size_t j = 0; j < fr.size(); ++j) {
+                        const prc_handle* fh = b->frames[fr[j]];
+                        it.fr.ratio_g[j] = fh->g_em;
+                        it.fr.ratio_eps[j] = reinterpret_cast<const float*>(reinterpret_cast<const char*>(fh->scalars) +
+                                                                            offsetof(EmScalars, eps));
+                    }
+                }
             }
             const int groups = (h->n_active + kLanes - 1) / kLanes;
             it.blocks = (groups + warps - 1) / warps;
@@ -1511,7 +1523,7 @@ BatchPlan plan_batch(prc_batch* b, const float* const* d_g, float* const* d_out,
         l.smem = smem;
         plan.launches.push_back(l);
     };
-    auto forward = [&](const std::vector<const float*>& in, const std::vector<float*>& out) {
+    auto forward = [&](const std::vector<const float*>& in, const std::vector<float*>& out, bool ratio) {
         std::vector<PrepItem> prep(n);
         std::vector<const float*> pin(n);
         for (int i = 0; i < n; ++i) {
@@ -1524,13 +1536,13 @@ BatchPlan plan_batch(prc_batch* b, const float* const* d_g, float* const* d_out,
         BatchPlan::Launch l{};
         l.kind = 2, l.offset = plan.add(prep), l.n_items = n;
         plan.launches.push_back(l);
-        projector_launch(Op::Forward, pin, out);
+        projector_launch(Op::Forward, pin, out, ratio);
     };
     if (forward_only) {  // one forward projection of every frame (autotuning)
         std::vector<const float*> in(n);
         std::vector<float*> out(n);
         for (int i = 0; i < n; ++i) in[i] = d_g[i], out[i] = b->frames[i]->vol[4];
-        forward(in, out);
+        forward(in, out, false);
         return plan;
     }
     // initialisation (prc_em_begin for every frame)
@@ -1540,9 +1552,13 @@ BatchPlan plan_batch(prc_batch* b, const float* const* d_g, float* const* d_out,
             l.kind = 3, l.frame = i, l.ptr = p;
             plan.launches.push_back(l);
         }
-    em_launch(EmPhase::Begin, plan.add(em_items()));
+    em_launch(EmPhase::Begin, plan.add(em_items()), n);
     for (int it = 0; it < iterations; ++it) {
-        const size_t items = plan.add(em_items());
+        const std::vector<EmItem> all = em_items();
+        const size_t items = plan.add(all);
+        std::vector<EmItem> unchunked;  // the frames whose ratio is a phase of its own
+        for (int i = 0; i < n; ++i)
+            if (b->chunk_of[i] < 0) unchunked.push_back(all[i]);
         std::vector<const float*> start(n), est_in(n);
         std::vector<float*> est(n), prev(n);
         for (int i = 0; i < n; ++i) {
@@ -1551,24 +1567,12 @@ BatchPlan plan_batch(prc_batch* b, const float* const* d_g, float* const* d_out,
             est_in[i] = bufs[i].est;
             prev[i] = bufs[i].prev;
         }
-        if (accel) em_launch(EmPhase::Extrapolate, items);
-        forward(start, est);
-        em_launch(EmPhase::Ratio, items);
-        if (!b->chunks.empty()) {  // the chunks' EM ratios, interleaved for their adjoint passes
-            std::vector<PackItem> pack(b->chunks.size());
-            for (size_t c = 0; c < b->chunks.size(); ++c) {
-                pack[c].fp.n = (int)b->chunks[c].size();
-                for (size_t j = 0; j < b->chunks[c].size(); ++j) pack[c].fp.f[j] = est_in[b->chunks[c][j]];
-                pack[c].v4 = b->chunk_r4[c];
-                pack[c].n = (long long)b->frames[b->chunks[c][0]]->n;
-            }
-            BatchPlan::Launch l{};
-            l.kind = 5, l.offset = plan.add(pack), l.n_items = (int)pack.size();
-            plan.launches.push_back(l);
-        }
-        projector_launch(Op::Adjoint, est_in, prev);
-        em_launch(EmPhase::Update, items);
-        if (beta > 0.0f || accel) em_launch(EmPhase::Finish, items);
+        if (accel) em_launch(EmPhase::Extrapolate, items, n);
+        forward(start, est, true);
+        if (!unchunked.empty()) em_launch(EmPhase::Ratio, plan.add(unchunked), (int)unchunked.size());
+        projector_launch(Op::Adjoint, est_in, prev, false);
+        em_launch(EmPhase::Update, items, n);
+        if (beta > 0.0f || accel) em_launch(EmPhase::Finish, items, n);
         for (int i = 0; i < n; ++i) {  // prc.cu:697-700
             if (accel) {
                 std::swap(bufs[i].y, bufs[i].h_prev);
@@ -1595,7 +1599,7 @@ int enqueue_plan(prc_batch* b, const BatchPlan& plan, float* const* d_out, float
     const int em_blocks = std::max(1, std::min(kReduceBlocks, 4096 / std::max(1, (int)b->frames.size())));
     for (const BatchPlan::Launch& l : plan.launches) {
         cudaError_t e = cudaSuccess;
-        const bool kernel = l.kind <= 2 || l.kind == 5;
+        const bool kernel = l.kind <= 2;
         if (timed && kernel) {
             std::pair<cudaEvent_t, cudaEvent_t> ev{nullptr, nullptr};
             PRC_CUDA(cudaEventCreate(&ev.first));
@@ -1622,9 +1626,7 @@ int enqueue_plan(prc_batch* b, const BatchPlan& plan, float* const* d_out, float
                 e = cudaMemcpyAsync(d_out[l.frame], l.ptr, b->frames[l.frame]->n * sizeof(float),
                                     cudaMemcpyDeviceToDevice, b->stream);
                 break;
-            case 5:
-                e = frame_pack_batch(reinterpret_cast<const PackItem*>(base + l.offset), l.n_items, b->stream);
-                break;
+
         }
         if (e != cudaSuccess) return fail(PRC_ERR_CUDA, std::string("CUDA error '") + cudaGetErrorString(e) +
                                                             "' in the batched MAP-EM schedule");

@@ -1346,16 +1346,6 @@ __global__ void forward_prep_batch_kernel(const PrepItem* items) {
     }
 }
 
-__global__ void frame_pack_batch_kernel(const PackItem* items) {
-    const PackItem it = items[blockIdx.y];
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < it.n; i += (long long)gridDim.x * blockDim.x) {
-        float v[kMaxFrames];
-#pragma unroll
-        for (int k = 0; k < kMaxFrames; ++k) v[k] = k < it.fp.n ? __ldg(it.fp.f[k] + i) : 0.0f;
-        it.v4[i] = make_float4(v[0], v[1], v[2], v[3]);
-    }
-}
-
 template <Op OP, bool EXACT, int NEAR_MODE, int FAR_MODE>
 cudaError_t launch(const ProjParams& p, const OpArgs& a, cudaStream_t s) {
     const int groups = (p.n_active + kLanes - 1) / kLanes;
@@ -1584,12 +1574,6 @@ cudaError_t project_frames(Op op, const ProjParams& p, const OpArgs& a, const Fr
         if (a.far.b16) return launch_frames<Op::Adjoint, kFieldBF16>(p, a, fr, s);
     }
     return cudaErrorInvalidValue;
-}
-
-cudaError_t frame_pack_batch(const PackItem* d_items, int n_items, cudaStream_t s) {
-    if (n_items == 0) return cudaSuccess;
-    frame_pack_batch_kernel<<<dim3(128, n_items), 256, 0, s>>>(d_items);
-    return cudaGetLastError();
 }
 
 cudaError_t forward_prep_batch(const PrepItem* d_items, int n_items, cudaStream_t s) {
