@@ -239,10 +239,10 @@ __global__ void geometry_weights_kernel(Grid g, float* geo_w) {
 // the volume's faces test each neighbour.  Per neighbour the arithmetic is update_body's, in the
 // same order, so the result is the same for every voxel.
 template <bool SUM>
-__global__ void __launch_bounds__(kEmThreads) update_active_kernel(
+__device__ __forceinline__ void update_active_body(
     const float* __restrict__ f, const float* __restrict__ back, const unsigned char* __restrict__ support,
-    float* __restrict__ next, const int* __restrict__ active, int n_active, Grid g, const float* __restrict__ geo_w,
-    float beta, float gamma, EmScalars* sc, Reduction r) {
+    float* __restrict__ next, const int* __restrict__ active, int n_active, const Grid& g, const float* __restrict__ geo_w,
+    float beta, float gamma, EmScalars* sc, const Reduction& r) {
     __shared__ float w_sh[27];
     if (threadIdx.x < 27) w_sh[threadIdx.x] = geo_w[threadIdx.x];
     __syncthreads();
@@ -291,6 +291,14 @@ __global__ void __launch_bounds__(kEmThreads) update_active_kernel(
             sc->sum = t[0];
             sc->scale = t[0] > 0.0 ? (float)(sc->support_sum / t[0]) : 1.0f;
         });
+}
+
+template <bool SUM>
+__global__ void __launch_bounds__(kEmThreads) update_active_kernel(
+    const float* __restrict__ f, const float* __restrict__ back, const unsigned char* __restrict__ support,
+    float* __restrict__ next, const int* __restrict__ active, int n_active, Grid g, const float* __restrict__ geo_w,
+    float beta, float gamma, EmScalars* sc, Reduction r) {
+    update_active_body<SUM>(f, back, support, next, active, n_active, g, geo_w, beta, gamma, sc, r);
 }
 
 // Count rescale and, when accelerating, the step h = next - y and the two FP64 inner products
@@ -381,11 +389,14 @@ __global__ void ratio_batch_kernel(const EmItem* items) {
     const EmItem& it = items[blockIdx.y];
     ratio_body(it.g, it.est, it.v.support, it.v.n, it.v.scalars);
 }
+// The batched RDP update over each item's tissue list (the single-volume em_update_active); `est`
+// is 0 off the support already (the forward preparation, the ratio or the chunk's epilogue put it there).
 template <bool SUM>
-__global__ void update_batch_kernel(const EmItem* items, float beta, float gamma, bool accelerate) {
+__global__ void __launch_bounds__(kEmThreads) update_batch_kernel(const EmItem* items, float beta, float gamma,
+                                                                  bool accelerate) {
     const EmItem& it = items[blockIdx.y];
-    update_body<SUM>(accelerate ? it.y : it.f, it.prev, it.v.support, it.est, it.grid, beta, gamma, it.v.scalars,
-                     it.v.red);
+    update_active_body<SUM>(accelerate ? it.y : it.f, it.prev, it.v.support, it.est, it.active, it.n_active, it.grid,
+                            it.geo_w, beta, gamma, it.v.scalars, it.v.red);
 }
 template <bool RESIDUAL>
 __global__ void finish_batch_kernel(const EmItem* items, bool use_scale) {

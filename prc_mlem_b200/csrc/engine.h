@@ -348,6 +348,8 @@ struct EmItem {
     Grid grid;
     int n_active;
     int pad;
+    const int* active;    // the tissue voxels (the RDP update visits only these)
+    const float* geo_w;   // the RDP's 27 neighbour distance weights
     const float* g_in;
     float* g;
     float* f;

@@ -1466,6 +1466,8 @@ BatchPlan plan_batch(prc_batch* b, const float* const* d_g, float* const* d_out,
             it.v = h->em_volumes();
             it.grid = h->g;
             it.n_active = h->n_active;
+            it.active = h->active;
+            it.geo_w = h->geo_w;
             it.g_in = d_g ? d_g[i] : nullptr;
             it.g = h->g_em;
             it.f = bufs[i].f, it.prev = bufs[i].prev, it.y = bufs[i].y, it.h_prev = bufs[i].h_prev,
