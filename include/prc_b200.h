@@ -195,9 +195,10 @@ int prc_em_run_host(prc_handle* h, const float* g_host, float* out_host, int ite
  * volume per process).  With the stored field (PRC_CACHE_FULL in both majors) every projection
  * reads the field once for up to four frames, and each frame's result is bit-identical to the
  * single-volume entry point's on the same input; other forms (and the bf16-volume precision in
- * MAP-EM) run the frames one after another through the single-volume entry points.  d_in / d_g and d_out are arrays of
- * n_frames device pointers to distinct volumes; enqueued on `stream` like the single-volume
- * forms.  The handle keeps n_frames sets of MAP-EM volumes (7 volumes each) after the first call;
+ * MAP-EM) run the frames one after another through the single-volume entry points.  d_in / d_g
+ * and d_out are arrays of n_frames device pointers to distinct volumes; enqueued on `stream`
+ * like the single-volume forms.  After the first call the handle keeps, for reuse, n_frames sets of MAP-EM volumes
+ * (7 volumes each) and two interleaved volumes (16 bytes per voxel) per group of four frames;
  * the single-volume MAP-EM state is separate and untouched. */
 int prc_forward_frames(prc_handle* h, int n_frames, const float* const* d_in, float* const* d_out, void* stream);
 int prc_adjoint_frames(prc_handle* h, int n_frames, const float* const* d_in, float* const* d_out, void* stream);
