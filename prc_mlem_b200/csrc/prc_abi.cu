@@ -39,6 +39,10 @@ int fail(int code, const std::string& msg) {
 
 void prc::set_last_error(const std::string& msg) { g_last_error = msg; }
 
+// One density map's projector and MAP-EM state.  A batch frame of the same study copies its
+// owner's handle (borrow_projector) and then resets what a handle owns (stream, allocations,
+// u, scratch, MAP-EM and frame state, timing events): a member added here that a handle owns
+// must be reset there as well, or the copy would share it.
 struct prc_handle {
     Grid g{};
     RangeModel model;
